@@ -1,0 +1,340 @@
+"""Benchmark of the SPH interpolation hot path on B200.
+
+Workload (one step): the Plummer-sphere configuration -- N = 2,000,000
+particles (a = 0.1, truncated at 10a, seed 1), symmetric strategy with
+nearest-particle h, outputs rho, grad rho, div A, curl A (8 fields) on the
+128^3 StructuredGrid over [-0.5, 0.5]^3, FP32C arithmetic (float pair sums with
+compensated accumulation; double inclusion test and finalisation).  The FP64
+path is timed beside it.
+
+value: samples/s with particles, LBVH and outputs resident in HBM (grid
+coordinates generated on the device), device time from CUDA events.
+e2e:   the same metric through the C ABI with host buffers: the host sample
+coordinates (pinned) are copied in and the 8 output fields copied out inside
+the timed region every step.
+
+Multi-GPU: samples shard over ranks (each rank owns a contiguous slab of
+z-planes of the grid; the particle set and its LBVH are replicated); there is
+no data-path collective.  --impl reference times the CPU restatement of the
+reference's multithreaded CPU path (oracle/, "port") on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "partia.jl_b200"))
+
+METRIC = "samples/s & HBM-roofline frac: FP32 vs FP64 path at stated err; grad/fwd time"
+UNIT = "samples/s"
+NGRID = 128
+CATALOG = dict(scalars=[0], shepard=[0], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])  # cols: rho, Ax, Ay, Az
+L_OUT = 8
+NCOL_USED = 4
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per launch of the point kernel from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "k_points_c2_traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                v = [s.strip() for s in out.stdout.strip().split(",")]
+                if len(v) >= 7:
+                    self.samples.append(v)
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def make_workload():
+    from partia_b200 import workloads as W
+    d = W.plummer_c2()
+    axis = np.linspace(-0.5, 0.5, NGRID)  # replaced by the LinRange values below
+    from partia_b200 import linrange
+    axis = linrange(-0.5, 0.5, NGRID)
+    return d, axis
+
+
+def cpu_reference(args, d, axis, steps, warmup, threads=None):
+    """Oracle port on the host cores over a bounded random sample of grid points."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    nthr = O.set_threads(threads or (os.cpu_count() or 1))
+    t0 = time.time()
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], d["h"], d["rho"], [d["rho"], d["Ax"], d["Ay"], d["Az"]])
+    build_s = time.time() - t0
+    rng = np.random.default_rng(12345)
+    cat = O.Catalog(**CATALOG)
+    # calibrate the sample size to ~args.cpu_seconds of work per step
+    probe = 512
+    idx = rng.integers(0, NGRID ** 3, probe)
+    i, r = idx % NGRID, idx // NGRID
+    s = (axis[i], axis[r % NGRID], axis[r // NGRID])
+    t0 = time.time()
+    orc.interp_points(*s, cat, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    per = max((time.time() - t0) / probe, 1e-7)
+    ns = int(min(max(args.cpu_seconds / per, 2000), NGRID ** 3))
+    times = []
+    for k in range(warmup + steps):
+        idx = rng.integers(0, NGRID ** 3, ns)
+        i, r = idx % NGRID, idx // NGRID
+        s = (axis[i], axis[r % NGRID], axis[r // NGRID])
+        t0 = time.time()
+        orc.interp_points(*s, cat, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+        dt = time.time() - t0
+        if k >= warmup:
+            times.append(dt)
+    val = ns / float(np.median(times))
+    return dict(value=val, unit=UNIT, cores=nthr, kind="port",
+                sample=f"{ns} random grid points of the 128^3 grid per step (of 2,097,152), FP64 oracle, "
+                       f"median of {steps}; LBVH build {build_s:.2f} s not timed"), times
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    d, axis = make_workload()
+    cb, times = cpu_reference(args, d, axis, max(args.steps, 1), max(min(args.warmup, 1), 0))
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Plummer sphere, N=2e6)",
+            "config": {"workload": "plummer-2M symmetric rho,grad rho,div A,curl A on 128^3 grid", "N": 2_000_000,
+                       "samples": NGRID ** 3},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=4.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    from partia_b200 import _lib as L
+    from partia_b200.engine import CatalogC, Context
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+
+    d, axis = make_workload()
+    ctx = Context(local)
+    stream = torch.cuda.Stream(device=dev)
+    L.load().psb_set_stream(ctx.h, stream.cuda_stream)
+    cols = [d["rho"], d["Ax"], d["Ay"], d["Az"]]
+    ctx.set_particles(d["x"], d["y"], d["z"], d["m"], d["h"], d["rho"], cols)
+    ctx.build(want_perm=False)
+    cat = CatalogC(**CATALOG)
+
+    # this rank's slab of z-planes
+    z0 = (NGRID * rank) // world
+    z1 = (NGRID * (rank + 1)) // world
+    az = axis[z0:z1]
+    ns = NGRID * NGRID * len(az)
+    outs = [torch.empty(ns, dtype=torch.float64, device=dev) for _ in range(L_OUT)]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step(prec):
+        ctx.interp_grid(axis, axis, az, cat, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, prec=prec, out=outs)
+        return ctx.last_stats
+
+    def timed(prec, steps, warmup):
+        for _ in range(warmup):
+            step(prec)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        kern_ms, pairs = [], 0
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))  # evict L2 between steps
+                ev[k][0].record(stream)
+            st = step(prec)
+            with torch.cuda.stream(stream):
+                ev[k][1].record(stream)
+            kern_ms.append(st.interp_ms)
+            pairs = st.pairs
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        return float(np.sum(step_ms)), step_ms, kern_ms, pairs
+
+    with ClockSampler(local) as clk:
+        tot32, steps32, kern32, pairs = timed(L.PSB_PREC_FP32C, args.steps, args.warmup)
+    launches_per_step = ctx.last_stats.launches
+    tot = torch.tensor([tot32], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+    total_samples = NGRID ** 3 if world > 1 else ns
+    value = total_samples * args.steps / (tot.item() / 1e3)
+
+    # FP64 path and accuracy of FP32C against it
+    fp64 = None
+    errs = None
+    if not args.no_fp64:
+        tot64, _, kern64, _ = timed(L.PSB_PREC_FP64, max(2, args.steps // 2), 1)
+        v64 = ns * max(2, args.steps // 2) / (tot64 / 1e3)
+        o32 = [o.clone() for o in outs]
+        step(L.PSB_PREC_FP64)
+        errs = {}
+        names = ["rho", "grad_rho_x", "grad_rho_y", "grad_rho_z", "div_A", "curl_A_x", "curl_A_y", "curl_A_z"]
+        for k in range(L_OUT):
+            a, b = o32[k].double(), outs[k].double()
+            fin = torch.isfinite(b)
+            scale = b[fin].abs().max().item()
+            errs[names[k]] = (a[fin] - b[fin]).abs().max().item() / scale if scale > 0 else 0.0
+        fp64 = {"value": v64, "unit": UNIT, "kernel_ms": float(np.median(kern64)),
+                "speedup_fp32c_vs_fp64": value / v64 if world == 1 else None}
+
+    # e2e through the C ABI with host buffers (pinned), copies inside the timed region
+    X, Y, Z = np.meshgrid(axis, axis, az, indexing="ij")
+    hx = torch.from_numpy(X.ravel(order="F").copy()).pin_memory()
+    hy = torch.from_numpy(Y.ravel(order="F").copy()).pin_memory()
+    hz = torch.from_numpy(Z.ravel(order="F").copy()).pin_memory()
+    hout = [torch.empty(ns, dtype=torch.float64).pin_memory() for _ in range(L_OUT)]
+    hxn, hyn, hzn = hx.numpy(), hy.numpy(), hz.numpy()
+    houtn = [o.numpy() for o in hout]
+
+    def e2e_step():
+        ctx.interp_points(hxn, hyn, hzn, cat, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                          prec=L.PSB_PREC_FP32C, out=houtn)
+        return ctx.last_stats
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_ms = []
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        torch.cuda.synchronize()
+        st = e2e_step()
+        e2e_ms.append(st.total_ms)
+    e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
+    e2e_val = total_samples * args.steps / (e2e_tot.item() / 1e3)
+
+    # roofline of the point kernel (algorithmic bytes per launch)
+    hbm, peak_kind = peaks()
+    kern_ms = float(np.median(kern32))
+    b_alg = ns * (0 + L_OUT * 8) + pairs * (6 + NCOL_USED) * 4
+    achieved = b_alg / (kern_ms / 1e3) / 1e9
+    tr = ncu_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            cpu, _ = cpu_reference(args, d, axis, 1, 0)
+        except Exception as e:  # the oracle build needs g++
+            cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": tot.item() / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "data": "synthetic (seeded Plummer sphere, N=2e6, numpy PCG64 seed 1)",
+            "config": {"workload": "plummer-2M symmetric rho,grad rho,div A,curl A on 128^3 grid",
+                       "N": 2_000_000, "samples": NGRID ** 3, "fields": L_OUT, "strategy": "symmetric",
+                       "h": "nearest particle", "precision": "FP32C", "l2": "flushed (256 MB write) between steps"},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * ns,
+                    "d2h_bytes_per_step": L_OUT * 8 * ns},
+            "gpu_launches": int(args.steps * launches_per_step),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                         "peak_kind": peak_kind,
+                         "traffic": (tr or {}).get("bytes_per_launch") if tr else None,
+                         "kernel": "k_points<double,FP32C,SYMMETRIC,4,INTERP>", "kernel_ms": kern_ms,
+                         "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg)},
+            "fp64": fp64, "fp32c_rel_err_vs_fp64": errs, "grad_fwd_time_ratio": None,
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    ctx.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,196 @@
+// interp.cuh -- device pieces of the interpolation kernels: sample sources,
+// M4 kernel functions, the line-integrated lookup, compensated accumulators
+// and the warp-cooperative stackless traversal.
+#pragma once
+
+#include "psb_common.cuh"
+
+namespace psb {
+
+enum { PREC_FP64 = 0, PREC_FP32C = 1 };
+enum { ST_GATHER = 0, ST_SCATTER = 1, ST_SYMMETRIC = 2 };
+enum { SRC_ARRAYS = 0, SRC_GRID = 1, SRC_BOX = 2, SRC_BEAM = 3 };
+enum { WHAT_INTERP = 0, WHAT_DENSITY = 1, WHAT_DIGEST = 2 };
+
+constexpr int MAX_OUT = 64;
+constexpr int MAX_KC = 8;   // distinct catalog columns per call
+constexpr int LUT_N = 4096;
+
+// Output recipes: each output field is a function of the per-sample sums
+// S1 = sum w, G = sum g, Sw[c] = sum A_c w, Sg[c] = sum A_c g,
+// Dm = sum m W, Dg = sum m gradW  (w = m/rho W, g = m/rho gradW), which is
+// the algebra of general_interpolation.jl:128-214 regrouped.
+enum { OP_SCALAR = 0, OP_GRADC = 1, OP_GRADD = 2, OP_DIV = 3, OP_CURL = 4 };
+struct Recipe {
+    int32_t L;
+    int32_t kc;           // distinct columns used
+    int32_t need_dg;      // density gradient requested
+    int8_t op[MAX_OUT];
+    int8_t a0[MAX_OUT], a1[MAX_OUT], a2[MAX_OUT], a3[MAX_OUT];
+};
+
+// ---------------------------------------------------------------------------
+// Sample sources.  A warp owns one tile of 32 samples; tiles are ordered so
+// that the 32 samples of a tile are spatially close.
+// ---------------------------------------------------------------------------
+template <class T> struct SampleSrc {
+    int kind;
+    int64_t ns;
+    const T* a[6];               // SRC_ARRAYS: x,y,z (points) or ox,oy,oz,dx,dy,dz (lines)
+    const uint32_t* order;       // SRC_ARRAYS: Morton order of the samples (nullable)
+    const T* ax; const T* ay; const T* az;
+    int64_t nx, ny, nz;
+    T frame[12];                 // position, right, up, forward
+    T params[6];                 // xmin,xmax, ymin,ymax, zmin,zmax
+    int64_t ntiles;
+};
+
+// sample index of (tile, lane), or -1
+template <class T> __device__ __forceinline__ int64_t sample_of(const SampleSrc<T>& s, int64_t tile, int lane) {
+    if (s.kind == SRC_ARRAYS) {
+        int64_t k = tile * 32 + lane;
+        if (k >= s.ns) return -1;
+        return s.order ? (int64_t)s.order[k] : k;
+    }
+    if (s.kind == SRC_BEAM) {  // 8 x 4 pixel tiles
+        int64_t nbx = (s.nx + 7) >> 3;
+        int64_t bx = tile % nbx, by = tile / nbx;
+        int64_t i = bx * 8 + (lane & 7), j = by * 4 + (lane >> 3);
+        if (i >= s.nx || j >= s.ny) return -1;
+        return i + s.nx * j;
+    }
+    // 4 x 4 x 2 voxel tiles
+    int64_t nbx = (s.nx + 3) >> 2, nby = (s.ny + 3) >> 2;
+    int64_t bx = tile % nbx, r = tile / nbx;
+    int64_t by = r % nby, bz = r / nby;
+    int64_t i = bx * 4 + (lane & 3), j = by * 4 + ((lane >> 2) & 3), k = bz * 2 + (lane >> 4);
+    if (i >= s.nx || j >= s.ny || k >= s.nz) return -1;
+    return i + s.nx * (j + s.ny * k);
+}
+
+// coordinates of sample k (points) or origin + direction (lines)
+template <class T> __device__ __forceinline__ void sample_coords(const SampleSrc<T>& s, int64_t k, T p[3], T d[3]) {
+    if (s.kind == SRC_ARRAYS) {
+        p[0] = s.a[0][k]; p[1] = s.a[1][k]; p[2] = s.a[2][k];
+        if (s.a[3]) { d[0] = s.a[3][k]; d[1] = s.a[4][k]; d[2] = s.a[5][k]; }
+        return;
+    }
+    if (s.kind == SRC_GRID) {
+        int64_t i = k % s.nx, r = k / s.nx;
+        p[0] = s.ax[i]; p[1] = s.ay[r % s.ny]; p[2] = s.az[r / s.ny];
+        return;
+    }
+    // Frame-based Cartesian plane / box, src/julia/Grids/grids/coordinate.jl:37-151:
+    // delta = (max - min) / (n - 1); xi = min + (i - 1) * delta;
+    // x = x0 + xi * rx + eta * ux [+ zeta * fx], evaluated left to right.
+    const T* f = s.frame;
+    int64_t i = k % s.nx, r = k / s.nx;
+    int64_t j = r % s.ny, l = r / s.ny;
+    T dx = X<T>::div(X<T>::sub(s.params[1], s.params[0]), (T)(s.nx - 1));
+    T dy = X<T>::div(X<T>::sub(s.params[3], s.params[2]), (T)(s.ny - 1));
+    T xi = X<T>::add(s.params[0], X<T>::mul((T)i, dx));
+    T eta = X<T>::add(s.params[2], X<T>::mul((T)j, dy));
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        p[c] = X<T>::add(X<T>::add(f[c], X<T>::mul(xi, f[3 + c])), X<T>::mul(eta, f[6 + c]));
+    if (s.kind == SRC_BOX) {
+        T dz = X<T>::div(X<T>::sub(s.params[5], s.params[4]), (T)(s.nz - 1));
+        T zeta = X<T>::add(s.params[4], X<T>::mul((T)l, dz));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) p[c] = X<T>::add(p[c], X<T>::mul(zeta, f[9 + c]));
+    } else {  // SRC_BEAM: every direction is the frame forward
+        d[0] = f[9]; d[1] = f[10]; d[2] = f[11];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// M4 spline (kernel_function/kernels/M4_spline.jl:13-36; 3D norm 1/pi).
+// The fast path evaluates f and f' together from q = r / h.
+// ---------------------------------------------------------------------------
+template <class C> __device__ __forceinline__ void m4_fdf(C q, C& f, C& df) {
+    C a = C(2) - q, b = C(1) - q;
+    C a2 = a * a, b2 = b * b;
+    C fo = C(0.25) * a2 * a;      // 1 <= q < 2
+    C dfo = C(-0.75) * a2;
+    C fi = fo - b2 * b;           // 0 <= q < 1
+    C dfi = dfo + C(3) * b2;
+    f = (q < C(1)) ? fi : ((q < C(2)) ? fo : C(0));
+    df = (q < C(1)) ? dfi : ((q < C(2)) ? dfo : C(0));
+}
+template <class C> __device__ __forceinline__ C m4_f(C q) {
+    C a = C(2) - q, b = C(1) - q;
+    C fo = C(0.25) * a * a * a;
+    C fi = fo - b * b * b;
+    return (q < C(1)) ? fi : ((q < C(2)) ? fo : C(0));
+}
+template <class C> __device__ __forceinline__ C inv_pi();
+template <> __device__ __forceinline__ double inv_pi<double>() { return 0.31830988618379067154; }
+template <> __device__ __forceinline__ float inv_pi<float>() { return 0.318309886183790671538f; }
+
+// ---------------------------------------------------------------------------
+// Compensated float accumulator (Kahan).  The _rn intrinsics keep the
+// compensation exact (no contraction).
+// ---------------------------------------------------------------------------
+struct KahanF {
+    float s, c;
+    __device__ __forceinline__ void zero() { s = 0.f; c = 0.f; }
+    __device__ __forceinline__ void add(float v) {
+        float y = __fsub_rn(v, c);
+        float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    __device__ __forceinline__ double get() const { return (double)s - (double)c; }
+};
+struct PlainD {
+    double s;
+    __device__ __forceinline__ void zero() { s = 0.0; }
+    __device__ __forceinline__ void add(double v) { s += v; }
+    __device__ __forceinline__ double get() const { return s; }
+};
+
+// ---------------------------------------------------------------------------
+// Warp-cooperative stackless DFS over left + escape links
+// (LinearBVHTraversalMacros.jl:26-108 and variants).  All lanes walk the same
+// node sequence.  A lane that prunes node X waits until the warp reaches
+// escape[X], which is exactly the node the lane's own stackless traversal
+// would visit next, so every lane sees the same leaves in the same order as
+// the reference's per-sample traversal.  The warp descends into X when any
+// active lane wants it.  The loop is bounded by 4n+8 steps.
+// node_fn(ni) -> true to descend (internal node record ni = id-1);
+// leaf_fn(li) -> processes 0-based Morton leaf li.
+// ---------------------------------------------------------------------------
+template <class NodeFn, class LeafFn>
+__device__ __forceinline__ bool warp_traverse(int32_t start, int64_t n, const int32_t* __restrict__ left,
+                                              const int32_t* __restrict__ escape, bool lane_valid,
+                                              NodeFn node_fn, LeafFn leaf_fn) {
+    int32_t node = start;
+    int32_t resume = lane_valid ? -1 : 0;
+    const int64_t bound = 4 * n + 8;
+    int64_t steps = 0;
+    const int64_t maxid = 2 * n - 1;
+    while (node != 0) {
+        // corrupt links (an id outside 1..2n-1) or a cycle end the walk with an error
+        if (++steps > bound || node < 0 || (int64_t)node > maxid) return false;
+        if (resume == node) resume = -1;
+        const bool active = (resume == -1);
+        if (node >= n) {
+            const int32_t esc = __ldg(&escape[node - 1]);
+            if (active) leaf_fn((int64_t)node - n);
+            node = esc;
+        } else {
+            const int32_t ni = node - 1;
+            const int32_t esc = __ldg(&escape[ni]);
+            bool want = false;
+            if (active) {
+                if (node_fn(ni)) want = true;
+                else resume = esc;
+            }
+            node = __any_sync(PSB_FULL, want) ? __ldg(&left[ni]) : esc;
+        }
+        if (__all_sync(PSB_FULL, resume == 0)) break;
+    }
+    return true;
+}
+
+}  // namespace psb

@@ -1,0 +1,287 @@
+// interp_host.cu -- host drivers of the interpolation calls: argument checks,
+// catalog -> output recipe, host<->device staging, sample ordering, launch,
+// statistics and device error words.
+#include "launch.hpp"
+#include "psb_ctx.hpp"
+#include "psb_host.hpp"
+
+namespace psb {
+
+template <class T> TreeView<T> tree_view(psb_ctx* c) {
+    TreeView<T> v;
+    v.n = c->n;
+    v.root = c->root;
+    v.left = c->left;
+    v.escape = c->escape;
+    v.range_lo = c->range_lo;
+    v.range_hi = c->range_hi;
+    for (int d = 0; d < 3; ++d) { v.nmin[d] = (const T*)c->nmin[d]; v.nmax[d] = (const T*)c->nmax[d]; }
+    v.nscale = (const T*)c->nscale;
+    v.x = (const T*)c->x; v.y = (const T*)c->y; v.z = (const T*)c->z;
+    v.h = (const T*)c->h; v.m = (const T*)c->m; v.rho = (const T*)c->rho;
+    v.cols = (const T* const*)c->d_cols;
+    v.ncol = c->ncol;
+    v.node_lo = c->node_lo; v.node_hi = c->node_hi; v.leaf4 = c->leaf4;
+    v.anchor = c->anchor; v.mrho = c->mrho; v.mf = c->mf;
+    v.coord_err = c->coord_err;
+    return v;
+}
+template TreeView<double> tree_view<double>(psb_ctx*);
+template TreeView<float> tree_view<float>(psb_ctx*);
+
+// InterpolationCatalogConcise -> per-output recipe over the distinct columns.
+// Output order: scalars, 3 per gradient, 1 per divergence, 3 per curl
+// (grid_interpolation/kernels/PointSamples_kernel.jl:30-71).
+int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu) {
+    rec = Recipe();
+    colu.clear();
+    if (!cat) return fail(c, PSB_EINVAL, "catalog must not be NULL");
+    if (cat->n_scalar < 0 || cat->n_grad < 0 || cat->n_div < 0 || cat->n_curl < 0)
+        return fail(c, PSB_EINVAL, "catalog counts must be non-negative");
+    if (line && (cat->n_grad || cat->n_div || cat->n_curl))
+        return fail(c, PSB_EINVAL, "line-integrated interpolation supports scalar quantities only");
+    const int L = cat->n_scalar + 3 * cat->n_grad + cat->n_div + 3 * cat->n_curl;
+    if (L > MAX_OUT) return fail(c, PSB_EUNSUPPORTED, "catalog expands to more than 64 output fields");
+    auto col_index = [&](int slot, int& ci) -> int {
+        if (slot < 0 || slot >= c->ncol) return fail(c, PSB_EINVAL, "catalog column slot " + std::to_string(slot) +
+                                                     " out of range (ncol=" + std::to_string(c->ncol) + ")");
+        for (size_t q = 0; q < colu.size(); ++q)
+            if (colu[q] == slot) { ci = (int)q; return PSB_OK; }
+        if ((int)colu.size() >= MAX_KC) return fail(c, PSB_EUNSUPPORTED, "catalog references more than 8 distinct columns");
+        colu.push_back(slot);
+        ci = (int)colu.size() - 1;
+        return PSB_OK;
+    };
+    int o = 0, ci, cj, ck, rc;
+    for (int j = 0; j < cat->n_scalar; ++j) {
+        if ((rc = col_index(cat->scalar_slots[j], ci))) return rc;
+        rec.op[o] = OP_SCALAR; rec.a0[o] = (int8_t)ci; rec.a1[o] = (int8_t)(cat->scalar_shepard[j] ? 1 : 0); ++o;
+    }
+    for (int j = 0; j < cat->n_grad; ++j) {
+        int slot = cat->grad_slots[j];
+        if (slot == -1) {
+            rec.need_dg = 1;
+            for (int d = 0; d < 3; ++d) { rec.op[o] = OP_GRADD; rec.a1[o] = (int8_t)d; ++o; }
+        } else {
+            if ((rc = col_index(slot, ci))) return rc;
+            for (int d = 0; d < 3; ++d) { rec.op[o] = OP_GRADC; rec.a0[o] = (int8_t)ci; rec.a1[o] = (int8_t)d; ++o; }
+        }
+    }
+    for (int j = 0; j < cat->n_div; ++j) {
+        if ((rc = col_index(cat->div_slots[3 * j], ci)) || (rc = col_index(cat->div_slots[3 * j + 1], cj)) ||
+            (rc = col_index(cat->div_slots[3 * j + 2], ck)))
+            return rc;
+        rec.op[o] = OP_DIV; rec.a0[o] = (int8_t)ci; rec.a1[o] = (int8_t)cj; rec.a2[o] = (int8_t)ck; ++o;
+    }
+    for (int j = 0; j < cat->n_curl; ++j) {
+        if ((rc = col_index(cat->curl_slots[3 * j], ci)) || (rc = col_index(cat->curl_slots[3 * j + 1], cj)) ||
+            (rc = col_index(cat->curl_slots[3 * j + 2], ck)))
+            return rc;
+        for (int d = 0; d < 3; ++d) {
+            rec.op[o] = OP_CURL; rec.a0[o] = (int8_t)ci; rec.a1[o] = (int8_t)cj; rec.a2[o] = (int8_t)ck;
+            rec.a3[o] = (int8_t)d; ++o;
+        }
+    }
+    rec.L = L;
+    rec.kc = (int)colu.size();
+    return PSB_OK;
+}
+
+static float ms_between(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+template <class T>
+static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, const psb_catalog* cat,
+                     int prec, void* const* out, uint32_t flags, psb_stats* stats, int what, int64_t* dcount,
+                     uint64_t* dhash, void* ha_out) {
+    const bool dev = (flags & PSB_FLAG_DEVICE_PTRS) != 0;
+    cudaStream_t s = c->stream;
+    const size_t es = sizeof(T);
+    const int64_t ns = rq.ns;
+    int launches = 0;
+
+    Args<T> A;
+    memset((void*)&A, 0, sizeof(A));
+    std::vector<int> colu;
+    if (what == WHAT_INTERP) {
+        int rc = make_recipe(c, cat, rq.line, A.rec, colu);
+        if (rc) return rc;
+    } else {
+        A.rec.L = (what == WHAT_DENSITY) ? 1 : 0;
+    }
+    const int L = A.rec.L;
+    if (what == WHAT_INTERP && L > 0 && !out) return fail(c, PSB_EINVAL, "output pointer array must not be NULL");
+    for (int k = 0; what == WHAT_INTERP && k < L && ns > 0; ++k)
+        if (!out[k]) return fail(c, PSB_EINVAL, "output pointer " + std::to_string(k) + " is NULL");
+    if (what == WHAT_DENSITY && ns > 0 && (!out || !out[0])) return fail(c, PSB_EINVAL, "density output is NULL");
+    if (what == WHAT_DIGEST && ns > 0 && (!dcount || !dhash)) return fail(c, PSB_EINVAL, "digest outputs are NULL");
+    const bool need_h = (st != ST_SCATTER) && !(hmode == PSB_H_NEAREST && !rq.line);
+    if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+
+    A.tv = tree_view<T>(c);
+    A.hmode = hmode;
+    A.err = c->d_err;
+    A.lut_d = c->lut_d;
+    A.lut_f = c->lut_f;
+    for (size_t q = 0; q < colu.size(); ++q) {
+        A.colT[q] = (const T*)c->cols[colu[q]];
+        A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
+    }
+    SampleSrc<T>& S = A.src;
+    S.kind = rq.kind;
+    S.ns = ns;
+
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[0], s), "event");
+    // ---- stage samples ----
+    const int narr = rq.line ? 6 : 3;
+    if (rq.kind == SRC_ARRAYS) {
+        if (dev) {
+            for (int q = 0; q < narr; ++q) S.a[q] = (const T*)rq.a[q];
+        } else if (ns > 0) {
+            char* buf = (char*)scratch(c, 0, es * ns * narr);
+            if (!buf) return fail(c, PSB_ENOMEM, "scratch allocation failed (samples)");
+            for (int q = 0; q < narr; ++q) {
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(buf + es * ns * q, rq.a[q], es * ns, cudaMemcpyHostToDevice, s), "sample H2D");
+                S.a[q] = (const T*)(buf + es * ns * q);
+            }
+        }
+        S.ntiles = (ns + 31) / 32;
+    } else if (rq.kind == SRC_GRID) {
+        char* buf = (char*)scratch(c, 14, es * (rq.nx + rq.ny + rq.nz));
+        if (!buf) return fail(c, PSB_ENOMEM, "scratch allocation failed (axes)");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(buf, rq.ax, es * rq.nx, cudaMemcpyHostToDevice, s), "axis H2D");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(buf + es * rq.nx, rq.ay, es * rq.ny, cudaMemcpyHostToDevice, s), "axis H2D");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(buf + es * (rq.nx + rq.ny), rq.az, es * rq.nz, cudaMemcpyHostToDevice, s), "axis H2D");
+        S.ax = (const T*)buf; S.ay = (const T*)(buf + es * rq.nx); S.az = (const T*)(buf + es * (rq.nx + rq.ny));
+        S.nx = rq.nx; S.ny = rq.ny; S.nz = rq.nz;
+        S.ntiles = ((rq.nx + 3) / 4) * ((rq.ny + 3) / 4) * ((rq.nz + 1) / 2);
+    } else {
+        memcpy(S.frame, rq.frame, es * 12);
+        memcpy(S.params, rq.params, es * (rq.kind == SRC_BOX ? 6 : 4));
+        S.nx = rq.nx; S.ny = rq.ny; S.nz = rq.nz;
+        S.ntiles = (rq.kind == SRC_BOX) ? ((rq.nx + 3) / 4) * ((rq.ny + 3) / 4) * ((rq.nz + 1) / 2)
+                                        : ((rq.nx + 7) / 8) * ((rq.ny + 3) / 4);
+    }
+    if (need_h) {
+        if (dev) A.hs = (const T*)hs;
+        else {
+            const int64_t nh = (hmode == PSB_H_PER_SAMPLE) ? ns : 1;
+            T* hb = (T*)scratch(c, 1, es * std::max<int64_t>(nh, 1));
+            if (!hb) return fail(c, PSB_ENOMEM, "scratch allocation failed (hs)");
+            if (nh > 0) PSB_CUDA_TRY(c, cudaMemcpyAsync(hb, hs, es * nh, cudaMemcpyHostToDevice, s), "hs H2D");
+            A.hs = hb;
+        }
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[1], s), "event");
+
+    // ---- Morton order of explicit samples ----
+    if (rq.kind == SRC_ARRAYS && ns > 64) {
+        uint64_t* codes = (uint64_t*)scratch(c, 3, sizeof(uint64_t) * ns);
+        uint32_t* idx = (uint32_t*)scratch(c, 4, sizeof(uint32_t) * ns);
+        if (!codes || !idx) return fail(c, PSB_ENOMEM, "scratch allocation failed (sample order)");
+        double3 lo = make_double3(c->bbox[0], c->bbox[1], c->bbox[2]);
+        double sc[3];
+        for (int d = 0; d < 3; ++d) {
+            double ext = c->bbox[3 + d] - c->bbox[d];
+            sc[d] = ext > 0 ? 2097151.0 / ext : 0.0;
+        }
+        k_sample_codes<T><<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(S.a[0], S.a[1], S.a[2], ns, lo,
+                                                                    make_double3(sc[0], sc[1], sc[2]), codes, idx);
+        PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
+        ++launches;
+        PSB_CUDA_TRY(c, radix_sort_pairs(codes, idx, ns, c, 6, &launches), "sample sort");
+        S.order = idx;
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[2], s), "event");
+
+    // ---- outputs ----
+    char* obuf = nullptr;
+    if (what == WHAT_DIGEST) {
+        if (dev) {
+            A.dig_count = dcount; A.dig_hash = dhash; A.ha_out = (T*)ha_out;
+        } else if (ns > 0) {
+            obuf = (char*)scratch(c, 2, (16 + es) * ns);
+            if (!obuf) return fail(c, PSB_ENOMEM, "scratch allocation failed (digest)");
+            A.dig_count = (int64_t*)obuf;
+            A.dig_hash = (uint64_t*)(obuf + 8 * ns);
+            A.ha_out = (T*)(obuf + 16 * ns);
+        }
+    } else {
+        if (dev) {
+            for (int q = 0; q < L; ++q) A.out[q] = (T*)out[q];
+        } else if (ns > 0 && L > 0) {
+            obuf = (char*)scratch(c, 2, es * ns * L);
+            if (!obuf) return fail(c, PSB_ENOMEM, "scratch allocation failed (outputs)");
+            for (int q = 0; q < L; ++q) A.out[q] = (T*)(obuf + es * ns * q);
+        }
+    }
+    unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 2 * sizeof(unsigned long long));
+    if (!dstats) return fail(c, PSB_ENOMEM, "scratch allocation failed (stats)");
+    PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 2 * sizeof(unsigned long long), s), "memset stats");
+    A.stats = dstats;
+
+    // ---- launch ----
+    if (ns > 0) {
+        cudaError_t e = rq.line ? launch_lines<T>(A, prec, st, A.rec.kc, what, s)
+                                : launch_points<T>(A, prec, st, A.rec.kc, what, s);
+        PSB_CUDA_TRY(c, e, "interpolation kernel launch");
+        ++launches;
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[3], s), "event");
+
+    // ---- copy back ----
+    if (!dev && ns > 0) {
+        if (what == WHAT_DIGEST) {
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(dcount, A.dig_count, 8 * ns, cudaMemcpyDeviceToHost, s), "digest D2H");
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(dhash, A.dig_hash, 8 * ns, cudaMemcpyDeviceToHost, s), "digest D2H");
+            if (ha_out) PSB_CUDA_TRY(c, cudaMemcpyAsync(ha_out, A.ha_out, es * ns, cudaMemcpyDeviceToHost, s), "digest D2H");
+        } else {
+            for (int q = 0; q < L; ++q)
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(out[q], A.out[q], es * ns, cudaMemcpyDeviceToHost, s), "output D2H");
+        }
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[4], s), "event");
+    unsigned long long hst[2] = {0, 0};
+    unsigned herr = 0;
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(hst, dstats, sizeof(hst), cudaMemcpyDeviceToHost, s), "stats D2H");
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(&herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, s), "error D2H");
+    PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+    if (herr) {
+        cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
+        cudaStreamSynchronize(s);
+        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+    }
+    if (stats) {
+        stats->h2d_ms = ms_between(c->ev[0], c->ev[1]);
+        stats->order_ms = ms_between(c->ev[1], c->ev[2]);
+        stats->nearest_ms = 0.0;
+        stats->interp_ms = ms_between(c->ev[2], c->ev[3]);
+        stats->d2h_ms = ms_between(c->ev[3], c->ev[4]);
+        stats->total_ms = ms_between(c->ev[0], c->ev[4]);
+        stats->pairs = (int64_t)hst[0];
+        stats->exact_retests = (int64_t)hst[1];
+        stats->launches = launches;
+    }
+    return PSB_OK;
+}
+
+int run(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, const psb_catalog* cat, int prec,
+        void* const* out, uint32_t flags, psb_stats* stats, int what, int64_t* dcount, uint64_t* dhash, void* ha_out) {
+    if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before interpolation");
+    if (rq.ns < 0) return fail(c, PSB_EINVAL, "sample count must be non-negative");
+    if (st < 0 || st > 2) return fail(c, PSB_EINVAL, "unknown interpolation strategy");
+    if (prec < 0 || prec > 1) return fail(c, PSB_EINVAL, "unknown precision mode");
+    if (hmode < 0 || hmode > 2) return fail(c, PSB_EINVAL, "unknown smoothing-length mode");
+    if (rq.line && st != ST_SCATTER && hmode == PSB_H_NEAREST)
+        return fail(c, PSB_EINVAL,
+                    "LineSamples_interpolation only supports itpScatter. Line-integrated samples do not have a "
+                    "well-defined query smoothing length ha, so itpGather and itpSymmetric are not supported.");
+    return c->dt == PSB_F64
+               ? run_typed<double>(c, rq, hmode, hs, st, cat, prec, out, flags, stats, what, dcount, dhash, ha_out)
+               : run_typed<float>(c, rq, hmode, hs, st, cat, prec, out, flags, stats, what, dcount, dhash, ha_out);
+}
+
+}  // namespace psb

@@ -1,0 +1,683 @@
+// interp.cu -- point and line interpolation kernels (forward path).
+//
+// Per-sample semantics follow
+//   grid_interpolation/kernels/PointSamples_kernel.jl:7-139   (nearest h, output order)
+//   single_point_interpolation/kernels/general_interpolation.jl:1-669
+//   single_point_interpolation/kernels/scalar_interpolation.jl:1-75 (_density_kernel)
+//   line_integrated_interpolation/kernels/line_integrated_scalar_interpolation.jl:76-214
+//   LinearBVH/LinearBVHQueries.jl:118-140 (LBVH_find_nearest_h)
+// with the traversal of LinearBVH/LinearBVHTraversalMacros.jl:26-953.
+//
+// Precision modes
+//  * exact geometry (double inputs in PSB_PREC_FP64, and every float input):
+//    distances, radii and the inclusion test use the reference's operation
+//    order with exactly rounded intrinsics, so neighbour sets are identical.
+//  * FP32C with double inputs: nodes are tested in float against boxes rounded
+//    outward (a conservative superset); a leaf is accepted or rejected in
+//    float only when it lies outside an error band around the support
+//    radius, otherwise the reference's double test decides.  Neighbour sets
+//    are therefore identical too.  Float differences use coordinates relative
+//    to a per-32-leaf anchor, so their error is relative to the separation.
+#pragma once
+#include <type_traits>
+#include "interp.cuh"
+
+namespace psb {
+
+template <class T> struct Args {
+    TreeView<T> tv;
+    SampleSrc<T> src;
+    int hmode;
+    const T* hs;
+    Recipe rec;
+    const T* colT[MAX_KC];
+    const float* colF[MAX_KC];
+    T* out[MAX_OUT];
+    int64_t* dig_count;
+    uint64_t* dig_hash;
+    T* ha_out;
+    const double* lut_d;
+    const float* lut_f;
+    unsigned* err;
+    unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests
+};
+
+// ---------------------------------------------------------------------------
+// Exact geometry (reference operation order), LinearBVHTraversalMacros.jl:800-953
+// ---------------------------------------------------------------------------
+template <class T> __device__ __forceinline__ T ex_d2_pp(const T p[3], T x, T y, T z) {
+    T s = T(0), d;
+    d = X<T>::sub(p[0], x); s = X<T>::add(s, X<T>::mul(d, d));
+    d = X<T>::sub(p[1], y); s = X<T>::add(s, X<T>::mul(d, d));
+    d = X<T>::sub(p[2], z); s = X<T>::add(s, X<T>::mul(d, d));
+    return s;
+}
+
+template <class T> __device__ __forceinline__ T ex_d2_pbox(const T p[3], const TreeView<T>& tv, int ni) {
+    T s = T(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        T a = __ldg(&tv.nmin[d][ni]), b = __ldg(&tv.nmax[d][ni]);
+        T t = p[d] < a ? X<T>::sub(a, p[d]) : (p[d] > b ? X<T>::sub(p[d], b) : T(0));
+        s = X<T>::add(s, X<T>::mul(t, t));
+    }
+    return s;
+}
+
+// _squared_distance_line_coords: delta = x - o
+template <class T> __device__ __forceinline__ T ex_d2_line(const T o[3], const T m[3], T x, T y, T z) {
+    T c[3] = {x, y, z};
+    T D2 = T(0), Dm = T(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        T D = X<T>::sub(c[d], o[d]);
+        D2 = X<T>::add(D2, X<T>::mul(D, D));
+        Dm = X<T>::add(Dm, X<T>::mul(D, m[d]));
+    }
+    return X<T>::sub(D2, X<T>::mul(Dm, Dm));
+}
+
+// _squared_distance_line_aabb_lower_bound (with _line_intersects_aabb)
+template <class T> __device__ __forceinline__ T ex_d2_line_box(const T o[3], const T m[3], const TreeView<T>& tv, int ni) {
+    T a[3], b[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { a[d] = __ldg(&tv.nmin[d][ni]); b[d] = __ldg(&tv.nmax[d][ni]); }
+    bool hit = true;
+    T tmin = -(T)INFINITY, tmax = (T)INFINITY;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        if (!hit) break;
+        if (m[d] == T(0)) {
+            if (o[d] < a[d] || o[d] > b[d]) hit = false;
+        } else {
+            T t0 = X<T>::div(X<T>::sub(a[d], o[d]), m[d]);
+            T t1 = X<T>::div(X<T>::sub(b[d], o[d]), m[d]);
+            if (t0 > t1) { T tt = t0; t0 = t1; t1 = tt; }
+            tmin = jmax(tmin, t0);
+            tmax = jmin(tmax, t1);
+            if (tmin > tmax) hit = false;
+        }
+    }
+    if (hit) return T(0);
+    const T half = T(0.5);
+    T c[3], r2 = T(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        c[d] = X<T>::mul(X<T>::add(a[d], b[d]), half);
+        T hh = X<T>::mul(X<T>::sub(b[d], a[d]), half);
+        r2 = X<T>::add(r2, X<T>::mul(hh, hh));
+    }
+    // _squared_distance_point_line(center, origin, direction): delta = p - o
+    T D2 = T(0), Dm = T(0);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        T D = X<T>::sub(c[d], o[d]);
+        D2 = X<T>::add(D2, X<T>::mul(D, D));
+        Dm = X<T>::add(Dm, X<T>::mul(D, m[d]));
+    }
+    T dc2 = X<T>::sub(D2, X<T>::mul(Dm, Dm));
+    if (dc2 <= r2) return T(0);
+    T dl = X<T>::sub(X<T>::sqrt(dc2), X<T>::sqrt(r2));
+    return X<T>::mul(dl, dl);
+}
+
+// radius^2 of a leaf or node: gather (K ha)^2, scatter (K hb)^2, symmetric max
+template <int ST, class T> __device__ __forceinline__ T ex_r2(T ra2, T hb) {
+    if (ST == ST_GATHER) return ra2;
+    T r = X<T>::mul(T(2), hb);
+    T r2 = X<T>::mul(r, r);
+    if (ST == ST_SCATTER) return r2;
+    return jmax(ra2, r2);
+}
+
+// ---------------------------------------------------------------------------
+// Conservative float geometry (FP32C with double inputs).
+// ---------------------------------------------------------------------------
+constexpr float U1 = 1.1920928955078125e-07f;  // 2^-23
+constexpr float RELM = 4.76837158203125e-07f;  // 2^-21
+
+// lower bound of the exact squared point-box distance
+__device__ __forceinline__ float lb_d2_pbox(const float pf[3], float pem, float4 lo, float4 hi) {
+    float tx = fmaxf(fmaxf(lo.x - pf[0], pf[0] - hi.x), 0.f);
+    float ty = fmaxf(fmaxf(lo.y - pf[1], pf[1] - hi.y), 0.f);
+    float tz = fmaxf(fmaxf(lo.z - pf[2], pf[2] - hi.z), 0.f);
+    tx = fmaxf(tx * (1.f - 2.f * U1) - pem, 0.f);
+    ty = fmaxf(ty * (1.f - 2.f * U1) - pem, 0.f);
+    tz = fmaxf(tz * (1.f - 2.f * U1) - pem, 0.f);
+    return (tx * tx + ty * ty + tz * tz) * (1.f - RELM);
+}
+
+// upper bound of the node radius^2 (node scale is rounded up)
+template <int ST> __device__ __forceinline__ float hi_r2_node(float ra2_hi, float scale_up) {
+    if (ST == ST_GATHER) return ra2_hi;
+    float r = 2.f * scale_up;
+    float r2 = r * r * (1.f + RELM);
+    if (ST == ST_SCATTER) return r2;
+    return fmaxf(ra2_hi, r2);
+}
+
+// lower bound of the squared distance between a line and a node box.
+// o, m: float line; el: absolute error allowance of the float line near the
+// box (origin and direction rounding).
+__device__ __forceinline__ float lb_d2_line_box(const float o[3], const float m[3], float el, float4 lo, float4 hi) {
+    float a[3] = {lo.x, lo.y, lo.z}, b[3] = {hi.x, hi.y, hi.z};
+    // centre / half-diagonal of the outward-rounded box
+    float c[3], r2 = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        c[d] = 0.5f * (a[d] + b[d]);
+        float hh = 0.5f * (b[d] - a[d]);
+        r2 += hh * hh;
+    }
+    float rb = sqrtf(r2) * (1.f + 4.f * U1);
+    float v[3], vm = 0.f, vv = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { v[d] = c[d] - o[d]; vm += v[d] * m[d]; }
+    float pp = 0.f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { float w = v[d] - vm * m[d]; pp += w * w; vv += v[d] * v[d]; }
+    float dc = sqrtf(pp);
+    float err = el + 8.f * U1 * sqrtf(vv);
+    float g = dc - rb - err;
+    if (g <= 0.f) return 0.f;
+    return g * g * (1.f - RELM);
+}
+
+// ---------------------------------------------------------------------------
+// Point kernel
+// ---------------------------------------------------------------------------
+template <class T, int PREC, int ST, int KC, int WHAT>
+__global__ void __launch_bounds__(128) k_points(const Args<T> A) {
+    using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
+    using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
+    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
+    const TreeView<T>& tv = A.tv;
+    const int lane = threadIdx.x & 31;
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tile >= A.src.ntiles) return;  // warp-uniform
+
+    const int64_t k = sample_of(A.src, tile, lane);
+    const bool valid = k >= 0;
+    T p[3] = {T(0), T(0), T(0)}, dd[3];
+    if (valid) sample_coords(A.src, k, p, dd);
+    float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+    const float pem = U1 * fmaxf(fmaxf(fabsf(pf[0]), fabsf(pf[1])), fabsf(pf[2])) + 1e-30f;
+    const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
+    unsigned long long n_pairs = 0, n_retest = 0;
+    bool ok = true;
+
+    // ---- sample smoothing length (LBVH_find_nearest_h or given) ----
+    T ha = T(0);
+    if (ST != ST_SCATTER) {
+        if (A.hmode == PSB_H_NEAREST) {
+            if (BAND) {
+                double best = INFINITY;
+                int64_t bidx = -1;
+                int64_t ctile = -1;
+                float prel[3] = {0.f, 0.f, 0.f}, ep = 0.f;
+                ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid,
+                    [&](int ni) {
+                        float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
+                        return !((double)lb > best);
+                    },
+                    [&](int64_t li) {
+                        int64_t t = li >> 5;
+                        if (t != ctile) {
+                            ctile = t;
+                            double q0 = (double)p[0] - __ldg(&tv.anchor[3 * t]);
+                            double q1 = (double)p[1] - __ldg(&tv.anchor[3 * t + 1]);
+                            double q2 = (double)p[2] - __ldg(&tv.anchor[3 * t + 2]);
+                            prel[0] = (float)q0; prel[1] = (float)q1; prel[2] = (float)q2;
+                            ep = U1 * fmaxf(fmaxf(fabsf(prel[0]), fabsf(prel[1])), fabsf(prel[2]));
+                        }
+                        float4 L = __ldg(&tv.leaf4[li]);
+                        float dx = prel[0] - L.x, dy = prel[1] - L.y, dz = prel[2] - L.z;
+                        float r = sqrtf(dx * dx + dy * dy + dz * dz);
+                        float e = 1.7320508f * (ep + U1 * fmaxf(fmaxf(fabsf(L.x), fabsf(L.y)), fabsf(L.z))) + 4.f * U1 * r + 1e-30f;
+                        float lo_r = fmaxf(r - e, 0.f);
+                        if ((double)(lo_r * lo_r * (1.f - RELM)) > best) return;
+                        double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                        if (d2 <= best && d2 < best) { best = d2; bidx = li; }
+                    });
+                if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
+            } else {
+                T best = (T)INFINITY;
+                int64_t bidx = -1;
+                ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid,
+                    [&](int ni) { return !(ex_d2_pbox<T>(p, tv, ni) > best); },
+                    [&](int64_t li) {
+                        T d2 = ex_d2_pp<T>(p, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
+                        if (d2 <= best && d2 < best) { best = d2; bidx = li; }
+                    });
+                if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
+            }
+        } else if (valid) {
+            ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
+        }
+    }
+    // radius = Kvalid * ha; radius2 = radius * radius (general_interpolation.jl:20-21)
+    const T ra = X<T>::mul(T(2), ha);
+    const T ra2 = X<T>::mul(ra, ra);
+    float ra2_hi = 0.f, ra2_lo = 0.f;
+    if (BAND && ST != ST_SCATTER) {
+        ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
+        ra2_lo = __double2float_rd((double)ra2) * (1.f - RELM);
+    }
+
+    // ---- per-sample constants of the kernel weights ----
+    const CT sig = inv_pi<CT>();
+    CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
+    if (ST != ST_SCATTER) {
+        ia = CT(1) / (CT)ha;
+        sa3 = sig * ia * ia * ia;
+        sa4 = sa3 * ia;
+    }
+
+    // ---- accumulators ----
+    Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
+    CT dens = CT(0);
+    S1.zero(); Dm.zero();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { G[d].zero(); Dg[d].zero(); }
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+        Sw[c].zero();
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Sg[c][d].zero();
+    }
+    uint64_t hsum = 0;
+    int64_t hcount = 0;
+    const int kc = A.rec.kc;
+    const bool need_dg = A.rec.need_dg != 0;
+
+    int64_t ctile = -1;
+    float prel[3] = {0.f, 0.f, 0.f}, ep = 0.f;
+
+    auto node_fn = [&](int ni) -> bool {
+        if (BAND) {
+            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
+            float lb = lb_d2_pbox(pf, pem, lo, hi);
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+        } else {
+            T d2n = ex_d2_pbox<T>(p, tv, ni);
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            return !(d2n > r2);
+        }
+    };
+
+    auto leaf_fn = [&](int64_t li) {
+        CT dx, dy, dz, d2;
+        T hb = T(0);
+        bool acc;
+        if (BAND) {
+            int64_t t = li >> 5;
+            if (t != ctile) {
+                ctile = t;
+                double q0 = (double)p[0] - __ldg(&tv.anchor[3 * t]);
+                double q1 = (double)p[1] - __ldg(&tv.anchor[3 * t + 1]);
+                double q2 = (double)p[2] - __ldg(&tv.anchor[3 * t + 2]);
+                prel[0] = (float)q0; prel[1] = (float)q1; prel[2] = (float)q2;
+                ep = U1 * fmaxf(fmaxf(fabsf(prel[0]), fabsf(prel[1])), fabsf(prel[2]));
+            }
+            float4 L = __ldg(&tv.leaf4[li]);
+            float fx = prel[0] - L.x, fy = prel[1] - L.y, fz = prel[2] - L.z;
+            float fd2 = fx * fx + fy * fy + fz * fz;
+            float r = sqrtf(fd2);
+            float e = 1.7320508f * (ep + U1 * fmaxf(fmaxf(fabsf(L.x), fabsf(L.y)), fabsf(L.z))) + 4.f * U1 * r + 1e-30f;
+            float rb2 = 4.f * L.w * L.w;
+            float r2lo, r2hi;
+            if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
+            else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
+            else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
+            float up = r + e, dn = fmaxf(r - e, 0.f);
+            if (up * up * (1.f + RELM) < r2lo) acc = true;
+            else if (dn * dn * (1.f - RELM) > r2hi) acc = false;
+            else {
+                ++n_retest;
+                T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
+            }
+            if (!acc) return;
+            dx = (CT)fx; dy = (CT)fy; dz = (CT)fz; d2 = (CT)fd2;
+            hb = (T)L.w;
+        } else {
+            T xb = __ldg(&tv.x[li]), yb = __ldg(&tv.y[li]), zb = __ldg(&tv.z[li]);
+            T e2 = ex_d2_pp<T>(p, xb, yb, zb);
+            hb = __ldg(&tv.h[li]);
+            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
+            dx = (CT)(p[0] - xb); dy = (CT)(p[1] - yb); dz = (CT)(p[2] - zb);
+            d2 = (CT)e2;
+        }
+        ++n_pairs;
+        if (WHAT == WHAT_DIGEST) {
+            ++hcount;
+            hsum += mix64((uint64_t)(li + 1));
+            return;
+        }
+        const CT r = sqrt(d2);
+        const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
+        CT Wsum, csum;  // kernel value and gradient coefficient (g = c * delta)
+        if (ST != ST_SCATTER) {
+            CT f, df;
+            m4_fdf<CT>(r * ia, f, df);
+            Wsum = sa3 * f;
+            csum = sa4 * df * invr;
+        }
+        if (ST != ST_GATHER) {
+            CT ib = CT(1) / (CT)hb;
+            CT sb3 = sig * ib * ib * ib;
+            CT f, df;
+            m4_fdf<CT>(r * ib, f, df);
+            CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
+            if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
+            else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
+        }
+        if (WHAT == WHAT_DENSITY) {
+            dens += (CT)tv.m[li] * Wsum;
+            return;
+        }
+        CT mr = (PREC == PREC_FP64) ? (CT)((double)tv.m[li] / (double)tv.rho[li]) : (CT)__ldg(&tv.mrho[li]);
+        const CT w = mr * Wsum;
+        const CT gc = mr * csum;
+        const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
+        S1.add(w);
+        G[0].add(gx); G[1].add(gy); G[2].add(gz);
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                CT a = (PREC == PREC_FP64) ? (CT)__ldg(&A.colT[c][li]) : (CT)__ldg(&A.colF[c][li]);
+                Sw[c].add(a * w);
+                Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+            }
+        }
+        if (need_dg) {
+            CT mb = (PREC == PREC_FP64) ? (CT)tv.m[li] : (CT)__ldg(&tv.mf[li]);
+            Dm.add(mb * Wsum);
+            CT mc = mb * csum;
+            Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+        }
+    };
+
+    bool ok2 = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
+    ok = ok && ok2;
+
+    // ---- outputs ----
+    if (valid) {
+        if (WHAT == WHAT_DIGEST) {
+            A.dig_count[k] = hcount;
+            A.dig_hash[k] = hsum;
+            if (A.ha_out) A.ha_out[k] = ha;
+        } else if (WHAT == WHAT_DENSITY) {
+            A.out[0][k] = (T)dens;
+        } else {
+            const double s1 = S1.get();
+            const int L = A.rec.L;
+            if (s1 == 0.0) {
+                for (int o = 0; o < L; ++o) A.out[o][k] = qnan<T>();
+            } else {
+                double sw[MAX_KC], sg[MAX_KC][3];
+#pragma unroll
+                for (int c = 0; c < KC; ++c) {
+                    sw[c] = Sw[c].get();
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
+                }
+                const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
+                const double inv = 1.0 / s1;
+                for (int o = 0; o < L; ++o) {
+                    const int op = A.rec.op[o];
+                    const int a0 = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
+                    double v;
+                    if (op == OP_SCALAR) {
+                        v = a1 ? sw[a0] * inv : sw[a0];
+                    } else if (op == OP_GRADC) {
+                        v = sg[a0][a1] - g[a1] * (sw[a0] * inv);
+                    } else if (op == OP_GRADD) {
+                        v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
+                    } else if (op == OP_DIV) {
+                        double f = sg[a0][0] + sg[a1][1] + sg[a2][2];
+                        double b = (sw[a0] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
+                        v = f - b;
+                    } else {  // OP_CURL, component a3
+                        double Ax = sw[a0] * inv, Ay = sw[a1] * inv, Az = sw[a2] * inv;
+                        double f, b;
+                        if (a3 == 0) { f = sg[a1][2] - sg[a2][1]; b = Ay * g[2] - Az * g[1]; }
+                        else if (a3 == 1) { f = sg[a2][0] - sg[a0][2]; b = Az * g[0] - Ax * g[2]; }
+                        else { f = sg[a0][1] - sg[a1][0]; b = Ax * g[1] - Ay * g[0]; }
+                        v = -(f - b);
+                    }
+                    A.out[o][k] = (T)v;
+                }
+            }
+        }
+    }
+    // ---- statistics and errors ----
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+        n_retest += __shfl_xor_sync(PSB_FULL, n_retest, o);
+    }
+    if (lane == 0 && A.stats) {
+        atomicAdd(&A.stats[0], n_pairs);
+        atomicAdd(&A.stats[1], n_retest);
+    }
+    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+// ---------------------------------------------------------------------------
+// Line kernel (line-integrated scalars, LUT kernel)
+// ---------------------------------------------------------------------------
+// _lin_lut, kernel_function/line_integrated_kernel.jl:13-19, with the
+// q >= q_max cut (:90-94) and the 1/h factor (:132-137).
+template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq) {
+    C q = r * invh;
+    if (q >= C(2)) return C(0);
+    C idxf = q / dq + C(1);
+    int i = (int)idxf;  // q >= 0
+    i = i < 1 ? 1 : (i > LUT_N - 1 ? LUT_N - 1 : i);
+    C t = idxf - C(i);
+    C v = lut[i - 1] * (C(1) - t) + lut[i] * t;
+    return invh * v;
+}
+
+template <class T, int PREC, int ST, int KC, int WHAT>
+__global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
+    using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
+    using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
+    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    CT* lut = (CT*)smem_raw;
+    {
+        for (int i = threadIdx.x; i < LUT_N; i += blockDim.x)
+            lut[i] = (PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i];
+    }
+    __syncthreads();
+    // dq = Q[2] - Q[1] of the 4096-point table = 2/4095 rounded to CT
+    const CT dq = (CT)(2.0 / 4095.0);
+
+    const TreeView<T>& tv = A.tv;
+    const int lane = threadIdx.x & 31;
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tile >= A.src.ntiles) return;
+    const int64_t k = sample_of(A.src, tile, lane);
+    const bool valid = k >= 0;
+    T o[3] = {T(0), T(0), T(0)}, m[3] = {T(0), T(0), T(1)};
+    if (valid) sample_coords(A.src, k, o, m);
+    float of[3] = {(float)o[0], (float)o[1], (float)o[2]};
+    float mf3[3] = {(float)m[0], (float)m[1], (float)m[2]};
+    // float line error near any box: origin rounding + direction rounding x distance
+    // |o|_1 and the particle coordinate scale S (coord_err = 2^-23 S)
+    const float onorm = fabsf(of[0]) + fabsf(of[1]) + fabsf(of[2]);
+    const float S = tv.coord_err / U1;
+    const float el = 4.f * U1 * (onorm + 6.f * S) + 1e-30f;
+    const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
+    unsigned long long n_pairs = 0, n_retest = 0;
+
+    T ha = T(0);
+    if (ST != ST_SCATTER && valid) ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
+    const T ra = X<T>::mul(T(2), ha);
+    const T ra2 = X<T>::mul(ra, ra);
+    float ra2_hi = 0.f, ra2_lo = 0.f;
+    if (BAND && ST != ST_SCATTER) {
+        ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
+        ra2_lo = __double2float_rd((double)ra2) * (1.f - RELM);
+    }
+    CT ia = (ST != ST_SCATTER) ? CT(1) / (CT)ha : CT(0);
+
+    Acc S1, Sw[KC];
+    S1.zero();
+#pragma unroll
+    for (int c = 0; c < KC; ++c) Sw[c].zero();
+    uint64_t hsum = 0;
+    int64_t hcount = 0;
+    const int kc = A.rec.kc;
+
+    int64_t ctile = -1;
+    float cf[3] = {0.f, 0.f, 0.f}, cerr = 0.f;
+
+    auto node_fn = [&](int ni) -> bool {
+        if (BAND) {
+            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
+            float lb = lb_d2_line_box(of, mf3, el, lo, hi);
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+        } else {
+            T d2n = ex_d2_line_box<T>(o, m, tv, ni);
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            return !(d2n > r2);
+        }
+    };
+
+    auto leaf_fn = [&](int64_t li) {
+        CT s;
+        T hb;
+        bool acc;
+        if (BAND) {
+            int64_t t = li >> 5;
+            if (t != ctile) {
+                // perpendicular offset of the tile anchor from the line, in double
+                ctile = t;
+                double q0 = __ldg(&tv.anchor[3 * t]) - (double)o[0];
+                double q1 = __ldg(&tv.anchor[3 * t + 1]) - (double)o[1];
+                double q2 = __ldg(&tv.anchor[3 * t + 2]) - (double)o[2];
+                double t0 = q0 * (double)m[0] + q1 * (double)m[1] + q2 * (double)m[2];
+                double c0 = q0 - t0 * (double)m[0], c1 = q1 - t0 * (double)m[1], c2 = q2 - t0 * (double)m[2];
+                cf[0] = (float)c0; cf[1] = (float)c1; cf[2] = (float)c2;
+                cerr = 1e-15f * (float)(fabs(q0) + fabs(q1) + fabs(q2) + 1.0);
+            }
+            float4 L = __ldg(&tv.leaf4[li]);
+            float v0 = L.x + cf[0], v1 = L.y + cf[1], v2 = L.z + cf[2];
+            float vm = v0 * mf3[0] + v1 * mf3[1] + v2 * mf3[2];
+            float w0 = v0 - vm * mf3[0], w1 = v1 - vm * mf3[1], w2 = v2 - vm * mf3[2];
+            float fs = w0 * w0 + w1 * w1 + w2 * w2;
+            float vn = fabsf(v0) + fabsf(v1) + fabsf(v2);
+            float ev = 8.f * U1 * (vn + fabsf(L.x) + fabsf(L.y) + fabsf(L.z)) + cerr + 1e-30f;
+            float r = sqrtf(fs);
+            float up = r + ev, dn = fmaxf(r - ev, 0.f);
+            float rb2 = 4.f * L.w * L.w;
+            float r2lo, r2hi;
+            if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
+            else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
+            else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
+            // the double reference value differs from the exact one by ~1e-16 |x-o|^2
+            float e64 = 4.5e-16f * (onorm + 6.f * S) * (onorm + 6.f * S);
+            if (up * up * (1.f + RELM) + e64 < r2lo) acc = true;
+            else if (dn * dn * (1.f - RELM) - e64 > r2hi) acc = false;
+            else {
+                ++n_retest;
+                T e2 = ex_d2_line<T>(o, m, tv.x[li], tv.y[li], tv.z[li]);
+                acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
+            }
+            if (!acc) return;
+            s = (CT)fs;
+            hb = (T)L.w;
+        } else {
+            T e2 = ex_d2_line<T>(o, m, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
+            hb = __ldg(&tv.h[li]);
+            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
+            s = (CT)e2;
+        }
+        ++n_pairs;
+        if (WHAT == WHAT_DIGEST) {
+            ++hcount;
+            hsum += mix64((uint64_t)(li + 1));
+            return;
+        }
+        const CT dr = sqrt(s < CT(0) ? CT(0) : s);
+        CT W;
+        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq);
+        else {
+            CT hbc = (CT)hb;
+            CT Wb = line_W<CT>(dr, hbc, CT(1) / hbc, lut, dq);
+            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq) + Wb);
+        }
+        CT mr = (PREC == PREC_FP64) ? (CT)((double)tv.m[li] / (double)tv.rho[li]) : (CT)__ldg(&tv.mrho[li]);
+        const CT w = mr * W;
+        S1.add(w);
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                CT a = (PREC == PREC_FP64) ? (CT)__ldg(&A.colT[c][li]) : (CT)__ldg(&A.colF[c][li]);
+                Sw[c].add(a * w);
+            }
+        }
+    };
+
+    bool ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
+
+    if (valid) {
+        if (WHAT == WHAT_DIGEST) {
+            A.dig_count[k] = hcount;
+            A.dig_hash[k] = hsum;
+            if (A.ha_out) A.ha_out[k] = ha;
+        } else {
+            const double s1 = S1.get();
+            const int L = A.rec.L;
+            if (s1 == 0.0) {
+                for (int q = 0; q < L; ++q) A.out[q][k] = qnan<T>();
+            } else {
+                double sw[MAX_KC];
+#pragma unroll
+                for (int c = 0; c < KC; ++c) sw[c] = Sw[c].get();
+                const double inv = 1.0 / s1;
+                for (int q = 0; q < L; ++q) {
+                    const int a0 = A.rec.a0[q];
+                    A.out[q][k] = (T)(A.rec.a1[q] ? sw[a0] * inv : sw[a0]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) {
+        n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, q);
+        n_retest += __shfl_xor_sync(PSB_FULL, n_retest, q);
+    }
+    if (lane == 0 && A.stats) {
+        atomicAdd(&A.stats[0], n_pairs);
+        atomicAdd(&A.stats[1], n_retest);
+    }
+    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+// ---------------------------------------------------------------------------
+// Sample ordering: Morton codes of sample positions (line origins) in the
+// particle bounding box, clamped, then the stable radix sort.
+// ---------------------------------------------------------------------------
+template <class T>
+__global__ void k_sample_codes(const T* x, const T* y, const T* z, int64_t ns, double3 lo, double3 sc,
+                               uint64_t* codes, uint32_t* idx) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    double v[3] = {(double)x[i], (double)y[i], (double)z[i]};
+    double l[3] = {lo.x, lo.y, lo.z}, s[3] = {sc.x, sc.y, sc.z};
+    uint64_t q[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        double f = (v[d] - l[d]) * s[d];
+        f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
+        q[d] = (uint64_t)f;
+    }
+    codes[i] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+    idx[i] = (uint32_t)i;
+}
+
+}  // namespace psb

@@ -1,0 +1,69 @@
+// launch.hpp -- template dispatch of the interpolation kernels.  The
+// instantiations are split over inst_*.cu so that they compile in parallel.
+#pragma once
+
+#include "interp_kernels.cuh"
+
+namespace psb {
+
+template <class T, int P, int S, int W>
+static void dispatch_points_k(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
+    if constexpr (W != WHAT_INTERP) {
+        k_points<T, P, S, 1, W><<<g, 128, 0, s>>>(a);
+    } else {
+        if (kc <= 1) k_points<T, P, S, 1, W><<<g, 128, 0, s>>>(a);
+        else if (kc <= 2) k_points<T, P, S, 2, W><<<g, 128, 0, s>>>(a);
+        else if (kc <= 4) k_points<T, P, S, 4, W><<<g, 128, 0, s>>>(a);
+        else k_points<T, P, S, 8, W><<<g, 128, 0, s>>>(a);
+    }
+}
+
+template <class T, int P, int W>
+static void dispatch_points_s(const Args<T>& a, int st, int kc, unsigned g, cudaStream_t s) {
+    if (st == ST_GATHER) dispatch_points_k<T, P, ST_GATHER, W>(a, kc, g, s);
+    else if (st == ST_SCATTER) dispatch_points_k<T, P, ST_SCATTER, W>(a, kc, g, s);
+    else dispatch_points_k<T, P, ST_SYMMETRIC, W>(a, kc, g, s);
+}
+
+template <class T, int P>
+static cudaError_t dispatch_points_p(const Args<T>& a, int st, int kc, int what, cudaStream_t s) {
+    unsigned g = (unsigned)((a.src.ntiles + 3) / 4);
+    if (g == 0) return cudaSuccess;
+    if (what == WHAT_INTERP) dispatch_points_s<T, P, WHAT_INTERP>(a, st, kc, g, s);
+    else if (what == WHAT_DENSITY) dispatch_points_s<T, P, WHAT_DENSITY>(a, st, kc, g, s);
+    else dispatch_points_s<T, P, WHAT_DIGEST>(a, st, kc, g, s);
+    return cudaGetLastError();
+}
+
+template <class T, int P, int S, int W>
+static void dispatch_lines_k(const Args<T>& a, int kc, unsigned g, size_t smem, cudaStream_t s) {
+    if constexpr (W != WHAT_INTERP) {
+        k_lines<T, P, S, 1, W><<<g, 128, smem, s>>>(a);
+    } else {
+        if (kc <= 1) k_lines<T, P, S, 1, W><<<g, 128, smem, s>>>(a);
+        else k_lines<T, P, S, 4, W><<<g, 128, smem, s>>>(a);
+    }
+}
+
+template <class T, int P, int W>
+static void dispatch_lines_s(const Args<T>& a, int st, int kc, unsigned g, size_t smem, cudaStream_t s) {
+    if (st == ST_GATHER) dispatch_lines_k<T, P, ST_GATHER, W>(a, kc, g, smem, s);
+    else if (st == ST_SCATTER) dispatch_lines_k<T, P, ST_SCATTER, W>(a, kc, g, smem, s);
+    else dispatch_lines_k<T, P, ST_SYMMETRIC, W>(a, kc, g, smem, s);
+}
+
+template <class T, int P>
+static cudaError_t dispatch_lines_p(const Args<T>& a, int st, int kc, int what, cudaStream_t s) {
+    unsigned g = (unsigned)((a.src.ntiles + 3) / 4);
+    if (g == 0) return cudaSuccess;
+    size_t smem = (size_t)LUT_N * (P == PREC_FP64 ? sizeof(double) : sizeof(float));
+    if (what == WHAT_INTERP) dispatch_lines_s<T, P, WHAT_INTERP>(a, st, kc, g, smem, s);
+    else dispatch_lines_s<T, P, WHAT_DIGEST>(a, st, kc, g, smem, s);
+    return cudaGetLastError();
+}
+
+// defined in inst_*.cu
+template <class T> cudaError_t launch_points(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
+template <class T> cudaError_t launch_lines(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
+
+}  // namespace psb

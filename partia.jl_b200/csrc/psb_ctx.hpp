@@ -1,0 +1,86 @@
+// psb_ctx.hpp -- host-side context of the C ABI (device buffers, stream, errors).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "psb_common.cuh"
+
+struct psb_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    // particles (device, Morton order after a build); element size es
+    int64_t n = 0;
+    psb_dtype dt = PSB_F64;
+    psb_kernel kern = PSB_KERNEL_M4;
+    size_t es = 8;
+    int32_t ncol = 0;
+    void* x = nullptr; void* y = nullptr; void* z = nullptr;
+    void* m = nullptr; void* h = nullptr; void* rho = nullptr;
+    std::vector<void*> cols;
+    void** d_cols = nullptr;
+
+    // LBVH
+    bool built = false;
+    int32_t root = 0;
+    uint64_t* codes = nullptr;
+    int64_t* order = nullptr;
+    int32_t* left = nullptr; int32_t* right = nullptr;
+    int32_t* escape = nullptr; int32_t* parent = nullptr;
+    int32_t* range_lo = nullptr; int32_t* range_hi = nullptr;
+    void* nmin[3] = {nullptr, nullptr, nullptr};
+    void* nmax[3] = {nullptr, nullptr, nullptr};
+    void* nscale = nullptr;
+    float4* node_lo = nullptr; float4* node_hi = nullptr; float4* leaf4 = nullptr;
+    double* anchor = nullptr; float* mrho = nullptr; float* mf = nullptr;
+    float* colsf = nullptr;  // float copies of the columns (double inputs), ncol x n
+    float coord_err = 0.f;
+    double bbox[6] = {0, 0, 0, 0, 0, 0};  // particle min x,y,z, max x,y,z
+
+    unsigned* d_err = nullptr;  // device error word
+    double* lut_d = nullptr;    // M4 line-integrated table (4096, double)
+    float* lut_f = nullptr;     // the same table rounded to float
+
+    // reusable scratch (grown on demand, freed with the context)
+    struct Slot { void* p = nullptr; size_t bytes = 0; };
+    Slot scratch[16];
+
+    cudaEvent_t ev[8] = {};
+};
+
+namespace psb {
+
+// Record an error message on the context and return the code.
+int fail(psb_ctx* c, int code, const std::string& msg);
+// Translate a CUDA error into PSB_ECUDA (or PSB_ENOMEM) with a message.
+int cuda_fail(psb_ctx* c, cudaError_t e, const char* what);
+// Grow-on-demand scratch slot k to at least `bytes`; returns nullptr on failure.
+void* scratch(psb_ctx* c, int k, size_t bytes);
+// Free every particle and tree buffer (not the scratch).
+void free_particles(psb_ctx* c);
+void free_tree(psb_ctx* c);
+
+// build.cu
+int build_lbvh(psb_ctx* c);
+
+// scan.cu helpers used by the build and the interpolation drivers
+cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, psb_ctx* c, int slot_base);
+cudaError_t inclusive_max_scan_i64(int64_t* data, int64_t n, psb_ctx* c, int slot_base);
+// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of key.
+// Results end in keys/vals (the alternates are scratch).
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches);
+
+template <class T> TreeView<T> tree_view(psb_ctx* c);
+
+}  // namespace psb
+
+#define PSB_CUDA_TRY(ctx, call, what)                         \
+    do {                                                      \
+        cudaError_t _e = (call);                              \
+        if (_e != cudaSuccess) return psb::cuda_fail(ctx, _e, what); \
+    } while (0)

@@ -1,0 +1,258 @@
+"""GPU parity: the CUDA library against the CPU oracle on identical inputs.
+
+Bit-exact: Morton codes, permutation, tree topology, node boxes and scales,
+per-sample neighbour sets (count + order-independent hash) and the nearest-h
+choice.  Floating-point fields: PSB_PREC_FP64 within 1e-12 and PSB_PREC_FP32C
+within 2e-6 of each field's max |value| (NaN masks identical).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+if not has_gpu():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+from partia_b200 import _lib as L  # noqa: E402
+from partia_b200.engine import CatalogC, Context  # noqa: E402
+
+FP64_TOL = 1e-12
+FP32C_TOL = 2e-6
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb), "NaN masks differ"
+    fin = ~na
+    if not fin.any():
+        return 0.0
+    scale = np.max(np.abs(b[fin]))
+    if scale == 0:
+        return float(np.max(np.abs(a[fin])))
+    return float(np.max(np.abs(a[fin] - b[fin])) / scale)
+
+
+def make_particles(n, seed, dtype=np.float64, hscale=1.2, ncolx=0):
+    rng = np.random.default_rng(seed)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    m = rng.uniform(0.5, 1.5, n) / n
+    h = hscale * (1.0 / n) ** (1 / 3) * rng.uniform(0.5, 2.0, n)
+    rho = rng.uniform(0.5, 2.0, n)
+    cols = [rho.copy(), np.sin(3 * x) + y, -y + 0.1 * rng.standard_normal(n), x + 0.1 * rng.standard_normal(n),
+            0.1 * z + 0.05 * rng.standard_normal(n)]
+    for k in range(ncolx):
+        cols.append(rng.standard_normal(n))
+    arrs = [a.astype(dtype) for a in (x, y, z, m, h, rho)]
+    return arrs, [c.astype(dtype) for c in cols]
+
+
+def pair(arrs, cols, dtype=np.float64):
+    orc = O.Oracle(*arrs, cols=cols, dtype=dtype)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols, dtype=dtype)
+    perm, codes = ctx.build(want_perm=True, want_codes=True)
+    return orc, ctx, perm, codes
+
+
+@pytest.mark.parametrize("n,seed,dtype", [(1, 0, np.float64), (2, 1, np.float64), (7, 2, np.float64),
+                                          (33, 3, np.float64), (1000, 4, np.float64), (50_000, 5, np.float64),
+                                          (20_000, 6, np.float32)])
+def test_build_bit_exact(n, seed, dtype):
+    arrs, cols = make_particles(n, seed, dtype)
+    orc, ctx, perm, codes = pair(arrs, cols, dtype)
+    assert np.array_equal(perm, orc.perm)
+    assert np.array_equal(codes, orc.codes)
+    to, tg = orc.tree(), ctx.tree()
+    assert to["root"] == tg["root"]
+    for k in ("left", "right", "escape", "parent"):
+        assert np.array_equal(to[k], tg[k]), k
+    for k in ("node_min", "node_max", "node_scale"):
+        assert np.array_equal(to[k], tg[k]), k
+
+
+def test_build_duplicates_and_degenerate_axes():
+    # identical codes (test/neighbor_search_tests.jl:236-247) and a flat axis
+    n = 64
+    rng = np.random.default_rng(11)
+    x = np.repeat(rng.random(8), 8)
+    y = np.full(n, 0.25)
+    z = np.repeat(rng.random(8), 8)
+    arrs = [x, y, z, np.full(n, 1.0 / n), np.full(n, 0.05), np.ones(n)]
+    orc, ctx, perm, codes = pair(arrs, [np.ones(n)])
+    assert np.array_equal(perm, orc.perm) and np.array_equal(codes, orc.codes)
+    assert np.all(np.diff(codes.astype(np.float64)) > 0)
+    to, tg = orc.tree(), ctx.tree()
+    for k in ("left", "right", "escape", "parent", "node_min", "node_max", "node_scale"):
+        assert np.array_equal(to[k], tg[k]), k
+
+
+def _samples(n, seed, lo=-0.05, hi=1.05):
+    rng = np.random.default_rng(seed)
+    return tuple(rng.uniform(lo, hi, n) for _ in range(3))
+
+
+@pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])
+@pytest.mark.parametrize("hmode", [O.H_NEAREST, O.H_PER_SAMPLE])
+def test_point_neighbour_sets(strategy, hmode):
+    arrs, cols = make_particles(30_000, 21)
+    orc, ctx, _, _ = pair(arrs, cols)
+    s = _samples(4000, 22)
+    hs = np.random.default_rng(23).uniform(0.01, 0.04, 4000) if hmode == O.H_PER_SAMPLE else None
+    co, ho, hao = orc.digest(s, strategy=strategy, hmode=hmode, hs=hs)
+    for fp32c in (False, True):
+        cg, hg, hag = ctx.digest(s, strategy=strategy, hmode=hmode, hs=hs, fp32c=fp32c)
+        assert np.array_equal(cg, co)
+        assert np.array_equal(hg, ho)
+        if strategy != O.SCATTER:
+            assert np.array_equal(hag, hao)
+    assert co.mean() > 10
+
+
+def test_nearest_h_matches_brute_force():
+    arrs, cols = make_particles(20_000, 31)
+    orc, ctx, _, _ = pair(arrs, cols)
+    s = _samples(3000, 32)
+    _, _, ha = ctx.digest(s, strategy=O.GATHER, hmode=O.H_NEAREST, fp32c=True)
+    idx = orc.brute_nearest(*s)
+    h_sorted = arrs[4][orc.perm]
+    assert np.array_equal(ha, h_sorted[idx])
+
+
+CATALOGS = {
+    "c1": dict(scalars=[0, 1], shepard=[0, 1]),
+    "c2": dict(scalars=[0], shepard=[0], grads=[0], divs=[2, 3, 4], curls=[2, 3, 4]),
+    "all": dict(scalars=[0, 1, 4], shepard=[0, 1, 1], grads=[-1, 1], divs=[2, 3, 4], curls=[4, 3, 2]),
+}
+
+
+@pytest.mark.parametrize("catname", list(CATALOGS))
+@pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])
+def test_point_fields(catname, strategy):
+    arrs, cols = make_particles(30_000, 41)
+    orc, ctx, _, _ = pair(arrs, cols)
+    s = _samples(5000, 42)
+    spec = CATALOGS[catname]
+    ocat = O.Catalog(**spec)
+    gcat = CatalogC(**spec)
+    ref = orc.interp_points(*s, ocat, strategy=strategy, hmode=O.H_NEAREST)
+    g64 = ctx.interp_points(*s, gcat, strategy=strategy, hmode=L.PSB_H_NEAREST, prec=L.PSB_PREC_FP64)
+    g32 = ctx.interp_points(*s, gcat, strategy=strategy, hmode=L.PSB_H_NEAREST, prec=L.PSB_PREC_FP32C)
+    for k in range(ocat.L):
+        assert rel_err(g64[k], ref[k]) <= FP64_TOL, (k, rel_err(g64[k], ref[k]))
+        assert rel_err(g32[k], ref[k]) <= FP32C_TOL, (k, rel_err(g32[k], ref[k]))
+
+
+def test_point_fields_float32_inputs():
+    arrs, cols = make_particles(20_000, 51, dtype=np.float32)
+    orc, ctx, _, _ = pair(arrs, cols, np.float32)
+    s = tuple(a.astype(np.float32) for a in _samples(3000, 52))
+    spec = CATALOGS["c2"]
+    ref = orc.interp_points(*s, O.Catalog(**spec), strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    co, ho, _ = orc.digest(s, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    cg, hg, _ = ctx.digest(s, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST)
+    assert np.array_equal(cg, co) and np.array_equal(hg, ho)
+    for prec in (L.PSB_PREC_FP64, L.PSB_PREC_FP32C):
+        g = ctx.interp_points(*s, CatalogC(**spec), strategy=L.PSB_SYMMETRIC, prec=prec)
+        for k in range(len(ref)):
+            # the reference accumulates in float32: compare at float32 accuracy
+            assert rel_err(g[k], ref[k]) <= 2e-4, (prec, k)
+
+
+def test_empty_neighbourhood_gives_nan_and_zero_density():
+    arrs, cols = make_particles(2000, 61)
+    orc, ctx, _, _ = pair(arrs, cols)
+    s = (np.array([5.0, 0.5]), np.array([5.0, 0.5]), np.array([5.0, 0.5]))
+    spec = CATALOGS["all"]
+    g = ctx.interp_points(*s, CatalogC(**spec), strategy=L.PSB_SCATTER)
+    r = orc.interp_points(*s, O.Catalog(**spec), strategy=O.SCATTER)
+    for k in range(len(r)):
+        assert np.isnan(g[k][0]) and np.isnan(r[k][0])
+        assert np.isfinite(g[k][1])
+    d = ctx.density(*s, strategy=L.PSB_SCATTER)
+    assert d[0] == 0.0 and d[1] > 0
+
+
+@pytest.mark.parametrize("strategy,hmode", [(O.SCATTER, O.H_PER_SAMPLE), (O.GATHER, O.H_PER_SAMPLE),
+                                            (O.SYMMETRIC, O.H_CONSTANT)])
+def test_line_neighbour_sets_and_fields(strategy, hmode):
+    arrs, cols = make_particles(30_000, 71)
+    orc, ctx, _, _ = pair(arrs, cols)
+    rng = np.random.default_rng(72)
+    nl = 3000
+    o = tuple(rng.uniform(-0.2, 1.2, nl) for _ in range(3))
+    d = rng.standard_normal((3, nl))
+    d /= np.linalg.norm(d, axis=0)
+    d = tuple(d)
+    hs = rng.uniform(0.01, 0.03, nl) if hmode == O.H_PER_SAMPLE else np.array([0.02])
+    co, ho, _ = orc.digest(o, d, strategy=strategy, hmode=hmode, hs=hs)
+    for fp32c in (False, True):
+        cg, hg, _ = ctx.digest(o, d, strategy=strategy, hmode=hmode, hs=hs, fp32c=fp32c)
+        assert np.array_equal(cg, co)
+        assert np.array_equal(hg, ho)
+    ref = orc.interp_lines(o, d, scalars=[0, 1], shepard=[0, 1], strategy=strategy, hmode=hmode, hs=hs)
+    cat = CatalogC(scalars=[0, 1], shepard=[0, 1])
+    for prec, tol in ((L.PSB_PREC_FP64, FP64_TOL), (L.PSB_PREC_FP32C, FP32C_TOL)):
+        g = ctx.interp_lines(o, d, cat, strategy=strategy, hmode=hmode, hs=hs, prec=prec)
+        for k in range(2):
+            assert rel_err(g[k], ref[k]) <= tol, (prec, k, rel_err(g[k], ref[k]))
+
+
+def test_grid_box_beam_match_explicit_samples():
+    from partia_b200 import workloads as W
+    arrs, cols = make_particles(20_000, 81)
+    _, ctx, _, _ = pair(arrs, cols)
+    cat = CatalogC(**CATALOGS["c2"])
+    ax = np.linspace(0.0, 1.0, 13)
+    ay = np.linspace(0.1, 0.9, 10)
+    az = np.linspace(0.2, 0.8, 7)
+    g = ctx.interp_grid(ax, ay, az, cat, strategy=L.PSB_SYMMETRIC)
+    X, Y, Z = np.meshgrid(ax, ay, az, indexing="ij")
+    p = ctx.interp_points(X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F"), cat, strategy=L.PSB_SYMMETRIC)
+    for a, b in zip(g, p):
+        assert np.array_equal(a, b, equal_nan=True)
+    fr = W.Frame((0.5, 0.5, 0.5), (0.3, -0.2, 1.0), (1.0, 0.0, -0.3))
+    fr.rotate(0.3, -0.2, 0.5)
+    farr = fr.as_array()
+    prm = np.array([-0.3, 0.3, -0.2, 0.25, -0.1, 0.1])
+    gb = ctx.interp_box(farr, prm, 9, 8, 5, cat, strategy=L.PSB_SYMMETRIC)
+    bx = W.box_coordinates(farr, (-0.3, 0.3, 9), (-0.2, 0.25, 8), (-0.1, 0.1, 5))
+    pb = ctx.interp_points(*bx, cat, strategy=L.PSB_SYMMETRIC)
+    for a, b in zip(gb, pb):
+        assert np.array_equal(a, b, equal_nan=True)
+    lcat = CatalogC(scalars=[0, 1], shepard=[0, 1])
+    gl = ctx.interp_beam(farr, prm[:4], 11, 6, lcat)
+    ox = W.plane_coordinates(farr, (-0.3, 0.3, 11), (-0.2, 0.25, 6))
+    fw = tuple(np.full(66, farr[9 + c]) for c in range(3))
+    pl = ctx.interp_lines(ox, fw, lcat)
+    for a, b in zip(gl, pl):
+        assert np.array_equal(a, b, equal_nan=True)
+
+
+def test_error_paths():
+    ctx = Context(0)
+    cat = CatalogC(scalars=[0])
+    x = np.zeros(3)
+    with pytest.raises(L.PsbError) as e:
+        ctx.interp_points(x, x, x, cat)
+    assert e.value.code == L.PSB_ESTATE
+    arrs, cols = make_particles(100, 91)
+    arrs[0][5] = np.nan
+    ctx.set_particles(*arrs, cols=cols)
+    with pytest.raises(L.PsbError) as e:
+        ctx.build()
+    assert e.value.code == L.PSB_EINVAL
+    arrs, cols = make_particles(100, 92)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build()
+    with pytest.raises(L.PsbError) as e:
+        ctx.interp_lines((x, x, x), (x, x, x + 1), cat, strategy=L.PSB_GATHER, hmode=L.PSB_H_NEAREST)
+    assert e.value.code == L.PSB_EINVAL
+    with pytest.raises(L.PsbError) as e:
+        ctx.interp_points(x, x, x, CatalogC(scalars=[99]))
+    assert e.value.code == L.PSB_EINVAL

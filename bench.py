@@ -204,9 +204,9 @@ def main():
     ctx.build(want_perm=False)
     cat = CatalogC(**CATALOG)
 
-    # this rank's slab of z-planes
-    z0 = (NGRID * rank) // world
-    z1 = (NGRID * (rank + 1)) // world
+    # this rank's slab of z-planes (samples shard; particles and LBVH are replicated)
+    from partia_b200.sharding import grid_slab
+    (z0, z1), _ = grid_slab(NGRID, NGRID, NGRID, rank, world)
     az = axis[z0:z1]
     ns = NGRID * NGRID * len(az)
     outs = [torch.empty(ns, dtype=torch.float64, device=dev) for _ in range(L_OUT)]
@@ -242,6 +242,7 @@ def main():
     with ClockSampler(local) as clk:
         tot32, steps32, kern32, pairs = timed(L.PSB_PREC_FP32C, args.steps, args.warmup)
     launches_per_step = ctx.last_stats.launches
+    ctx_steps = ctx.last_stats.warp_steps
     tot = torch.tensor([tot32], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(tot, op=dist.ReduceOp.MAX)
@@ -254,6 +255,7 @@ def main():
     if not args.no_fp64:
         tot64, _, kern64, _ = timed(L.PSB_PREC_FP64, max(2, args.steps // 2), 1)
         v64 = ns * max(2, args.steps // 2) / (tot64 / 1e3)
+        step(L.PSB_PREC_FP32C)
         o32 = [o.clone() for o in outs]
         step(L.PSB_PREC_FP64)
         errs = {}
@@ -325,7 +327,8 @@ def main():
                          "peak_kind": peak_kind,
                          "traffic": (tr or {}).get("bytes_per_launch") if tr else None,
                          "kernel": "k_points<double,FP32C,SYMMETRIC,4,INTERP>", "kernel_ms": kern_ms,
-                         "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg)},
+                         "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg),
+                         "warp_steps_per_launch": int(ctx_steps)},
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs, "grad_fwd_time_ratio": None,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -57,7 +57,7 @@ typedef enum {
 
 typedef enum { PSB_F64 = 0, PSB_F32 = 1 } psb_dtype;
 
-/* SPH kernel families of src/julia/KernelInterpolation/kernel_function/kernels/*.jl.
+/* SPH kernel families of src/julia/KernelInterpolation/kernel_function/kernels/ (one file each).
  * This build evaluates PSB_KERNEL_M4 (M4_spline.jl); the others return
  * PSB_EUNSUPPORTED. */
 typedef enum {
@@ -125,6 +125,10 @@ typedef struct {
     double d2h_ms;         /* device -> host copies inside the call              */
     int64_t pairs;         /* accepted (sample, particle) pairs                  */
     int64_t exact_retests; /* FP32C pairs re-decided in double near the support  */
+    int64_t warp_steps;    /* tree-walk steps summed over warps                  */
+    int64_t spans;         /* leaf spans processed (summed over warps)           */
+    int64_t span_tests;    /* (span, sample) pairs tested                        */
+    int64_t body_iters;    /* pair-body loop iterations summed over warps        */
     int32_t launches;      /* kernels launched by the call                       */
     int32_t reserved;
 } psb_stats;

@@ -252,6 +252,13 @@ __global__ void k_refit_check(const unsigned* visited, int64_t nint, unsigned* e
     if (t < nint && visited[t] != 2u) atomicOr(err, PSB_DERR_REFIT);
 }
 
+// (left, escape, range_lo, range_hi) of every internal node in one 16-byte record
+__global__ void k_pack_links(int64_t nint, const int32_t* left, const int32_t* escape, const int32_t* rlo,
+                             const int32_t* rhi, int4* links) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nint) links[t] = make_int4(left[t], escape[t], rlo[t], rhi[t]);
+}
+
 // ---- float traversal records ---------------------------------------------------------
 template <class T>
 __global__ void k_pack_nodes(int64_t nint, const T* mnx, const T* mny, const T* mnz, const T* mxx, const T* mxy,
@@ -391,6 +398,8 @@ static int build_typed(psb_ctx* c) {
 
     // float traversal records
     const int64_t ntile = (n + 31) / 32;
+    PSB_CUDA_TRY(c, cudaMalloc(&c->links, sizeof(int4) * nalloc), "cudaMalloc links");
+    if (nint > 0) k_pack_links<<<grid_for(nint), BT, 0, s>>>(nint, c->left, c->escape, c->range_lo, c->range_hi, c->links);
     PSB_CUDA_TRY(c, cudaMalloc(&c->node_lo, sizeof(float4) * nalloc), "cudaMalloc node_lo");
     PSB_CUDA_TRY(c, cudaMalloc(&c->node_hi, sizeof(float4) * nalloc), "cudaMalloc node_hi");
     PSB_CUDA_TRY(c, cudaMalloc(&c->leaf4, sizeof(float4) * n), "cudaMalloc leaf4");

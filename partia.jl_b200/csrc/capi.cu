@@ -50,7 +50,7 @@ template <class P> static void dfree_t(P*& p) {
 void free_tree(psb_ctx* c) {
     dfree_t(c->codes); dfree_t(c->order);
     dfree_t(c->left); dfree_t(c->right); dfree_t(c->escape); dfree_t(c->parent);
-    dfree_t(c->range_lo); dfree_t(c->range_hi);
+    dfree_t(c->range_lo); dfree_t(c->range_hi); dfree_t(c->links);
     for (int d = 0; d < 3; ++d) { dfree(c->nmin[d]); dfree(c->nmax[d]); }
     dfree(c->nscale);
     dfree_t(c->node_lo); dfree_t(c->node_hi); dfree_t(c->leaf4);

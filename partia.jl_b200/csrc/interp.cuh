@@ -108,12 +108,14 @@ template <class T> __device__ __forceinline__ void sample_coords(const SampleSrc
 // The fast path evaluates f and f' together from q = r / h.
 // ---------------------------------------------------------------------------
 template <class C> __device__ __forceinline__ void m4_fdf(C q, C& f, C& df) {
-    C a = C(2) - q, b = C(1) - q;
-    C a2 = a * a, b2 = b * b;
+    // inner piece expanded to avoid cancellation at small q:
+    //   1/4 (2-q)^3 - (1-q)^3 = 1 + q^2 (3/4 q - 3/2),  its derivative q (9/4 q - 3)
+    C a = C(2) - q;
+    C a2 = a * a;
     C fo = C(0.25) * a2 * a;      // 1 <= q < 2
     C dfo = C(-0.75) * a2;
-    C fi = fo - b2 * b;           // 0 <= q < 1
-    C dfi = dfo + C(3) * b2;
+    C fi = C(1) + q * q * (C(0.75) * q - C(1.5));
+    C dfi = q * (C(2.25) * q - C(3));
     f = (q < C(1)) ? fi : ((q < C(2)) ? fo : C(0));
     df = (q < C(1)) ? dfi : ((q < C(2)) ? dfo : C(0));
 }
@@ -191,6 +193,66 @@ __device__ __forceinline__ bool warp_traverse(int32_t start, int64_t n, const in
         if (__all_sync(PSB_FULL, resume == 0)) break;
     }
     return true;
+}
+
+// ---------------------------------------------------------------------------
+// Warp-cooperative stackless DFS with leaf spans.  Same walk as
+// warp_traverse, but an internal node whose subtree holds at most SPAN leaves
+// (a contiguous Morton range [range_lo, range_hi]) is handed to span_fn as a
+// whole instead of being descended, and the walk continues at its escape.
+// links[ni] = (left, escape, range_lo, range_hi) of internal node ni (1-based
+// ids / leaf indices), one 16-byte load per step.  span_fn(lo, cnt, part)
+// receives the 0-based first leaf, the leaf count and whether this lane takes
+// part; it is called by all 32 lanes (it may use warp-synchronous code).
+// For point queries this visits, for every lane, exactly the leaves whose
+// inclusion test can succeed: point-box distances are monotone in every
+// rounding (a box distance never exceeds the distance to a point inside it),
+// so skipping the pruning tests inside a span cannot add or lose a neighbour,
+// and leaves are still visited in increasing index (DFS) order.
+// ---------------------------------------------------------------------------
+constexpr int SPAN = 32;
+
+template <class NodeFn, class SpanFn>
+__device__ __forceinline__ bool warp_traverse_spans(int32_t start, int64_t n, const int4* __restrict__ links,
+                                                    const int32_t* __restrict__ escape, bool lane_valid,
+                                                    NodeFn node_fn, SpanFn span_fn, int64_t& steps) {
+    int32_t node = start;
+    int32_t resume = lane_valid ? -1 : 0;
+    const int64_t bound = steps + 4 * n + 8;
+    const int64_t maxid = 2 * n - 1;
+    bool ok = true;
+    while (node != 0) {
+        if (++steps > bound || node < 0 || (int64_t)node > maxid) { ok = false; break; }
+        if (resume == node) resume = -1;
+        const bool active = (resume == -1);
+        if (node >= n) {  // a leaf reached directly: a span of one
+            const int32_t esc = __ldg(&escape[node - 1]);
+            span_fn((int64_t)node - n, 1, active);
+            node = esc;
+        } else {
+            const int32_t ni = node - 1;
+            const int4 lk = __ldg(&links[ni]);
+            bool want = false;
+            if (active) {
+                if (node_fn(ni)) want = true;
+                else resume = lk.y;
+            }
+            if (!__any_sync(PSB_FULL, want)) {
+                node = lk.y;
+            } else {
+                const int cnt = lk.w - lk.z + 1;
+                if (cnt <= SPAN) {
+                    span_fn((int64_t)lk.z - 1, cnt, want);
+                    if (want) resume = lk.y;
+                    node = lk.y;
+                } else {
+                    node = lk.x;
+                }
+            }
+        }
+        if (__all_sync(PSB_FULL, resume == 0)) break;
+    }
+    return ok;
 }
 
 }  // namespace psb

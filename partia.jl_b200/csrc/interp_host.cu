@@ -15,6 +15,13 @@ template <class T> TreeView<T> tree_view(psb_ctx* c) {
     v.escape = c->escape;
     v.range_lo = c->range_lo;
     v.range_hi = c->range_hi;
+    v.links = c->links;
+    v.codes = c->codes;
+    for (int d = 0; d < 3; ++d) {
+        v.qlo[d] = c->bbox[d];
+        double ext = c->bbox[3 + d] - c->bbox[d];
+        v.qscale[d] = ext > 0 ? 2097151.0 / ext : 0.0;
+    }
     for (int d = 0; d < 3; ++d) { v.nmin[d] = (const T*)c->nmin[d]; v.nmax[d] = (const T*)c->nmax[d]; }
     v.nscale = (const T*)c->nscale;
     v.x = (const T*)c->x; v.y = (const T*)c->y; v.z = (const T*)c->z;
@@ -218,9 +225,9 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
             for (int q = 0; q < L; ++q) A.out[q] = (T*)(obuf + es * ns * q);
         }
     }
-    unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 2 * sizeof(unsigned long long));
+    unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 8 * sizeof(unsigned long long));
     if (!dstats) return fail(c, PSB_ENOMEM, "scratch allocation failed (stats)");
-    PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 2 * sizeof(unsigned long long), s), "memset stats");
+    PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), s), "memset stats");
     A.stats = dstats;
 
     // ---- launch ----
@@ -244,7 +251,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
         }
     }
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[4], s), "event");
-    unsigned long long hst[2] = {0, 0};
+    unsigned long long hst[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned herr = 0;
     PSB_CUDA_TRY(c, cudaMemcpyAsync(hst, dstats, sizeof(hst), cudaMemcpyDeviceToHost, s), "stats D2H");
     PSB_CUDA_TRY(c, cudaMemcpyAsync(&herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, s), "error D2H");
@@ -263,6 +270,10 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
         stats->total_ms = ms_between(c->ev[0], c->ev[4]);
         stats->pairs = (int64_t)hst[0];
         stats->exact_retests = (int64_t)hst[1];
+        stats->warp_steps = (int64_t)hst[2];
+        stats->spans = (int64_t)hst[3];
+        stats->span_tests = (int64_t)hst[4];
+        stats->body_iters = (int64_t)hst[5];
         stats->launches = launches;
     }
     return PSB_OK;

@@ -39,7 +39,7 @@ template <class T> struct Args {
     const double* lut_d;
     const float* lut_f;
     unsigned* err;
-    unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests
+    unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests, [2] traversal steps
 };
 
 // ---------------------------------------------------------------------------
@@ -184,287 +184,6 @@ __device__ __forceinline__ float lb_d2_line_box(const float o[3], const float m[
 }
 
 // ---------------------------------------------------------------------------
-// Point kernel
-// ---------------------------------------------------------------------------
-template <class T, int PREC, int ST, int KC, int WHAT>
-__global__ void __launch_bounds__(128) k_points(const Args<T> A) {
-    using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
-    using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
-    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
-    const TreeView<T>& tv = A.tv;
-    const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile >= A.src.ntiles) return;  // warp-uniform
-
-    const int64_t k = sample_of(A.src, tile, lane);
-    const bool valid = k >= 0;
-    T p[3] = {T(0), T(0), T(0)}, dd[3];
-    if (valid) sample_coords(A.src, k, p, dd);
-    float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
-    const float pem = U1 * fmaxf(fmaxf(fabsf(pf[0]), fabsf(pf[1])), fabsf(pf[2])) + 1e-30f;
-    const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
-    unsigned long long n_pairs = 0, n_retest = 0;
-    bool ok = true;
-
-    // ---- sample smoothing length (LBVH_find_nearest_h or given) ----
-    T ha = T(0);
-    if (ST != ST_SCATTER) {
-        if (A.hmode == PSB_H_NEAREST) {
-            if (BAND) {
-                double best = INFINITY;
-                int64_t bidx = -1;
-                int64_t ctile = -1;
-                float prel[3] = {0.f, 0.f, 0.f}, ep = 0.f;
-                ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid,
-                    [&](int ni) {
-                        float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
-                        return !((double)lb > best);
-                    },
-                    [&](int64_t li) {
-                        int64_t t = li >> 5;
-                        if (t != ctile) {
-                            ctile = t;
-                            double q0 = (double)p[0] - __ldg(&tv.anchor[3 * t]);
-                            double q1 = (double)p[1] - __ldg(&tv.anchor[3 * t + 1]);
-                            double q2 = (double)p[2] - __ldg(&tv.anchor[3 * t + 2]);
-                            prel[0] = (float)q0; prel[1] = (float)q1; prel[2] = (float)q2;
-                            ep = U1 * fmaxf(fmaxf(fabsf(prel[0]), fabsf(prel[1])), fabsf(prel[2]));
-                        }
-                        float4 L = __ldg(&tv.leaf4[li]);
-                        float dx = prel[0] - L.x, dy = prel[1] - L.y, dz = prel[2] - L.z;
-                        float r = sqrtf(dx * dx + dy * dy + dz * dz);
-                        float e = 1.7320508f * (ep + U1 * fmaxf(fmaxf(fabsf(L.x), fabsf(L.y)), fabsf(L.z))) + 4.f * U1 * r + 1e-30f;
-                        float lo_r = fmaxf(r - e, 0.f);
-                        if ((double)(lo_r * lo_r * (1.f - RELM)) > best) return;
-                        double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                        if (d2 <= best && d2 < best) { best = d2; bidx = li; }
-                    });
-                if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
-            } else {
-                T best = (T)INFINITY;
-                int64_t bidx = -1;
-                ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid,
-                    [&](int ni) { return !(ex_d2_pbox<T>(p, tv, ni) > best); },
-                    [&](int64_t li) {
-                        T d2 = ex_d2_pp<T>(p, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
-                        if (d2 <= best && d2 < best) { best = d2; bidx = li; }
-                    });
-                if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
-            }
-        } else if (valid) {
-            ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
-        }
-    }
-    // radius = Kvalid * ha; radius2 = radius * radius (general_interpolation.jl:20-21)
-    const T ra = X<T>::mul(T(2), ha);
-    const T ra2 = X<T>::mul(ra, ra);
-    float ra2_hi = 0.f, ra2_lo = 0.f;
-    if (BAND && ST != ST_SCATTER) {
-        ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
-        ra2_lo = __double2float_rd((double)ra2) * (1.f - RELM);
-    }
-
-    // ---- per-sample constants of the kernel weights ----
-    const CT sig = inv_pi<CT>();
-    CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
-    if (ST != ST_SCATTER) {
-        ia = CT(1) / (CT)ha;
-        sa3 = sig * ia * ia * ia;
-        sa4 = sa3 * ia;
-    }
-
-    // ---- accumulators ----
-    Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
-    CT dens = CT(0);
-    S1.zero(); Dm.zero();
-#pragma unroll
-    for (int d = 0; d < 3; ++d) { G[d].zero(); Dg[d].zero(); }
-#pragma unroll
-    for (int c = 0; c < KC; ++c) {
-        Sw[c].zero();
-#pragma unroll
-        for (int d = 0; d < 3; ++d) Sg[c][d].zero();
-    }
-    uint64_t hsum = 0;
-    int64_t hcount = 0;
-    const int kc = A.rec.kc;
-    const bool need_dg = A.rec.need_dg != 0;
-
-    int64_t ctile = -1;
-    float prel[3] = {0.f, 0.f, 0.f}, ep = 0.f;
-
-    auto node_fn = [&](int ni) -> bool {
-        if (BAND) {
-            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
-            float lb = lb_d2_pbox(pf, pem, lo, hi);
-            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
-        } else {
-            T d2n = ex_d2_pbox<T>(p, tv, ni);
-            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
-            return !(d2n > r2);
-        }
-    };
-
-    auto leaf_fn = [&](int64_t li) {
-        CT dx, dy, dz, d2;
-        T hb = T(0);
-        bool acc;
-        if (BAND) {
-            int64_t t = li >> 5;
-            if (t != ctile) {
-                ctile = t;
-                double q0 = (double)p[0] - __ldg(&tv.anchor[3 * t]);
-                double q1 = (double)p[1] - __ldg(&tv.anchor[3 * t + 1]);
-                double q2 = (double)p[2] - __ldg(&tv.anchor[3 * t + 2]);
-                prel[0] = (float)q0; prel[1] = (float)q1; prel[2] = (float)q2;
-                ep = U1 * fmaxf(fmaxf(fabsf(prel[0]), fabsf(prel[1])), fabsf(prel[2]));
-            }
-            float4 L = __ldg(&tv.leaf4[li]);
-            float fx = prel[0] - L.x, fy = prel[1] - L.y, fz = prel[2] - L.z;
-            float fd2 = fx * fx + fy * fy + fz * fz;
-            float r = sqrtf(fd2);
-            float e = 1.7320508f * (ep + U1 * fmaxf(fmaxf(fabsf(L.x), fabsf(L.y)), fabsf(L.z))) + 4.f * U1 * r + 1e-30f;
-            float rb2 = 4.f * L.w * L.w;
-            float r2lo, r2hi;
-            if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
-            else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
-            else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
-            float up = r + e, dn = fmaxf(r - e, 0.f);
-            if (up * up * (1.f + RELM) < r2lo) acc = true;
-            else if (dn * dn * (1.f - RELM) > r2hi) acc = false;
-            else {
-                ++n_retest;
-                T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
-            }
-            if (!acc) return;
-            dx = (CT)fx; dy = (CT)fy; dz = (CT)fz; d2 = (CT)fd2;
-            hb = (T)L.w;
-        } else {
-            T xb = __ldg(&tv.x[li]), yb = __ldg(&tv.y[li]), zb = __ldg(&tv.z[li]);
-            T e2 = ex_d2_pp<T>(p, xb, yb, zb);
-            hb = __ldg(&tv.h[li]);
-            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
-            dx = (CT)(p[0] - xb); dy = (CT)(p[1] - yb); dz = (CT)(p[2] - zb);
-            d2 = (CT)e2;
-        }
-        ++n_pairs;
-        if (WHAT == WHAT_DIGEST) {
-            ++hcount;
-            hsum += mix64((uint64_t)(li + 1));
-            return;
-        }
-        const CT r = sqrt(d2);
-        const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
-        CT Wsum, csum;  // kernel value and gradient coefficient (g = c * delta)
-        if (ST != ST_SCATTER) {
-            CT f, df;
-            m4_fdf<CT>(r * ia, f, df);
-            Wsum = sa3 * f;
-            csum = sa4 * df * invr;
-        }
-        if (ST != ST_GATHER) {
-            CT ib = CT(1) / (CT)hb;
-            CT sb3 = sig * ib * ib * ib;
-            CT f, df;
-            m4_fdf<CT>(r * ib, f, df);
-            CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
-            if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
-            else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
-        }
-        if (WHAT == WHAT_DENSITY) {
-            dens += (CT)tv.m[li] * Wsum;
-            return;
-        }
-        CT mr = (PREC == PREC_FP64) ? (CT)((double)tv.m[li] / (double)tv.rho[li]) : (CT)__ldg(&tv.mrho[li]);
-        const CT w = mr * Wsum;
-        const CT gc = mr * csum;
-        const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
-        S1.add(w);
-        G[0].add(gx); G[1].add(gy); G[2].add(gz);
-#pragma unroll
-        for (int c = 0; c < KC; ++c) {
-            if (c < kc) {
-                CT a = (PREC == PREC_FP64) ? (CT)__ldg(&A.colT[c][li]) : (CT)__ldg(&A.colF[c][li]);
-                Sw[c].add(a * w);
-                Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
-            }
-        }
-        if (need_dg) {
-            CT mb = (PREC == PREC_FP64) ? (CT)tv.m[li] : (CT)__ldg(&tv.mf[li]);
-            Dm.add(mb * Wsum);
-            CT mc = mb * csum;
-            Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
-        }
-    };
-
-    bool ok2 = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
-    ok = ok && ok2;
-
-    // ---- outputs ----
-    if (valid) {
-        if (WHAT == WHAT_DIGEST) {
-            A.dig_count[k] = hcount;
-            A.dig_hash[k] = hsum;
-            if (A.ha_out) A.ha_out[k] = ha;
-        } else if (WHAT == WHAT_DENSITY) {
-            A.out[0][k] = (T)dens;
-        } else {
-            const double s1 = S1.get();
-            const int L = A.rec.L;
-            if (s1 == 0.0) {
-                for (int o = 0; o < L; ++o) A.out[o][k] = qnan<T>();
-            } else {
-                double sw[MAX_KC], sg[MAX_KC][3];
-#pragma unroll
-                for (int c = 0; c < KC; ++c) {
-                    sw[c] = Sw[c].get();
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
-                }
-                const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
-                const double inv = 1.0 / s1;
-                for (int o = 0; o < L; ++o) {
-                    const int op = A.rec.op[o];
-                    const int a0 = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
-                    double v;
-                    if (op == OP_SCALAR) {
-                        v = a1 ? sw[a0] * inv : sw[a0];
-                    } else if (op == OP_GRADC) {
-                        v = sg[a0][a1] - g[a1] * (sw[a0] * inv);
-                    } else if (op == OP_GRADD) {
-                        v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
-                    } else if (op == OP_DIV) {
-                        double f = sg[a0][0] + sg[a1][1] + sg[a2][2];
-                        double b = (sw[a0] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
-                        v = f - b;
-                    } else {  // OP_CURL, component a3
-                        double Ax = sw[a0] * inv, Ay = sw[a1] * inv, Az = sw[a2] * inv;
-                        double f, b;
-                        if (a3 == 0) { f = sg[a1][2] - sg[a2][1]; b = Ay * g[2] - Az * g[1]; }
-                        else if (a3 == 1) { f = sg[a2][0] - sg[a0][2]; b = Az * g[0] - Ax * g[2]; }
-                        else { f = sg[a0][1] - sg[a1][0]; b = Ax * g[1] - Ay * g[0]; }
-                        v = -(f - b);
-                    }
-                    A.out[o][k] = (T)v;
-                }
-            }
-        }
-    }
-    // ---- statistics and errors ----
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
-        n_retest += __shfl_xor_sync(PSB_FULL, n_retest, o);
-    }
-    if (lane == 0 && A.stats) {
-        atomicAdd(&A.stats[0], n_pairs);
-        atomicAdd(&A.stats[1], n_retest);
-    }
-    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
-}
-
-// ---------------------------------------------------------------------------
 // Line kernel (line-integrated scalars, LUT kernel)
 // ---------------------------------------------------------------------------
 // _lin_lut, kernel_function/line_integrated_kernel.jl:13-19, with the
@@ -480,38 +199,51 @@ template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C
     return invh * v;
 }
 
+// Per-warp shared-memory stage of a span of leaves (FP32C line path).
+template <int KC> struct LStage {
+    float4 L[SPAN];
+    float mr[SPAN];
+    float col[KC][SPAN];
+};
+
 template <class T, int PREC, int ST, int KC, int WHAT>
 __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
+    // FP32C with double inputs: float tests with a double fallback, leaf
+    // spans.  Otherwise the reference's own arithmetic node by node, so that
+    // the pruning decisions (including the rounding of the line-box lower
+    // bound) are the reference's.
     constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* lut = (CT*)smem_raw;
-    {
-        for (int i = threadIdx.x; i < LUT_N; i += blockDim.x)
-            lut[i] = (PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i];
-    }
+    __shared__ LStage<KC> lstage_all[4];
+    for (int i = threadIdx.x; i < LUT_N; i += blockDim.x)
+        lut[i] = (PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i];
     __syncthreads();
     // dq = Q[2] - Q[1] of the 4096-point table = 2/4095 rounded to CT
     const CT dq = (CT)(2.0 / 4095.0);
 
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int wib = threadIdx.x >> 5;
+    LStage<KC>& st = lstage_all[wib];
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     if (tile >= A.src.ntiles) return;
     const int64_t k = sample_of(A.src, tile, lane);
     const bool valid = k >= 0;
     T o[3] = {T(0), T(0), T(0)}, m[3] = {T(0), T(0), T(1)};
     if (valid) sample_coords(A.src, k, o, m);
-    float of[3] = {(float)o[0], (float)o[1], (float)o[2]};
-    float mf3[3] = {(float)m[0], (float)m[1], (float)m[2]};
-    // float line error near any box: origin rounding + direction rounding x distance
+    const float of[3] = {(float)o[0], (float)o[1], (float)o[2]};
+    const float mf3[3] = {(float)m[0], (float)m[1], (float)m[2]};
     // |o|_1 and the particle coordinate scale S (coord_err = 2^-23 S)
     const float onorm = fabsf(of[0]) + fabsf(of[1]) + fabsf(of[2]);
     const float S = tv.coord_err / U1;
     const float el = 4.f * U1 * (onorm + 6.f * S) + 1e-30f;
+    const float e64 = 4.5e-16f * (onorm + 6.f * S) * (onorm + 6.f * S);
     const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
     unsigned long long n_pairs = 0, n_retest = 0;
+    int64_t steps = 0;
 
     T ha = T(0);
     if (ST != ST_SCATTER && valid) ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
@@ -522,7 +254,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
         ra2_lo = __double2float_rd((double)ra2) * (1.f - RELM);
     }
-    CT ia = (ST != ST_SCATTER) ? CT(1) / (CT)ha : CT(0);
+    const CT ia = (ST != ST_SCATTER) ? CT(1) / (CT)ha : CT(0);
 
     Acc S1, Sw[KC];
     S1.zero();
@@ -532,70 +264,8 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     int64_t hcount = 0;
     const int kc = A.rec.kc;
 
-    int64_t ctile = -1;
-    float cf[3] = {0.f, 0.f, 0.f}, cerr = 0.f;
-
-    auto node_fn = [&](int ni) -> bool {
-        if (BAND) {
-            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
-            float lb = lb_d2_line_box(of, mf3, el, lo, hi);
-            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
-        } else {
-            T d2n = ex_d2_line_box<T>(o, m, tv, ni);
-            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
-            return !(d2n > r2);
-        }
-    };
-
-    auto leaf_fn = [&](int64_t li) {
-        CT s;
-        T hb;
-        bool acc;
-        if (BAND) {
-            int64_t t = li >> 5;
-            if (t != ctile) {
-                // perpendicular offset of the tile anchor from the line, in double
-                ctile = t;
-                double q0 = __ldg(&tv.anchor[3 * t]) - (double)o[0];
-                double q1 = __ldg(&tv.anchor[3 * t + 1]) - (double)o[1];
-                double q2 = __ldg(&tv.anchor[3 * t + 2]) - (double)o[2];
-                double t0 = q0 * (double)m[0] + q1 * (double)m[1] + q2 * (double)m[2];
-                double c0 = q0 - t0 * (double)m[0], c1 = q1 - t0 * (double)m[1], c2 = q2 - t0 * (double)m[2];
-                cf[0] = (float)c0; cf[1] = (float)c1; cf[2] = (float)c2;
-                cerr = 1e-15f * (float)(fabs(q0) + fabs(q1) + fabs(q2) + 1.0);
-            }
-            float4 L = __ldg(&tv.leaf4[li]);
-            float v0 = L.x + cf[0], v1 = L.y + cf[1], v2 = L.z + cf[2];
-            float vm = v0 * mf3[0] + v1 * mf3[1] + v2 * mf3[2];
-            float w0 = v0 - vm * mf3[0], w1 = v1 - vm * mf3[1], w2 = v2 - vm * mf3[2];
-            float fs = w0 * w0 + w1 * w1 + w2 * w2;
-            float vn = fabsf(v0) + fabsf(v1) + fabsf(v2);
-            float ev = 8.f * U1 * (vn + fabsf(L.x) + fabsf(L.y) + fabsf(L.z)) + cerr + 1e-30f;
-            float r = sqrtf(fs);
-            float up = r + ev, dn = fmaxf(r - ev, 0.f);
-            float rb2 = 4.f * L.w * L.w;
-            float r2lo, r2hi;
-            if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
-            else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
-            else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
-            // the double reference value differs from the exact one by ~1e-16 |x-o|^2
-            float e64 = 4.5e-16f * (onorm + 6.f * S) * (onorm + 6.f * S);
-            if (up * up * (1.f + RELM) + e64 < r2lo) acc = true;
-            else if (dn * dn * (1.f - RELM) - e64 > r2hi) acc = false;
-            else {
-                ++n_retest;
-                T e2 = ex_d2_line<T>(o, m, tv.x[li], tv.y[li], tv.z[li]);
-                acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
-            }
-            if (!acc) return;
-            s = (CT)fs;
-            hb = (T)L.w;
-        } else {
-            T e2 = ex_d2_line<T>(o, m, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
-            hb = __ldg(&tv.h[li]);
-            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
-            s = (CT)e2;
-        }
+    // line-integrated weight of one accepted pair (s = squared distance)
+    auto body = [&](int64_t li, CT s, CT hb, CT mr, const CT* cols) {
         ++n_pairs;
         if (WHAT == WHAT_DIGEST) {
             ++hcount;
@@ -606,23 +276,106 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         CT W;
         if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq);
         else {
-            CT hbc = (CT)hb;
-            CT Wb = line_W<CT>(dr, hbc, CT(1) / hbc, lut, dq);
+            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq);
             W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq) + Wb);
         }
-        CT mr = (PREC == PREC_FP64) ? (CT)((double)tv.m[li] / (double)tv.rho[li]) : (CT)__ldg(&tv.mrho[li]);
         const CT w = mr * W;
         S1.add(w);
 #pragma unroll
-        for (int c = 0; c < KC; ++c) {
-            if (c < kc) {
-                CT a = (PREC == PREC_FP64) ? (CT)__ldg(&A.colT[c][li]) : (CT)__ldg(&A.colF[c][li]);
-                Sw[c].add(a * w);
-            }
-        }
+        for (int c = 0; c < KC; ++c)
+            if (c < kc) Sw[c].add(cols[c] * w);
     };
 
-    bool ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
+    bool ok;
+    if constexpr (BAND) {
+        auto node_fn = [&](int ni) -> bool {
+            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
+            float lb = lb_d2_line_box(of, mf3, el, lo, hi);
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+        };
+        // perpendicular offset of a tile anchor from the line, in double
+        auto perp_anchor = [&](int64_t t, float c[3], float& cerr) {
+            double q0 = __ldg(&tv.anchor[3 * t]) - (double)o[0];
+            double q1 = __ldg(&tv.anchor[3 * t + 1]) - (double)o[1];
+            double q2 = __ldg(&tv.anchor[3 * t + 2]) - (double)o[2];
+            double t0 = q0 * (double)m[0] + q1 * (double)m[1] + q2 * (double)m[2];
+            c[0] = (float)(q0 - t0 * (double)m[0]);
+            c[1] = (float)(q1 - t0 * (double)m[1]);
+            c[2] = (float)(q2 - t0 * (double)m[2]);
+            cerr = 1e-15f * (float)(fabs(q0) + fabs(q1) + fabs(q2) + 1.0);
+        };
+        auto span_fn = [&](int64_t lo, int cnt, bool part) {
+            __syncwarp();
+            if (lane < cnt) {
+                const int64_t li = lo + lane;
+                st.L[lane] = __ldg(&tv.leaf4[li]);
+                if (WHAT != WHAT_DIGEST) {
+                    st.mr[lane] = __ldg(&tv.mrho[li]);
+#pragma unroll
+                    for (int c = 0; c < KC; ++c)
+                        if (c < kc) st.col[c][lane] = __ldg(&A.colF[c][li]);
+                }
+            }
+            __syncwarp();
+            if (!part) return;
+            const int64_t t0 = lo >> 5;
+            float c0[3], c1[3] = {0.f, 0.f, 0.f}, ce0, ce1 = 0.f;
+            perp_anchor(t0, c0, ce0);
+            if (((lo + cnt - 1) >> 5) != t0) perp_anchor(t0 + 1, c1, ce1);
+            for (int j = 0; j < cnt; ++j) {
+                const bool second = ((lo + j) >> 5) != t0;
+                const float* cf = second ? c1 : c0;
+                const float cerr = second ? ce1 : ce0;
+                const float4 L = st.L[j];
+                float v0 = L.x + cf[0], v1 = L.y + cf[1], v2 = L.z + cf[2];
+                float vm = v0 * mf3[0] + v1 * mf3[1] + v2 * mf3[2];
+                float w0 = v0 - vm * mf3[0], w1 = v1 - vm * mf3[1], w2 = v2 - vm * mf3[2];
+                float fs = w0 * w0 + w1 * w1 + w2 * w2;
+                float vn = fabsf(v0) + fabsf(v1) + fabsf(v2);
+                float ev = 8.f * U1 * (vn + fabsf(L.x) + fabsf(L.y) + fabsf(L.z)) + cerr + 1e-30f;
+                float r = sqrtf(fs);
+                float up = r + ev, dn = fmaxf(r - ev, 0.f);
+                float rb2 = 4.f * L.w * L.w;
+                float r2lo, r2hi;
+                if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
+                else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
+                else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
+                bool acc;
+                if (up * up * (1.f + RELM) + e64 < r2lo) acc = true;
+                else if (dn * dn * (1.f - RELM) - e64 > r2hi) acc = false;
+                else {
+                    ++n_retest;
+                    const int64_t li = lo + j;
+                    T e2 = ex_d2_line<T>(o, m, tv.x[li], tv.y[li], tv.z[li]);
+                    acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
+                }
+                if (!acc) continue;
+                CT cols[KC];
+#pragma unroll
+                for (int c = 0; c < KC; ++c) cols[c] = (c < kc) ? (CT)st.col[c][j] : CT(0);
+                body(lo + j, (CT)fs, (CT)L.w, (CT)st.mr[j], cols);
+            }
+        };
+        ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps);
+    } else {
+        auto node_fn = [&](int ni) -> bool {
+            ++steps;
+            T d2n = ex_d2_line_box<T>(o, m, tv, ni);
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            return !(d2n > r2);
+        };
+        auto leaf_fn = [&](int64_t li) {
+            T e2 = ex_d2_line<T>(o, m, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
+            T hb = __ldg(&tv.h[li]);
+            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
+            CT cols[KC];
+#pragma unroll
+            for (int c = 0; c < KC; ++c) cols[c] = (c < kc) ? (CT)__ldg(&A.colT[c][li]) : CT(0);
+            CT mr = (WHAT == WHAT_DIGEST) ? CT(0) : (CT)((double)tv.m[li] / (double)tv.rho[li]);
+            body(li, (CT)e2, (CT)hb, mr, cols);
+        };
+        ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
+    }
 
     if (valid) {
         if (WHAT == WHAT_DIGEST) {
@@ -654,6 +407,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     if (lane == 0 && A.stats) {
         atomicAdd(&A.stats[0], n_pairs);
         atomicAdd(&A.stats[1], n_retest);
+        atomicAdd(&A.stats[2], (unsigned long long)steps);
     }
     if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
 }

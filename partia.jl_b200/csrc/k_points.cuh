@@ -1,0 +1,692 @@
+// k_points.cuh -- point-sample interpolation kernel.
+//
+// One warp owns a tile of 32 spatially close samples (one per lane) and walks
+// the LBVH once for all of them (warp_traverse_spans).  A span of <= 32
+// consecutive leaves is processed "transposed": lane j holds leaf j of the
+// span; for every sample s that wants the span (a ballot), all lanes test
+// their leaf against sample s at once and the ballot of the results is sample
+// s's accept mask.  Each lane then runs the pair bodies of its own mask, in
+// increasing leaf order (the reference's DFS order).
+//
+// Inclusion decisions: exact reference arithmetic for double inputs in
+// PSB_PREC_FP64 and for float inputs; with double inputs in PSB_PREC_FP32C a
+// float test classifies each pair as surely in, surely out or undecided, and
+// undecided pairs are decided by the reference's double test.
+#pragma once
+
+#include "interp_kernels.cuh"
+
+namespace psb {
+
+// Per-warp shared memory: the span's leaves and the tile's samples.
+template <class T, bool BAND, int KC> struct PStage {
+    // leaves
+    T x[SPAN], y[SPAN], z[SPAN], h[SPAN], m[SPAN], rho[SPAN];
+    T col[KC][SPAN];
+    // samples
+    T px[SPAN], py[SPAN], pz[SPAN], ra2[SPAN], best[SPAN];
+};
+template <class T, int KC> struct PStage<T, true, KC> {
+    static constexpr int NB = 1;            // spans batched before the pair bodies run
+    static constexpr int SB = NB * SPAN;
+    // leaves of up to NB spans (slot b*32 + j = leaf j of batched span b)
+    float4 Q[SB];       // position relative to the warp anchor, h (inclusion tests)
+    float4 Lr[SB];      // position relative to the leaf's own 32-leaf tile anchor (pair bodies)
+    float4 K[SB];       // 1/h, sigma/h^3, sigma/h^4, m/rho
+    float mf[SB];       // m
+    float col[KC][SB];
+    int64_t lo[NB];     // first leaf of each batched span
+    float eq[SPAN];     // nearest search: error bound of Q
+    // samples: position relative to the warp anchor + its error, radius bounds
+    float4 P[SPAN];
+    float2 R[SPAN];
+    float2 AB[SPAN];    // per-span squared thresholds: surely in below A, surely out above B
+    float thr[SPAN];    // nearest search: candidate threshold on the float d2
+};
+
+template <class T, int PREC, int ST, int KC, int WHAT>
+__global__ void __launch_bounds__(128) k_points(const Args<T> A) {
+    using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
+    using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
+    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
+    constexpr bool SHIFT = (PREC == PREC_FP32C);  // accumulate A - A0 (cancellation-free gradients)
+    __shared__ PStage<T, BAND, KC> stage_all[4];
+    const TreeView<T>& tv = A.tv;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    auto& st = stage_all[wib];
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (tile >= A.src.ntiles) return;  // warp-uniform
+
+    const int64_t k = sample_of(A.src, tile, lane);
+    const bool valid = k >= 0;
+    T p[3] = {T(0), T(0), T(0)}, dd[3];
+    if (valid) sample_coords(A.src, k, p, dd);
+    const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+    const float pem = U1 * fmaxf(fmaxf(fabsf(pf[0]), fabsf(pf[1])), fabsf(pf[2])) + 1e-30f;
+    const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
+    const int kc = A.rec.kc;
+    const bool need_dg = A.rec.need_dg != 0;
+    unsigned long long n_pairs = 0, n_retest = 0;
+    unsigned long long n_spans = 0, n_parts = 0, n_bodyit = 0;  // main-pass work counters (warp-uniform)
+    int64_t steps = 0;
+    bool ok = true;
+
+    // warp anchor: the first valid sample of the tile
+    const unsigned vmask = __ballot_sync(PSB_FULL, valid);
+    const int first = vmask ? __ffs(vmask) - 1 : 0;
+    const double cw[3] = {__shfl_sync(PSB_FULL, (double)p[0], first), __shfl_sync(PSB_FULL, (double)p[1], first),
+                          __shfl_sync(PSB_FULL, (double)p[2], first)};
+    if constexpr (BAND) {
+        float sr[3] = {(float)((double)p[0] - cw[0]), (float)((double)p[1] - cw[1]), (float)((double)p[2] - cw[2])};
+        float es = U1 * (fabsf(sr[0]) + fabsf(sr[1]) + fabsf(sr[2])) + 1e-30f;
+        st.P[lane] = make_float4(sr[0], sr[1], sr[2], es);
+    } else {
+        st.px[lane] = p[0]; st.py[lane] = p[1]; st.pz[lane] = p[2];
+    }
+
+    // stage leaves [lo, lo+cnt): lane j takes leaf lo+j (all lanes call)
+    auto stage_span = [&](int64_t lo, int cnt, bool with_cols) -> float {
+        __syncwarp();
+        float eqmax = 0.f;
+        if (lane < cnt) {
+            const int64_t li = lo + lane;
+            if constexpr (BAND) {
+                const float4 L = __ldg(&tv.leaf4[li]);
+                const int64_t t = li >> 5;
+                float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
+                float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
+                float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
+                st.Q[lane] = make_float4(q0, q1, q2, L.w);
+                eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
+                              fabsf(q0) + fabsf(q1) + fabsf(q2));
+                st.eq[lane] = eqmax;
+            } else {
+                st.x[lane] = __ldg(&tv.x[li]); st.y[lane] = __ldg(&tv.y[li]); st.z[lane] = __ldg(&tv.z[li]);
+                st.h[lane] = __ldg(&tv.h[li]);
+                if (with_cols) {
+                    st.m[lane] = __ldg(&tv.m[li]); st.rho[lane] = __ldg(&tv.rho[li]);
+#pragma unroll
+                    for (int c = 0; c < KC; ++c)
+                        if (c < kc) st.col[c][lane] = __ldg(&A.colT[c][li]);
+                }
+            }
+        }
+        __syncwarp();
+        return eqmax;
+    };
+
+    // ---- sample smoothing length (LBVH_find_nearest_h or given) ----
+    // The reference starts its nearest search with an infinite bound.  Here the
+    // bound starts at the exact distance to the particle next to the sample
+    // in Morton order (found by binary search of the sorted codes), and ties
+    // are resolved towards the smaller leaf index, so the result is the same
+    // argmin -- the first leaf in DFS order with the minimum distance.
+    T ha = T(0);
+    if (ST != ST_SCATTER) {
+        if (A.hmode == PSB_H_NEAREST) {
+            double best = INFINITY;
+            int64_t bidx = -1;
+            if (valid) {
+                uint64_t q[3];
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    double f = ((double)p[d] - tv.qlo[d]) * tv.qscale[d];
+                    f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
+                    q[d] = (uint64_t)f;
+                }
+                const uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+                int64_t lo = 0, hi = tv.n;  // first index with codes[i] >= code
+                while (lo < hi) {
+                    int64_t mid = (lo + hi) >> 1;
+                    if (__ldg(&tv.codes[mid]) < code) lo = mid + 1;
+                    else hi = mid;
+                }
+                const int64_t c0 = lo > 0 ? lo - 1 : 0;
+                const int64_t c1 = lo < tv.n ? lo : tv.n - 1;
+                const double d0 = (double)ex_d2_pp<T>(p, tv.x[c0], tv.y[c0], tv.z[c0]);
+                const double d1 = (double)ex_d2_pp<T>(p, tv.x[c1], tv.y[c1], tv.z[c1]);
+                if (d1 < d0) { best = d1; bidx = c1; } else { best = d0; bidx = c0; }
+            }
+            auto better = [&](double d2, int64_t li) { return d2 < best || (d2 == best && li < bidx); };
+            auto node_fn = [&](int ni) -> bool {
+                if constexpr (BAND) {
+                    float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
+                    return !((double)lb > best);
+                } else {
+                    return !((double)ex_d2_pbox<T>(p, tv, ni) > best);
+                }
+            };
+            auto span_fn = [&](int64_t lo, int cnt, bool part) {
+                float eqmax = stage_span(lo, cnt, false);
+                const unsigned parts = __ballot_sync(PSB_FULL, part);
+                if (!parts) return;
+                unsigned cand = 0;
+                if constexpr (BAND) {
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) eqmax = fmaxf(eqmax, __shfl_xor_sync(PSB_FULL, eqmax, o));
+                    // candidates: float d2 not above (sqrt(best) + error)^2
+                    {
+                        const float4 Pme = st.P[lane];
+                        float bs = (float)sqrt(best);
+                        float e = 1.7320508f * (Pme.w + eqmax) + 4.f * U1 * bs + 1e-30f;
+                        float t = (bs + e) * (1.f + 4.f * U1);
+                        st.thr[lane] = isinf(best) ? INFINITY : t * t;
+                    }
+                    __syncwarp();
+                    const float4 Q = st.Q[lane < cnt ? lane : 0];
+                    for (unsigned pp = parts; pp; pp &= pp - 1) {
+                        const int s = __ffs(pp) - 1;
+                        const float4 P = st.P[s];
+                        const float thr = st.thr[s];
+                        float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                        bool c = (lane < cnt) && (dx * dx + dy * dy + dz * dz <= thr);
+                        unsigned b = __ballot_sync(PSB_FULL, c);
+                        if (lane == s) cand = b;
+                    }
+                    for (; cand; cand &= cand - 1) {
+                        const int64_t li = lo + __ffs(cand) - 1;
+                        double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                        if (better(d2, li)) { best = d2; bidx = li; }
+                    }
+                } else {
+                    st.best[lane] = (T)best;
+                    __syncwarp();
+                    const int j = lane < cnt ? lane : 0;
+                    const T xj = st.x[j], yj = st.y[j], zj = st.z[j];
+                    for (unsigned pp = parts; pp; pp &= pp - 1) {
+                        const int s = __ffs(pp) - 1;
+                        const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
+                        bool c = (lane < cnt) && (ex_d2_pp<T>(ps, xj, yj, zj) <= st.best[s]);
+                        unsigned b = __ballot_sync(PSB_FULL, c);
+                        if (lane == s) cand = b;
+                    }
+                    for (; cand; cand &= cand - 1) {
+                        const int jj = __ffs(cand) - 1;
+                        double d2 = (double)ex_d2_pp<T>(p, st.x[jj], st.y[jj], st.z[jj]);
+                        if (better(d2, lo + jj)) { best = d2; bidx = lo + jj; }
+                    }
+                }
+            };
+            ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+            if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
+        } else if (valid) {
+            ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
+        }
+    }
+    // radius = Kvalid * ha; radius2 = radius * radius (general_interpolation.jl:20-21)
+    const T ra = X<T>::mul(T(2), ha);
+    const T ra2 = X<T>::mul(ra, ra);
+    if constexpr (BAND) {
+        float ralo = 0.f, rahi = 0.f;
+        if (ST != ST_SCATTER) {
+            ralo = __double2float_rd((double)ra) * (1.f - 2.f * U1);
+            rahi = __double2float_ru((double)ra) * (1.f + 2.f * U1);
+        }
+        st.R[lane] = make_float2(ralo, rahi);
+    } else {
+        st.ra2[lane] = ra2;
+    }
+    float ra2_hi = 0.f;
+    if (BAND && ST != ST_SCATTER) ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
+
+    // ---- per-sample constants of the kernel weights ----
+    const CT sig = inv_pi<CT>();
+    CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
+    if (ST != ST_SCATTER) {
+        ia = CT(1) / (CT)ha;
+        sa3 = sig * ia * ia * ia;
+        sa4 = sa3 * ia;
+    }
+
+    // ---- accumulators ----
+    Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
+    CT dens = CT(0);
+    CT a0[KC];
+    bool have0 = false;
+    S1.zero(); Dm.zero();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { G[d].zero(); Dg[d].zero(); }
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+        Sw[c].zero();
+        a0[c] = CT(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Sg[c][d].zero();
+    }
+    uint64_t hsum = 0;
+    int64_t hcount = 0;
+
+    // kernel weights and accumulation of one accepted pair (leaf j of the stage)
+    auto body = [&](int64_t li, int j, CT dx, CT dy, CT dz, CT d2, CT hb) {
+        ++n_pairs;
+        if (WHAT == WHAT_DIGEST) {
+            ++hcount;
+            hsum += mix64((uint64_t)(li + 1));
+            return;
+        }
+        const CT r = sqrt(d2);
+        const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
+        CT Wsum = CT(0), csum = CT(0);  // kernel value and gradient coefficient (grad W = c * delta)
+        if (ST != ST_SCATTER) {
+            CT f, df;
+            m4_fdf<CT>(r * ia, f, df);
+            Wsum = sa3 * f;
+            csum = sa4 * df * invr;
+        }
+        if (ST != ST_GATHER) {
+            CT ib = CT(1) / hb;
+            CT sb3 = sig * ib * ib * ib;
+            CT f, df;
+            m4_fdf<CT>(r * ib, f, df);
+            CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
+            if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
+            else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
+        }
+        CT mb, mr;
+        if constexpr (BAND) {
+            mr = (CT)st.K[j].w;
+            mb = (CT)st.mf[j];
+        } else {
+            mb = (CT)st.m[j];
+            mr = (CT)((double)st.m[j] / (double)st.rho[j]);
+        }
+        if (WHAT == WHAT_DENSITY) {
+            dens += mb * Wsum;
+            return;
+        }
+        const CT w = mr * Wsum;
+        const CT gc = mr * csum;
+        const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
+        S1.add(w);
+        G[0].add(gx); G[1].add(gy); G[2].add(gz);
+        if (SHIFT && !have0) {
+            have0 = true;
+#pragma unroll
+            for (int c = 0; c < KC; ++c)
+                if (c < kc) a0[c] = (CT)st.col[c][j];
+        }
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                CT a = (CT)st.col[c][j];
+                if (SHIFT) a -= a0[c];
+                Sw[c].add(a * w);
+                Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+            }
+        }
+        if (need_dg) {
+            Dm.add(mb * Wsum);
+            CT mc = mb * csum;
+            Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+        }
+    };
+
+    auto node_fn = [&](int ni) -> bool {
+        if constexpr (BAND) {
+            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
+            float lb = lb_d2_pbox(pf, pem, lo, hi);
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+        } else {
+            T d2n = ex_d2_pbox<T>(p, tv, ni);
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            return !(d2n > r2);
+        }
+    };
+
+    if constexpr (BAND) {
+        // ---- FP32C main pass: batched spans, transposed tests, flattened pair loop ----
+        constexpr int NB = PStage<T, true, KC>::NB;
+        int nb = 0;                                   // batched spans (warp-uniform)
+        unsigned acc0 = 0, acc1 = 0, acc2 = 0, acc3 = 0;
+        unsigned unc0 = 0, unc1 = 0, unc2 = 0, unc3 = 0;
+        const float4 Pme = st.P[lane];
+        const float2 Rme = st.R[lane];
+        float R0[3] = {0.f, 0.f, 0.f}, R1[3] = {0.f, 0.f, 0.f};
+        int64_t rt0 = 0;
+        float esmax = Pme.w, rahimax = Rme.y;  // tile-wide maxima (sample error, sample radius)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            esmax = fmaxf(esmax, __shfl_xor_sync(PSB_FULL, esmax, o));
+            rahimax = fmaxf(rahimax, __shfl_xor_sync(PSB_FULL, rahimax, o));
+        }
+
+        auto pair_body = [&](int b, int j) {
+            const int slot = b * SPAN + j;
+            ++n_pairs;
+            if (WHAT == WHAT_DIGEST) {
+                ++hcount;
+                hsum += mix64((uint64_t)(st.lo[b] + j + 1));
+                return;
+            }
+            const float4 Lj = st.Lr[slot];
+            const float4 K = st.K[slot];
+            const bool first_tile = ((st.lo[b] + j) >> 5) == rt0;
+            const float dx = (first_tile ? R0[0] : R1[0]) - Lj.x;
+            const float dy = (first_tile ? R0[1] : R1[1]) - Lj.y;
+            const float dz = (first_tile ? R0[2] : R1[2]) - Lj.z;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
+            const float r = d2 * invr;
+            float Wsum = 0.f, csum = 0.f;
+            if (ST != ST_SCATTER) {
+                float f, df;
+                m4_fdf<float>(r * (float)ia, f, df);
+                Wsum = (float)sa3 * f;
+                csum = (float)sa4 * df;
+            }
+            if (ST != ST_GATHER) {
+                float f, df;
+                m4_fdf<float>(r * K.x, f, df);
+                if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
+                else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
+            }
+            csum *= invr;
+            if (WHAT == WHAT_DENSITY) {
+                Dm.add(st.mf[slot] * Wsum);
+                return;
+            }
+            const float w = K.w * Wsum;
+            const float gc = K.w * csum;
+            const float gx = gc * dx, gy = gc * dy, gz = gc * dz;
+            S1.add(w);
+            G[0].add(gx); G[1].add(gy); G[2].add(gz);
+            if (SHIFT && !have0) {
+                have0 = true;
+#pragma unroll
+                for (int c = 0; c < KC; ++c)
+                    if (c < kc) a0[c] = st.col[c][slot];
+            }
+#pragma unroll
+            for (int c = 0; c < KC; ++c) {
+                if (c < kc) {
+                    const float a = st.col[c][slot] - (float)a0[c];
+                    Sw[c].add(a * w);
+                    Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+                }
+            }
+            if (need_dg) {
+                const float mb = st.mf[slot];
+                Dm.add(mb * Wsum);
+                const float mc = mb * csum;
+                Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+            }
+        };
+
+        auto flush = [&]() {
+            // undecided pairs: the reference's double test
+            for (int b = 0; b < nb; ++b) {
+                unsigned u = b == 0 ? unc0 : b == 1 ? unc1 : b == 2 ? unc2 : unc3;
+                unsigned add = 0;
+                for (; u; u &= u - 1) {
+                    const int jj = __ffs(u) - 1;
+                    const int64_t li = st.lo[b] + jj;
+                    ++n_retest;
+                    T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) add |= 1u << jj;
+                }
+                if (b == 0) acc0 |= add; else if (b == 1) acc1 |= add; else if (b == 2) acc2 |= add; else acc3 |= add;
+            }
+            unc0 = unc1 = unc2 = unc3 = 0;
+            n_bodyit += __reduce_max_sync(PSB_FULL, (unsigned)(__popc(acc0) + __popc(acc1) + __popc(acc2) + __popc(acc3)));
+            // one flattened loop over the pairs of all batched spans, in leaf order
+            while (true) {
+                int b;
+                unsigned* m;
+                if (acc0) { b = 0; m = &acc0; }
+                else if (acc1) { b = 1; m = &acc1; }
+                else if (acc2) { b = 2; m = &acc2; }
+                else if (acc3) { b = 3; m = &acc3; }
+                else break;
+                const int jj = __ffs(*m) - 1;
+                *m &= *m - 1;
+                pair_body(b, jj);
+            }
+            nb = 0;
+            __syncwarp();
+        };
+
+        auto span_fn = [&](int64_t lo, int cnt, bool part) {
+            const unsigned parts = __ballot_sync(PSB_FULL, part);
+            if (!parts) return;
+            const int b = nb;
+            const int slot = b * SPAN + lane;
+            float eq = 0.f, Aj = 0.f, Bj = 0.f, hb = 0.f;
+            if (lane < cnt) {
+                const int64_t li = lo + lane;
+                const float4 L = __ldg(&tv.leaf4[li]);
+                const int64_t t = li >> 5;
+                const float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
+                const float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
+                const float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                const float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
+                hb = L.w;
+                st.Q[slot] = make_float4(q0, q1, q2, hb);
+                st.Lr[slot] = L;
+                eq = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
+                           fabsf(q0) + fabsf(q1) + fabsf(q2));
+                if (WHAT != WHAT_DIGEST) {
+                    const float ih = 1.f / hb;
+                    const float s3 = (float)sig * ih * ih * ih;
+                    st.K[slot] = make_float4(ih, s3, s3 * ih, __ldg(&tv.mrho[li]));
+                    if (need_dg || WHAT == WHAT_DENSITY) st.mf[slot] = __ldg(&tv.mf[li]);
+#pragma unroll
+                    for (int c = 0; c < KC; ++c)
+                        if (c < kc) st.col[c][slot] = __ldg(&A.colF[c][li]);
+                }
+            }
+            if (lane == 0) st.lo[b] = lo;
+            // this lane's sample relative to the anchors of the span's (at most
+            // two) 32-leaf tiles, in double then rounded: the pair separation
+            // R - L then carries only the rounding of two small vectors
+            {
+                const int64_t t0 = lo >> 5;
+                const int64_t t1 = (lo + cnt - 1) >> 5;
+                rt0 = t0;
+                R0[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t0]));
+                R0[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t0 + 1]));
+                R0[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t0 + 2]));
+                R1[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t1]));
+                R1[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t1 + 1]));
+                R1[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t1 + 2]));
+            }
+            // error bound of float distances for this span, the same for every pair
+            float eqm = eq;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) eqm = fmaxf(eqm, __shfl_xor_sync(PSB_FULL, eqm, o));
+            const float rbhi = 2.f * hb * (1.f + 2.f * U1), rblo = 2.f * hb * (1.f - 2.f * U1);
+            // the rounding of r itself enters through 4 U1 r (r <= the larger radius)
+            float rmax = rahimax;
+            if (ST != ST_GATHER) {
+                float rb = rbhi;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) rb = fmaxf(rb, __shfl_xor_sync(PSB_FULL, rb, o));
+                rmax = fmaxf(rmax, rb);
+            }
+            const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
+            if (ST != ST_GATHER && lane < cnt) {
+                const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
+                Aj = il * il;
+                Bj = ih2 * ih2;
+            }
+            {
+                float As = 0.f, Bs = 0.f;
+                if (ST != ST_SCATTER) {
+                    const float il = fmaxf((Rme.x - E) * (1.f - 4.f * U1), 0.f), ih2 = (Rme.y + E) * (1.f + 4.f * U1);
+                    As = il * il;
+                    Bs = ih2 * ih2;
+                }
+                st.AB[lane] = make_float2(As, Bs);
+            }
+            __syncwarp();
+            const float4 Q = st.Q[lane < cnt ? slot : b * SPAN];
+            unsigned myacc = 0, myunc = 0;
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const float4 P = st.P[s];
+                const float2 AB = st.AB[s];
+                const float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                const bool in = (lane < cnt) && d2 < fmaxf(AB.x, Aj);
+                const bool un = (lane < cnt) && !in && !(d2 > fmaxf(AB.y, Bj));
+                const unsigned bi = __ballot_sync(PSB_FULL, in), bu = __ballot_sync(PSB_FULL, un);
+                if (lane == s) { myacc = bi; myunc = bu; }
+            }
+            if (b == 0) { acc0 = myacc; unc0 = myunc; }
+            else if (b == 1) { acc1 = myacc; unc1 = myunc; }
+            else if (b == 2) { acc2 = myacc; unc2 = myunc; }
+            else { acc3 = myacc; unc3 = myunc; }
+            ++n_spans;
+            n_parts += __popc(parts);
+            nb = b + 1;
+            __syncwarp();
+            if (nb == NB) flush();  // pair bodies of this span (R0 / R1 belong to it)
+        };
+        ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+        if (nb > 0) flush();
+        if (WHAT == WHAT_DENSITY) dens = (CT)Dm.get();
+    } else {
+        const bool with_cols = (WHAT != WHAT_DIGEST);
+        auto span_fn = [&](int64_t lo, int cnt, bool part) {
+            stage_span(lo, cnt, with_cols);
+            const unsigned parts = __ballot_sync(PSB_FULL, part);
+            if (!parts) return;
+            ++n_spans;
+            n_parts += __popc(parts);
+            unsigned acc = 0, unc = 0;
+            const int j = lane < cnt ? lane : 0;
+            if constexpr (BAND) {
+                const float4 Q = st.Q[j];
+                const float eq = st.eq[j];
+                const float rblo = 2.f * Q.w * (1.f - 2.f * U1), rbhi = 2.f * Q.w * (1.f + 2.f * U1);
+                for (unsigned pp = parts; pp; pp &= pp - 1) {
+                    const int s = __ffs(pp) - 1;
+                    const float4 P = st.P[s];
+                    const float2 R = st.R[s];
+                    float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                    float d2 = dx * dx + dy * dy + dz * dz;
+                    float rlo, rhi;
+                    if (ST == ST_GATHER) { rlo = R.x; rhi = R.y; }
+                    else if (ST == ST_SCATTER) { rlo = rblo; rhi = rbhi; }
+                    else { rlo = fmaxf(R.x, rblo); rhi = fmaxf(R.y, rbhi); }
+                    float e = 1.7320508f * (P.w + eq) + 4.f * U1 * rhi + 1e-30f;
+                    float il = (rlo - e) * (1.f - 4.f * U1), ih = (rhi + e) * (1.f + 4.f * U1);
+                    bool in = (lane < cnt) && il > 0.f && d2 < il * il;
+                    bool un = (lane < cnt) && !in && !(d2 > ih * ih);
+                    unsigned bi = __ballot_sync(PSB_FULL, in), bu = __ballot_sync(PSB_FULL, un);
+                    if (lane == s) { acc = bi; unc = bu; }
+                }
+                // undecided pairs: the reference's double test
+                for (unsigned u = unc; u; u &= u - 1) {
+                    const int jj = __ffs(u) - 1;
+                    const int64_t li = lo + jj;
+                    ++n_retest;
+                    T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) acc |= 1u << jj;
+                }
+                const float sr0 = st.P[lane].x, sr1 = st.P[lane].y, sr2 = st.P[lane].z;
+                n_bodyit += __reduce_max_sync(PSB_FULL, (unsigned)__popc(acc));
+                for (; acc; acc &= acc - 1) {
+                    const int jj = __ffs(acc) - 1;
+                    const float4 Qj = st.Q[jj];
+                    float fx = sr0 - Qj.x, fy = sr1 - Qj.y, fz = sr2 - Qj.z;
+                    body(lo + jj, jj, (CT)fx, (CT)fy, (CT)fz, (CT)(fx * fx + fy * fy + fz * fz), (CT)Qj.w);
+                }
+            } else {
+                const T xj = st.x[j], yj = st.y[j], zj = st.z[j], hj = st.h[j];
+                const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj);  // (2 hb)^2
+                for (unsigned pp = parts; pp; pp &= pp - 1) {
+                    const int s = __ffs(pp) - 1;
+                    const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
+                    const T ra2s = st.ra2[s];
+                    T e2 = ex_d2_pp<T>(ps, xj, yj, zj);
+                    T r2 = (ST == ST_GATHER) ? ra2s : ((ST == ST_SCATTER) ? r2b : jmax(ra2s, r2b));
+                    bool in = (lane < cnt) && (e2 <= r2);
+                    unsigned bi = __ballot_sync(PSB_FULL, in);
+                    if (lane == s) acc = bi;
+                }
+                n_bodyit += __reduce_max_sync(PSB_FULL, (unsigned)__popc(acc));
+                for (; acc; acc &= acc - 1) {
+                    const int jj = __ffs(acc) - 1;
+                    const T xb = st.x[jj], yb = st.y[jj], zb = st.z[jj];
+                    const T e2 = ex_d2_pp<T>(p, xb, yb, zb);
+                    body(lo + jj, jj, (CT)(p[0] - xb), (CT)(p[1] - yb), (CT)(p[2] - zb), (CT)e2, (CT)st.h[jj]);
+                }
+            }
+        };
+
+        ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+    }
+
+    // ---- outputs ----
+    if (valid) {
+        if (WHAT == WHAT_DIGEST) {
+            A.dig_count[k] = hcount;
+            A.dig_hash[k] = hsum;
+            if (A.ha_out) A.ha_out[k] = ha;
+        } else if (WHAT == WHAT_DENSITY) {
+            A.out[0][k] = (T)dens;
+        } else {
+            const double s1 = S1.get();
+            const int L = A.rec.L;
+            if (s1 == 0.0) {
+                for (int o = 0; o < L; ++o) A.out[o][k] = qnan<T>();
+            } else {
+                // sums of (A - A0) w and (A - A0) g; gradients, divergences and
+                // curls are invariant under the shift, scalars add A0 back.
+                double sw[MAX_KC], sg[MAX_KC][3], sh[MAX_KC];
+#pragma unroll
+                for (int c = 0; c < KC; ++c) {
+                    sw[c] = Sw[c].get();
+                    sh[c] = (double)a0[c];
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
+                }
+                const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
+                const double inv = 1.0 / s1;
+                for (int o = 0; o < L; ++o) {
+                    const int op = A.rec.op[o];
+                    const int a0i = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
+                    double v;
+                    if (op == OP_SCALAR) {
+                        v = a1 ? sw[a0i] * inv + sh[a0i] : sw[a0i] + sh[a0i] * s1;
+                    } else if (op == OP_GRADC) {
+                        v = sg[a0i][a1] - g[a1] * (sw[a0i] * inv);
+                    } else if (op == OP_GRADD) {
+                        v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
+                    } else if (op == OP_DIV) {
+                        double f = sg[a0i][0] + sg[a1][1] + sg[a2][2];
+                        double b = (sw[a0i] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
+                        v = f - b;
+                    } else {  // OP_CURL, component a3
+                        double Ax = sw[a0i] * inv, Ay = sw[a1] * inv, Az = sw[a2] * inv;
+                        double f, b;
+                        if (a3 == 0) { f = sg[a1][2] - sg[a2][1]; b = Ay * g[2] - Az * g[1]; }
+                        else if (a3 == 1) { f = sg[a2][0] - sg[a0i][2]; b = Az * g[0] - Ax * g[2]; }
+                        else { f = sg[a0i][1] - sg[a1][0]; b = Ax * g[1] - Ay * g[0]; }
+                        v = -(f - b);
+                    }
+                    A.out[o][k] = (T)v;
+                }
+            }
+        }
+    }
+    // ---- statistics and errors ----
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+        n_retest += __shfl_xor_sync(PSB_FULL, n_retest, o);
+    }
+    if (lane == 0 && A.stats) {
+        atomicAdd(&A.stats[0], n_pairs);
+        atomicAdd(&A.stats[1], n_retest);
+        atomicAdd(&A.stats[2], (unsigned long long)steps);
+        atomicAdd(&A.stats[3], n_spans);
+        atomicAdd(&A.stats[4], n_parts);
+        atomicAdd(&A.stats[5], n_bodyit);
+    }
+    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+}  // namespace psb

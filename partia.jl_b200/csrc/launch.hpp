@@ -2,7 +2,7 @@
 // instantiations are split over inst_*.cu so that they compile in parallel.
 #pragma once
 
-#include "interp_kernels.cuh"
+#include "k_points.cuh"
 
 namespace psb {
 

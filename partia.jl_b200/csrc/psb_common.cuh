@@ -81,6 +81,10 @@ template <class T> struct TreeView {
     int32_t root;
     const int32_t* left;     // 2n-1
     const int32_t* escape;   // 2n-1
+    const int4* links;       // n-1: (left, escape, range_lo, range_hi) of internal nodes
+    const uint64_t* codes;   // n sorted, de-duplicated Morton codes
+    double qlo[3];           // particle bounding-box minimum (Morton quantisation)
+    double qscale[3];        // (2^21 - 1) / extent per axis, 0 for a flat axis
     const int32_t* range_lo; // n-1, first leaf (1-based) of internal node
     const int32_t* range_hi; // n-1, last leaf (1-based)
     const T* nmin[3];        // n-1 each

@@ -33,6 +33,7 @@ struct psb_ctx {
     int32_t* left = nullptr; int32_t* right = nullptr;
     int32_t* escape = nullptr; int32_t* parent = nullptr;
     int32_t* range_lo = nullptr; int32_t* range_hi = nullptr;
+    int4* links = nullptr;
     void* nmin[3] = {nullptr, nullptr, nullptr};
     void* nmax[3] = {nullptr, nullptr, nullptr};
     void* nscale = nullptr;

@@ -52,7 +52,9 @@ class Stats(C.Structure):
     _fields_ = [
         ("total_ms", C.c_double), ("h2d_ms", C.c_double), ("order_ms", C.c_double),
         ("nearest_ms", C.c_double), ("interp_ms", C.c_double), ("d2h_ms", C.c_double),
-        ("pairs", C.c_int64), ("exact_retests", C.c_int64), ("launches", C.c_int32), ("reserved", C.c_int32),
+        ("pairs", C.c_int64), ("exact_retests", C.c_int64), ("warp_steps", C.c_int64), ("spans", C.c_int64),
+        ("span_tests", C.c_int64), ("body_iters", C.c_int64), ("launches", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
     def as_dict(self):

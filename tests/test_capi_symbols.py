@@ -1,0 +1,53 @@
+"""The C-ABI library loads and exports every function include/partia_b200.h
+declares; host-only calls behave without a GPU."""
+import ctypes as C
+import os
+import subprocess
+
+import pytest
+
+from partia_b200 import _lib as L
+
+
+def test_library_built_and_exports_header_symbols():
+    assert os.path.exists(L.LIB_PATH), "build with make -C partia.jl_b200/csrc"
+    lib = L.load()
+    declared = L.header_symbols()
+    assert len(declared) >= 15
+    for name in declared:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", L.LIB_PATH], capture_output=True, text=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if " T " in ln}
+    assert set(declared) <= exported
+    # nothing else is exported from the product library
+    assert {s for s in exported if s.startswith("psb_")} == set(declared)
+
+
+def test_abi_version_and_null_context_handling():
+    lib = L.load()
+    assert lib.psb_abi_version() == 1
+    assert lib.psb_destroy(None) == L.PSB_OK
+    assert lib.psb_last_error(None) == b"null context"
+    assert lib.psb_build_lbvh(None, None, None) == L.PSB_EINVAL
+    assert lib.psb_create(None, 0) == L.PSB_EINVAL
+
+
+def test_header_compiles_as_c():
+    src = '#include "partia_b200.h"\nint main(void){ psb_stats s; psb_catalog c; (void)s; (void)c; return 0; }\n'
+    inc = os.path.dirname(L.HEADER_PATH)
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", inc, "-x", "c", "-", "-fsyntax-only"],
+                       input=src, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_struct_layouts_match_python_binding():
+    # psb_stats / psb_catalog sizes as seen by C
+    src = ('#include <stdio.h>\n#include "partia_b200.h"\n'
+           'int main(void){ printf("%zu %zu\\n", sizeof(psb_stats), sizeof(psb_catalog)); return 0; }\n')
+    inc = os.path.dirname(L.HEADER_PATH)
+    exe = "/tmp/psb_sizes"
+    r = subprocess.run(["gcc", "-std=c99", "-I", inc, "-x", "c", "-", "-o", exe], input=src, capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    a, b = map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split())
+    assert a == C.sizeof(L.Stats) and b == C.sizeof(L.Catalog)

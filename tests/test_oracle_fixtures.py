@@ -1,0 +1,158 @@
+"""Oracle pins on the reference's deterministic interpolation fixtures.
+
+ * 4-particle fixture + 3 point samples, symmetric, nearest-particle h,
+   scalar + divergence vs brute force at rtol 1e-10
+   (test/point_samples_interpolation_tests.jl:53-79,
+    test/grid_interpolation_test_common.jl:40-71)
+ * line fixture + 3 lines, scatter, line-integrated scalars vs brute force at
+   rtol 1e-10 (test/point_samples_interpolation_tests.jl:121-155,
+   test/grid_interpolation_test_common.jl:108-144)
+ * 12^3 lattice with variable h, analytic linear fields, all three
+   strategies, the reference's atol/rtol
+   (test/point_samples_interpolation_tests.jl:211-239,
+    test/interpolation_analytic_test_common.jl:31-75)
+ * uniform vector field: divergence = curl = 0 to 1e-12
+   (test/interpolation_tests.jl:305-336)
+ * empty neighbourhoods: density 0, every other field NaN
+   (test/interpolation_tests.jl:52-117)
+"""
+import math
+
+import numpy as np
+import pytest
+
+import bruteforce as B
+import oracle as O
+
+
+def fixture_points():
+    P = dict(x=np.array([0.15, 0.35, 0.55, 0.75]), y=np.array([0.20, 0.60, 0.25, 0.70]),
+             z=np.array([0.25, 0.45, 0.80, 0.30]), h=np.array([0.28, 0.24, 0.26, 0.22]),
+             rho=np.array([1.0, 0.95, 1.05, 1.1]), m=np.array([0.4, 0.45, 0.42, 0.38]))
+    cols = [np.array([10.0, 11.0, 13.0, 12.0]), np.array([0.1, -0.2, 0.3, -0.1]),
+            np.array([0.0, 0.25, -0.15, 0.2]), np.array([-0.05, 0.1, 0.2, -0.1])]
+    return P, cols
+
+
+def make_oracle(P, cols):
+    return O.Oracle(P["x"], P["y"], P["z"], P["m"], P["h"], P["rho"], cols)
+
+
+def test_point_fixture_symmetric_nearest_h():
+    P, cols = fixture_points()
+    orc = make_oracle(P, cols)
+    s = (np.array([0.20, 0.40, 0.65]), np.array([0.25, 0.55, 0.50]), np.array([0.30, 0.50, 0.35]))
+    cat = O.Catalog(scalars=[0], shepard=[1], divs=[1, 2, 3])
+    out = orc.interp_points(*s, cat, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    for i in range(3):
+        p = np.array([s[0][i], s[1][i], s[2][i]])
+        ha = B.nearest_h(P, p)
+        ref = B.general(P, cols, p, ha, "symmetric", scalars=[0], shepard=[1], divs=[(1, 2, 3)])
+        assert out[0][i] == pytest.approx(ref[0], rel=1e-10, abs=1e-12)
+        assert out[1][i] == pytest.approx(ref[1], rel=1e-10, abs=1e-12)
+
+
+@pytest.mark.parametrize("strategy,name", [(O.GATHER, "gather"), (O.SCATTER, "scatter"), (O.SYMMETRIC, "symmetric")])
+def test_point_fixture_all_fields(strategy, name):
+    P, cols = fixture_points()
+    orc = make_oracle(P, cols)
+    rng = np.random.default_rng(3)
+    s = tuple(rng.uniform(0.1, 0.8, 20) for _ in range(3))
+    spec = dict(scalars=[0, 1], shepard=[1, 0], grads=[0, -1], divs=[(1, 2, 3)], curls=[(1, 2, 3)])
+    cat = O.Catalog(scalars=spec["scalars"], shepard=spec["shepard"], grads=spec["grads"],
+                    divs=[c for t in spec["divs"] for c in t], curls=[c for t in spec["curls"] for c in t])
+    out = orc.interp_points(*s, cat, strategy=strategy, hmode=O.H_NEAREST)
+    for i in range(20):
+        p = np.array([s[0][i], s[1][i], s[2][i]])
+        ha = B.nearest_h(P, p)
+        ref = B.general(P, cols, p, ha, name, **spec)
+        got = [o[i] for o in out]
+        for a, b in zip(got, ref):
+            if math.isnan(b):
+                assert math.isnan(a)
+            else:
+                assert a == pytest.approx(b, rel=1e-10, abs=1e-12)
+
+
+def test_line_fixture_scatter():
+    P, cols = fixture_points()
+    cols = cols[:2]
+    orc = make_oracle(P, cols)
+    r2 = 1 / math.sqrt(2.0)
+    o = (np.array([0.20, 0.40, 0.55]), np.array([0.25, 0.35, 0.45]), np.array([0.00, 0.10, 0.20]))
+    d = (np.array([0.0, r2, 1.0]), np.array([0.0, 0.0, 0.0]), np.array([1.0, r2, 0.0]))
+    out = orc.interp_lines(o, d, scalars=[0, 1], shepard=[1, 1], strategy=O.SCATTER)
+    table = O.line_table()
+    for i in range(3):
+        ref = B.line_quantities(P, cols, [o[k][i] for k in range(3)], [d[k][i] for k in range(3)], 0.0, "scatter",
+                                [0, 1], [1, 1], table)
+        assert out[0][i] == pytest.approx(ref[0], rel=1e-10, abs=1e-12)
+        assert out[1][i] == pytest.approx(ref[1], rel=1e-10, abs=1e-12)
+
+
+def lattice(nx=12, eta=1.2):
+    dx = 1.0 / nx
+    c = np.arange(dx / 2, 1.0 - dx / 2 + 1e-12, dx)
+    X, Y, Z = np.meshgrid(c, c, c, indexing="ij")   # x outermost, z fastest, as the Julia loop
+    x, y, z = X.ravel(), Y.ravel(), Z.ravel()
+    n = len(x)
+    h = eta * dx * (1.0 + 0.18 * (x - 0.5) - 0.10 * (y - 0.5) + 0.08 * (z - 0.5))
+    P = dict(x=x, y=y, z=z, m=np.full(n, dx ** 3), h=h, rho=np.ones(n))
+    cols = [x + y + z, x.copy(), y.copy(), z.copy()]
+    return P, cols
+
+
+@pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])
+def test_analytic_linear_fields(strategy):
+    P, cols = lattice()
+    orc = make_oracle(P, cols)
+    s = (np.array([0.35, 0.45, 0.55]), np.array([0.40, 0.50, 0.45]), np.array([0.45, 0.35, 0.50]))
+    cat = O.Catalog(scalars=[0], shepard=[1], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])
+    out = orc.interp_points(*s, cat, strategy=strategy, hmode=O.H_NEAREST)
+    for i in range(3):
+        p = [s[0][i], s[1][i], s[2][i]]
+        assert out[0][i] == pytest.approx(sum(p), abs=2e-2, rel=1e-2)
+        for k in (1, 2, 3):
+            assert out[k][i] == pytest.approx(1.0, abs=6e-2, rel=1e-2)
+        assert out[4][i] == pytest.approx(3.0, abs=1e-1, rel=2e-2)
+        for k in (5, 6, 7):
+            assert out[k][i] == pytest.approx(0.0, abs=5e-2)
+
+
+@pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])
+def test_uniform_field_div_curl_vanish(strategy):
+    x = np.array([0.0, 0.05, 0.11, -0.08])
+    y = np.array([0.02, -0.03, 0.04, 0.01])
+    z = np.array([0.0, 0.01, -0.02, 0.03])
+    n = 4
+    cols = [np.full(n, 1.0), np.full(n, -2.0), np.full(n, 0.5)]
+    orc = O.Oracle(x, y, z, np.ones(n), np.full(n, 0.12), np.ones(n), cols)
+    cat = O.Catalog(divs=[0, 1, 2], curls=[0, 1, 2])
+    out = orc.interp_points(x[:1], y[:1], z[:1], cat, strategy=strategy, hmode=O.H_PER_SAMPLE, hs=[0.12])
+    for o in out:
+        assert abs(o[0]) <= 1e-12
+
+
+def test_empty_neighbourhood_semantics():
+    P, cols = fixture_points()
+    orc = make_oracle(P, cols)
+    far = (np.array([9.0]), np.array([9.0]), np.array([9.0]))
+    cat = O.Catalog(scalars=[0], shepard=[1], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])
+    out = orc.interp_points(*far, cat, strategy=O.SCATTER)
+    assert all(math.isnan(o[0]) for o in out)
+    assert orc.density(*far, strategy=O.SCATTER)[0] == 0.0
+    lo = orc.interp_lines(far, (np.array([1.0]), np.array([0.0]), np.array([0.0])), scalars=[0], strategy=O.SCATTER)
+    assert math.isnan(lo[0][0])
+
+
+def test_density_kernel_matches_brute_force():
+    P, cols = lattice(8)
+    orc = make_oracle(P, cols)
+    rng = np.random.default_rng(5)
+    s = tuple(rng.uniform(0.1, 0.9, 10) for _ in range(3))
+    ha = rng.uniform(0.1, 0.2, 10)
+    got = orc.density(*s, strategy=O.GATHER, hmode=O.H_PER_SAMPLE, hs=ha)
+    for i in range(10):
+        p = np.array([s[0][i], s[1][i], s[2][i]])
+        sel, d, r, hb = B._neighbours(P, p, ha[i], "gather")
+        assert got[i] == pytest.approx(np.sum(P["m"][sel] * B.W(r, ha[i])), rel=1e-12)

@@ -259,6 +259,35 @@ int psb_neighbor_digest(psb_ctx* ctx, int32_t kind, int64_t ns,
                         int64_t* count_out, uint64_t* hash_out, void* ha_out,
                         uint32_t flags);
 
+/* ---- interpolation without device allocation -------------------------------- */
+
+/* No counterpart in the reference: an addition of this library.
+ * psb_interp_points with PSB_FLAG_DEVICE_PTRS semantics (sx, sy, sz, hs and
+ * every out[k] are device pointers) that allocates no device memory.  It is
+ * for callers that cannot allocate while they interpolate: a host whose device
+ * memory is held by another framework's caching pool, where a cudaMalloc in
+ * mid-step can fail; a pipeline with a memory budget fixed at start-up; a
+ * caller that cannot take the device-wide synchronisation of a cudaFree.  Its
+ * per-call scratch (sample Morton order and counters) is one file-scope device
+ * array of PSB_NOALLOC_SCRATCH_BYTES, resident on every GPU that loads the
+ * library.
+ *  - ns <= PSB_NOALLOC_MAX_SAMPLES, else PSB_EINVAL (split the call);
+ *  - the first call on a device looks the array's address up once, with that
+ *    device current; make it before any stream capture begins;
+ *  - all calls on a device share the array: calls whose GPU work overlaps
+ *    (several streams or contexts on one device) race and must be serialised
+ *    by the caller;
+ *  - particles and LBVH must already be on the device (psb_set_particles and
+ *    psb_build_lbvh allocate; this call does not).
+ * Results equal psb_interp_points' for the same arguments. */
+#define PSB_NOALLOC_MAX_SAMPLES 262144
+#define PSB_NOALLOC_SCRATCH_BYTES (8u << 20)
+int psb_interp_points_noalloc(psb_ctx* ctx, int64_t ns,
+                              const void* sx, const void* sy, const void* sz,
+                              psb_hmode hmode, const void* hs, psb_strategy strategy,
+                              const psb_catalog* cat, psb_precision prec,
+                              void* const* out, psb_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,11 @@ cudaError_t inclusive_max_scan_i64(int64_t* data, int64_t n, psb_ctx* c, int slo
 // Stable LSD radix sort of (key, value) pairs on the low `bits` bits of key.
 // Results end in keys/vals (the alternates are scratch).
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches);
+// The same sort on caller-provided scratch of at least
+// radix_sort_pairs_scratch_bytes(n) bytes (256-byte aligned); allocates nothing.
+size_t radix_sort_pairs_scratch_bytes(int64_t n);
+cudaError_t radix_sort_pairs_in(uint64_t* keys, uint32_t* vals, int64_t n, void* scratch_space, size_t bytes,
+                                cudaStream_t s, int* launches);
 
 template <class T> TreeView<T> tree_view(psb_ctx* c);
 

@@ -278,4 +278,90 @@ cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx*
     return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// The same sort on caller-provided scratch (no allocation).  Used by the
+// no-allocation interpolation entry point; the scratch layout is
+//   [vary (8 B) | alternate keys | alternate values | digit counts | scan partials]
+// each part 256-byte aligned.
+// ---------------------------------------------------------------------------
+namespace {
+inline size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t scan_partials_bytes(int64_t n) {
+    size_t total = 0;
+    while (n > SCAN_TILE) {
+        n = (n + SCAN_TILE - 1) / SCAN_TILE;
+        total += al256(sizeof(uint32_t) * n);
+    }
+    return total;
+}
+
+cudaError_t scan_u32_in(const uint32_t* in, uint32_t* out, int64_t n, char* part_space, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    int64_t nb = (n + SCAN_TILE - 1) / SCAN_TILE;
+    if (nb == 1) {
+        k_tile_scan<uint32_t, OpSum><<<1, SCAN_THREADS, 0, s>>>(in, out, n, nullptr, OpSum(), 0u, false);
+        return cudaGetLastError();
+    }
+    uint32_t* part = (uint32_t*)part_space;
+    k_tile_reduce<uint32_t, OpSum><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, part, OpSum(), 0u);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    e = scan_u32_in(part, part, nb, part_space + al256(sizeof(uint32_t) * nb), s);
+    if (e != cudaSuccess) return e;
+    k_tile_scan<uint32_t, OpSum><<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, out, n, part, OpSum(), 0u, false);
+    return cudaGetLastError();
+}
+}  // namespace
+
+size_t radix_sort_pairs_scratch_bytes(int64_t n) {
+    const int64_t nblocks = (n + RS_TILE - 1) / RS_TILE;
+    return al256(8) + al256(sizeof(uint64_t) * n) + al256(sizeof(uint32_t) * n) +
+           al256(sizeof(uint32_t) * 256 * nblocks) + scan_partials_bytes(256 * nblocks);
+}
+
+cudaError_t radix_sort_pairs_in(uint64_t* keys, uint32_t* vals, int64_t n, void* scratch_space, size_t bytes,
+                                cudaStream_t s, int* launches) {
+    if (n <= 1) return cudaSuccess;
+    if (bytes < radix_sort_pairs_scratch_bytes(n)) return cudaErrorInvalidValue;
+    char* sp = (char*)scratch_space;
+    unsigned long long* d_or = (unsigned long long*)sp;
+    sp += al256(8);
+    uint64_t* kalt = (uint64_t*)sp;
+    sp += al256(sizeof(uint64_t) * n);
+    uint32_t* valt = (uint32_t*)sp;
+    sp += al256(sizeof(uint32_t) * n);
+    const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
+    uint32_t* cnt = (uint32_t*)sp;
+    sp += al256(sizeof(uint32_t) * 256 * (size_t)nblocks);
+    char* parts = sp;
+
+    cudaError_t e = cudaMemsetAsync(d_or, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    k_key_xor_or<<<grid, 256, 0, s>>>(keys, n, d_or);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    unsigned long long vary = 0;
+    if ((e = cudaMemcpyAsync(&vary, d_or, sizeof(vary), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+    if (launches) *launches += 1;
+    uint64_t* ksrc = keys; uint32_t* vsrc = vals;
+    uint64_t* kdst = kalt; uint32_t* vdst = valt;
+    for (int shift = 0; shift < 64; shift += 8) {
+        if (((vary >> shift) & 255ull) == 0) continue;
+        k_rs_count<<<nblocks, RS_THREADS, 0, s>>>(ksrc, n, shift, cnt, nblocks);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if ((e = scan_u32_in(cnt, cnt, (int64_t)256 * nblocks, parts, s)) != cudaSuccess) return e;
+        k_rs_scatter<<<nblocks, RS_THREADS, 0, s>>>(ksrc, vsrc, kdst, vdst, n, shift, cnt, nblocks);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (launches) *launches += 4;
+        std::swap(ksrc, kdst); std::swap(vsrc, vdst);
+    }
+    if (ksrc != keys) {
+        if ((e = cudaMemcpyAsync(keys, ksrc, sizeof(uint64_t) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(vals, vsrc, sizeof(uint32_t) * n, cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 }  // namespace psb

@@ -29,6 +29,7 @@ PSB_PREC_FP64, PSB_PREC_FP32C = 0, 1
 PSB_H_NEAREST, PSB_H_PER_SAMPLE, PSB_H_CONSTANT = 0, 1, 2
 PSB_FLAG_DEVICE_PTRS = 1
 PSB_FLAG_FP32C_DECISIONS = 0x100
+PSB_NOALLOC_MAX_SAMPLES = 262144
 
 
 class PsbError(RuntimeError):
@@ -72,6 +73,8 @@ _SIGS = {
     "psb_build_lbvh": ([_vp, _vp, _vp], C.c_int),
     "psb_get_tree": ([_vp] * 9, C.c_int),
     "psb_interp_points": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp], C.c_int),
+    "psb_interp_points_noalloc": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
+                                  C.c_int),
     "psb_interp_grid": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp],
                         C.c_int),
     "psb_interp_box": ([_vp, _vp, _vp, _i64, _i64, _i64, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp],

@@ -61,28 +61,63 @@ def ncu_traffic():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region through NVML (read-only queries, every 10 ms); nvidia-smi when NVML
+    is unavailable."""
 
-    def __init__(self, index=0):
-        self.index = index
-        self.samples = []
+    REASONS = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown")]
+
+    def __init__(self, cuda_index=0):
+        self.cuda_index = cuda_index
+        self.samples = []   # (sm_mhz, max_mhz, [reasons])
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        self._h = None
+        try:
+            import pynvml
+            import torch
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(cuda_index)
+            try:
+                self._h = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+            except Exception:
+                bus = "%08x:%02x:%02x.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+                self._h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            self._nvml = pynvml
+        except Exception:
+            self._nvml = None
 
-    def _run(self):
-        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    def _sample_nvml(self):
+        nv = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(self._h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        rs = [name for name, const in self.REASONS if bits & getattr(nv, const, 0)]
+        self.samples.append((float(sm), float(mx), rs))
+
+    def _sample_smi(self):
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
+        out = subprocess.run(["nvidia-smi", "-i", str(self.cuda_index), f"--query-gpu={q}",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+        v = [x.strip() for x in out.stdout.strip().split(",")]
+        if len(v) >= 6:
+            rs = [self.REASONS[k][0] for k in range(4) if v[2 + k].lower() == "active"]
+            self.samples.append((float(v[0]), float(v[1]), rs))
+
+    def _run(self):
         while not self._stop.is_set():
             try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                v = [s.strip() for s in out.stdout.strip().split(",")]
-                if len(v) >= 7:
-                    self.samples.append(v)
+                self._sample_nvml() if self._nvml else self._sample_smi()
             except Exception:
                 pass
-            self._stop.wait(0.2)
+            self._stop.wait(0.01 if self._nvml else 0.2)
 
     def __enter__(self):
         self._t = threading.Thread(target=self._run, daemon=True)
@@ -96,20 +131,17 @@ class ClockSampler:
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for s in self.samples for k in range(4) if s[3 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(s[1] for s in self.samples),
+                "sm_mhz_min": min(sm), "reasons": sorted({r for s in self.samples for r in s[2]}),
+                "samples": len(self.samples), "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def make_workload():
     from partia_b200 import workloads as W
-    d = W.plummer_c2()
-    axis = np.linspace(-0.5, 0.5, NGRID)  # replaced by the LinRange values below
     from partia_b200 import linrange
+    d = W.plummer_c2()
     axis = linrange(-0.5, 0.5, NGRID)
     return d, axis
 
@@ -159,7 +191,7 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Plummer sphere, N=2e6)",
-            "config": {"workload": "plummer-2M symmetric rho,grad rho,div A,curl A on 128^3 grid", "N": 2_000_000,
+            "config": {"workload": f"plummer-2M symmetric rho,grad rho,div A,curl A on {NGRID}^3 grid", "N": 2_000_000,
                        "samples": NGRID ** 3},
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
@@ -167,15 +199,19 @@ def run_reference(args):
 
 
 def main():
+    global NGRID
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--grid", type=int, default=NGRID, help="grid points per axis (128 = the workload; smaller "
+                    "values only for profiling captures)")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     args = ap.parse_args()
+    NGRID = args.grid
     if args.impl == "reference":
         run_reference(args)
         return
@@ -202,6 +238,11 @@ def main():
     cols = [d["rho"], d["Ax"], d["Ay"], d["Az"]]
     ctx.set_particles(d["x"], d["y"], d["z"], d["m"], d["h"], d["rho"], cols)
     ctx.build(want_perm=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ctx.build(want_perm=False)  # second build: module loading excluded
+    torch.cuda.synchronize()
+    build_ms = (time.perf_counter() - t0) * 1e3
     cat = CatalogC(**CATALOG)
 
     # this rank's slab of z-planes (samples shard; particles and LBVH are replicated)
@@ -300,6 +341,9 @@ def main():
     # roofline of the point kernel (algorithmic bytes per launch)
     hbm, peak_kind = peaks()
     kern_ms = float(np.median(kern32))
+    # grid coordinates are generated on the device (S_in = 0); outputs are
+    # written in the input element type (f64, 8 B); the FP32C pair record is
+    # (x, y, z, h, m, rho + the catalog's columns) in float
     b_alg = ns * (0 + L_OUT * 8) + pairs * (6 + NCOL_USED) * 4
     achieved = b_alg / (kern_ms / 1e3) / 1e9
     tr = ncu_traffic()
@@ -317,7 +361,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": tot.item() / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
             "data": "synthetic (seeded Plummer sphere, N=2e6, numpy PCG64 seed 1)",
-            "config": {"workload": "plummer-2M symmetric rho,grad rho,div A,curl A on 128^3 grid",
+            "config": {"workload": f"plummer-2M symmetric rho,grad rho,div A,curl A on {NGRID}^3 grid",
                        "N": 2_000_000, "samples": NGRID ** 3, "fields": L_OUT, "strategy": "symmetric",
                        "h": "nearest particle", "precision": "FP32C", "l2": "flushed (256 MB write) between steps"},
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * ns,
@@ -330,6 +374,7 @@ def main():
                          "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg),
                          "warp_steps_per_launch": int(ctx_steps)},
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs, "grad_fwd_time_ratio": None,
+            "build_ms": build_ms,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

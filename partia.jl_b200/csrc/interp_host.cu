@@ -218,7 +218,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
         }
     } else {
         if (dev) {
-            for (int q = 0; q < L; ++q) A.out[q] = (T*)out[q];
+            for (int q = 0; ns > 0 && q < L; ++q) A.out[q] = (T*)out[q];
         } else if (ns > 0 && L > 0) {
             obuf = (char*)scratch(c, 2, es * ns * L);
             if (!obuf) return fail(c, PSB_ENOMEM, "scratch allocation failed (outputs)");

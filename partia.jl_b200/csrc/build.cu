@@ -285,7 +285,7 @@ __global__ void k_pack_nodes(int64_t nint, const T* mnx, const T* mny, const T* 
 // the exact coordinates (anchor 0).
 template <class T>
 __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, const T* h, const T* m, const T* rho,
-                              float4* leaf4, double* anchor, float* mrho, float* mf) {
+                              float4* leaf4, double* anchor, float* mrho, float* mf, float4* leafK) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     int64_t t0 = i & ~(int64_t)31;
@@ -300,8 +300,13 @@ __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, con
         r = make_float4((float)x[i], (float)y[i], (float)z[i], (float)h[i]);
     }
     leaf4[i] = r;
-    mrho[i] = (float)((double)m[i] / (double)rho[i]);
+    const float mr = (float)((double)m[i] / (double)rho[i]);
+    mrho[i] = mr;
     mf[i] = (float)m[i];
+    // kernel-weight factors of the float pair bodies
+    const float ih = 1.f / r.w;
+    const float s3 = 0.318309886183790671538f * ih * ih * ih;
+    leafK[i] = make_float4(ih, s3, s3 * ih, mr);
 }
 
 __global__ void k_to_float(const double* src, int64_t n, float* dst) {
@@ -406,12 +411,13 @@ static int build_typed(psb_ctx* c) {
     PSB_CUDA_TRY(c, cudaMalloc(&c->anchor, sizeof(double) * 3 * ntile), "cudaMalloc anchor");
     PSB_CUDA_TRY(c, cudaMalloc(&c->mrho, sizeof(float) * n), "cudaMalloc mrho");
     PSB_CUDA_TRY(c, cudaMalloc(&c->mf, sizeof(float) * n), "cudaMalloc mf");
+    PSB_CUDA_TRY(c, cudaMalloc(&c->leafK, sizeof(float4) * n), "cudaMalloc leafK");
     if (nint > 0)
         k_pack_nodes<T><<<grid_for(nint), BT, 0, s>>>(nint, (const T*)c->nmin[0], (const T*)c->nmin[1],
                                                       (const T*)c->nmin[2], (const T*)c->nmax[0], (const T*)c->nmax[1],
                                                       (const T*)c->nmax[2], (const T*)c->nscale, c->node_lo, c->node_hi);
     k_pack_leaves<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->x, (const T*)c->y, (const T*)c->z, (const T*)c->h,
-                                                (const T*)c->m, (const T*)c->rho, c->leaf4, c->anchor, c->mrho, c->mf);
+                                                (const T*)c->m, (const T*)c->rho, c->leaf4, c->anchor, c->mrho, c->mf, c->leafK);
     if (sizeof(T) == 8 && c->ncol > 0) {
         PSB_CUDA_TRY(c, cudaMalloc(&c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
         for (int k = 0; k < c->ncol; ++k)

@@ -19,7 +19,7 @@ int cuda_fail(psb_ctx* c, cudaError_t e, const char* what) {
 }
 
 void* scratch(psb_ctx* c, int k, size_t bytes) {
-    if (k < 0 || k >= 16) return nullptr;
+    if (k < 0 || k >= (int)(sizeof(c->scratch) / sizeof(c->scratch[0]))) return nullptr;
     auto& sl = c->scratch[k];
     if (sl.bytes >= bytes && sl.p) return sl.p;
     if (sl.p) {
@@ -54,7 +54,7 @@ void free_tree(psb_ctx* c) {
     for (int d = 0; d < 3; ++d) { dfree(c->nmin[d]); dfree(c->nmax[d]); }
     dfree(c->nscale);
     dfree_t(c->node_lo); dfree_t(c->node_hi); dfree_t(c->leaf4);
-    dfree_t(c->anchor); dfree_t(c->mrho); dfree_t(c->mf); dfree_t(c->colsf);
+    dfree_t(c->anchor); dfree_t(c->mrho); dfree_t(c->mf); dfree_t(c->leafK); dfree_t(c->colsf);
     c->built = false;
     c->root = 0;
 }

@@ -24,6 +24,23 @@
 
 namespace psb {
 
+// Buffers of the two-kernel point path (one batch of tiles): the collect
+// kernel writes, for every sample, its accepted leaves as (first leaf, mask)
+// entries of up to 32 consecutive leaves, and its smoothing length; the body
+// kernel reads them.  A tile with a sample of more than RCAP entries is
+// marked (cnt = 0xFF for all its lanes) and listed in ovf_tiles; the
+// single-kernel path computes those tiles instead.
+constexpr int RCAP = 32;
+struct SplitBufs {
+    uint2* ent;          // [tile][RCAP][32]
+    uint8_t* cnt;        // [tile][32]
+    void* ha;            // [tile][32], element type T
+    int32_t* ovf_tiles;  // absolute tile ids
+    unsigned* ovf_count;
+    int64_t tile0;       // first tile of the batch
+    int64_t ntiles;      // tiles in the batch
+};
+
 template <class T> struct Args {
     TreeView<T> tv;
     SampleSrc<T> src;
@@ -40,6 +57,10 @@ template <class T> struct Args {
     const float* lut_f;
     unsigned* err;
     unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests, [2] traversal steps
+    SplitBufs sp;
+    // single-kernel path over a device list of tiles (nullptr: every tile)
+    const int32_t* tile_list;
+    const unsigned* tile_count;
 };
 
 // ---------------------------------------------------------------------------

@@ -44,6 +44,156 @@ template <class T, int KC> struct PStage<T, true, KC> {
     float thr[SPAN];    // nearest search: candidate threshold on the float d2
 };
 
+// Output fields of one sample from its sums (general_interpolation.jl:128-214):
+// NaN everywhere when S1 = 0, then each recipe op in catalog order.
+template <class T, class Acc, class CT, int KC>
+__device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k, const Acc& S1, const Acc (&G)[3],
+                                                     const Acc (&Sw)[KC], const Acc (&Sg)[KC][3], const Acc& Dm,
+                                                     const Acc (&Dg)[3], const CT (&a0)[KC]) {
+    const double s1 = S1.get();
+    const int L = A.rec.L;
+    if (s1 == 0.0) {
+        for (int o = 0; o < L; ++o) A.out[o][k] = qnan<T>();
+    } else {
+        // sums of (A - A0) w and (A - A0) g; gradients, divergences and
+        // curls are invariant under the shift, scalars add A0 back.
+        double sw[MAX_KC], sg[MAX_KC][3], sh[MAX_KC];
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            sw[c] = Sw[c].get();
+            sh[c] = (double)a0[c];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
+        }
+        const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
+        const double inv = 1.0 / s1;
+        for (int o = 0; o < L; ++o) {
+            const int op = A.rec.op[o];
+            const int a0i = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
+            double v;
+            if (op == OP_SCALAR) {
+                v = a1 ? sw[a0i] * inv + sh[a0i] : sw[a0i] + sh[a0i] * s1;
+            } else if (op == OP_GRADC) {
+                v = sg[a0i][a1] - g[a1] * (sw[a0i] * inv);
+            } else if (op == OP_GRADD) {
+                v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
+            } else if (op == OP_DIV) {
+                double f = sg[a0i][0] + sg[a1][1] + sg[a2][2];
+                double b = (sw[a0i] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
+                v = f - b;
+            } else {  // OP_CURL, component a3
+                double Ax = sw[a0i] * inv, Ay = sw[a1] * inv, Az = sw[a2] * inv;
+                double f, b;
+                if (a3 == 0) { f = sg[a1][2] - sg[a2][1]; b = Ay * g[2] - Az * g[1]; }
+                else if (a3 == 1) { f = sg[a2][0] - sg[a0i][2]; b = Az * g[0] - Ax * g[2]; }
+                else { f = sg[a0i][1] - sg[a1][0]; b = Ax * g[1] - Ay * g[0]; }
+                v = -(f - b);
+            }
+            A.out[o][k] = (T)v;
+        }
+    }
+}
+
+// LBVH_find_nearest_h (LinearBVHQueries.jl:118-140) for the warp's samples:
+// the smoothing length of the nearest particle, NaN without particles.  The
+// reference starts its search with an infinite bound.  Here the bound starts
+// at the exact distance to the particle next to the sample in Morton order
+// (found by binary search of the sorted codes), and ties are resolved towards
+// the smaller leaf index, so the result is the same argmin -- the first leaf
+// in DFS order with the minimum distance.  stage_span(lo, cnt, false) stages
+// the positions of leaves [lo, lo+cnt) in st (Q and eq for float tests, x y z
+// otherwise); st.P / st.px.. hold the samples.
+template <class T, bool BAND, class Stage, class StageSpan>
+__device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, StageSpan& stage_span, int lane,
+                                            bool valid, const T p[3], const float pf[3], float pem, int32_t start,
+                                            int64_t& steps, bool& ok) {
+    double best = INFINITY;
+    int64_t bidx = -1;
+    if (valid) {
+        uint64_t q[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            double f = ((double)p[d] - tv.qlo[d]) * tv.qscale[d];
+            f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
+            q[d] = (uint64_t)f;
+        }
+        const uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
+        int64_t lo = 0, hi = tv.n;  // first index with codes[i] >= code
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (__ldg(&tv.codes[mid]) < code) lo = mid + 1;
+            else hi = mid;
+        }
+        const int64_t c0 = lo > 0 ? lo - 1 : 0;
+        const int64_t c1 = lo < tv.n ? lo : tv.n - 1;
+        const double d0 = (double)ex_d2_pp<T>(p, tv.x[c0], tv.y[c0], tv.z[c0]);
+        const double d1 = (double)ex_d2_pp<T>(p, tv.x[c1], tv.y[c1], tv.z[c1]);
+        if (d1 < d0) { best = d1; bidx = c1; } else { best = d0; bidx = c0; }
+    }
+    auto better = [&](double d2, int64_t li) { return d2 < best || (d2 == best && li < bidx); };
+    auto node_fn = [&](int ni) -> bool {
+        if constexpr (BAND) {
+            float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
+            return !((double)lb > best);
+        } else {
+            return !((double)ex_d2_pbox<T>(p, tv, ni) > best);
+        }
+    };
+    auto span_fn = [&](int64_t lo, int cnt, bool part) {
+        float eqmax = stage_span(lo, cnt, false);
+        const unsigned parts = __ballot_sync(PSB_FULL, part);
+        if (!parts) return;
+        unsigned cand = 0;
+        if constexpr (BAND) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) eqmax = fmaxf(eqmax, __shfl_xor_sync(PSB_FULL, eqmax, o));
+            // candidates: float d2 not above (sqrt(best) + error)^2
+            {
+                const float4 Pme = st.P[lane];
+                float bs = (float)sqrt(best);
+                float e = 1.7320508f * (Pme.w + eqmax) + 4.f * U1 * bs + 1e-30f;
+                float t = (bs + e) * (1.f + 4.f * U1);
+                st.thr[lane] = isinf(best) ? INFINITY : t * t;
+            }
+            __syncwarp();
+            const float4 Q = st.Q[lane < cnt ? lane : 0];
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const float4 P = st.P[s];
+                const float thr = st.thr[s];
+                float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                bool c = (lane < cnt) && (dx * dx + dy * dy + dz * dz <= thr);
+                unsigned b = __ballot_sync(PSB_FULL, c);
+                if (lane == s) cand = b;
+            }
+            for (; cand; cand &= cand - 1) {
+                const int64_t li = lo + __ffs(cand) - 1;
+                double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                if (better(d2, li)) { best = d2; bidx = li; }
+            }
+        } else {
+            st.best[lane] = (T)best;
+            __syncwarp();
+            const int j = lane < cnt ? lane : 0;
+            const T xj = st.x[j], yj = st.y[j], zj = st.z[j];
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
+                bool c = (lane < cnt) && (ex_d2_pp<T>(ps, xj, yj, zj) <= st.best[s]);
+                unsigned b = __ballot_sync(PSB_FULL, c);
+                if (lane == s) cand = b;
+            }
+            for (; cand; cand &= cand - 1) {
+                const int jj = __ffs(cand) - 1;
+                double d2 = (double)ex_d2_pp<T>(p, st.x[jj], st.y[jj], st.z[jj]);
+                if (better(d2, lo + jj)) { best = d2; bidx = lo + jj; }
+            }
+        }
+    };
+    ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+    return valid ? ((bidx >= 0) ? tv.h[bidx] : qnan<T>()) : T(0);
+}
+
 template <class T, int PREC, int ST, int KC, int WHAT>
 __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
@@ -55,8 +205,13 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     auto& st = stage_all[wib];
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
-    if (tile >= A.src.ntiles) return;  // warp-uniform
+    int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (A.tile_list) {  // the tiles the two-kernel path handed back
+        if (tile >= (int64_t)*A.tile_count) return;
+        tile = A.tile_list[tile];
+    } else if (tile >= A.src.ntiles) {
+        return;  // warp-uniform
+    }
 
     const int64_t k = sample_of(A.src, tile, lane);
     const bool valid = k >= 0;
@@ -118,99 +273,10 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     };
 
     // ---- sample smoothing length (LBVH_find_nearest_h or given) ----
-    // The reference starts its nearest search with an infinite bound.  Here the
-    // bound starts at the exact distance to the particle next to the sample
-    // in Morton order (found by binary search of the sorted codes), and ties
-    // are resolved towards the smaller leaf index, so the result is the same
-    // argmin -- the first leaf in DFS order with the minimum distance.
     T ha = T(0);
     if (ST != ST_SCATTER) {
         if (A.hmode == PSB_H_NEAREST) {
-            double best = INFINITY;
-            int64_t bidx = -1;
-            if (valid) {
-                uint64_t q[3];
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    double f = ((double)p[d] - tv.qlo[d]) * tv.qscale[d];
-                    f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
-                    q[d] = (uint64_t)f;
-                }
-                const uint64_t code = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
-                int64_t lo = 0, hi = tv.n;  // first index with codes[i] >= code
-                while (lo < hi) {
-                    int64_t mid = (lo + hi) >> 1;
-                    if (__ldg(&tv.codes[mid]) < code) lo = mid + 1;
-                    else hi = mid;
-                }
-                const int64_t c0 = lo > 0 ? lo - 1 : 0;
-                const int64_t c1 = lo < tv.n ? lo : tv.n - 1;
-                const double d0 = (double)ex_d2_pp<T>(p, tv.x[c0], tv.y[c0], tv.z[c0]);
-                const double d1 = (double)ex_d2_pp<T>(p, tv.x[c1], tv.y[c1], tv.z[c1]);
-                if (d1 < d0) { best = d1; bidx = c1; } else { best = d0; bidx = c0; }
-            }
-            auto better = [&](double d2, int64_t li) { return d2 < best || (d2 == best && li < bidx); };
-            auto node_fn = [&](int ni) -> bool {
-                if constexpr (BAND) {
-                    float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
-                    return !((double)lb > best);
-                } else {
-                    return !((double)ex_d2_pbox<T>(p, tv, ni) > best);
-                }
-            };
-            auto span_fn = [&](int64_t lo, int cnt, bool part) {
-                float eqmax = stage_span(lo, cnt, false);
-                const unsigned parts = __ballot_sync(PSB_FULL, part);
-                if (!parts) return;
-                unsigned cand = 0;
-                if constexpr (BAND) {
-#pragma unroll
-                    for (int o = 16; o > 0; o >>= 1) eqmax = fmaxf(eqmax, __shfl_xor_sync(PSB_FULL, eqmax, o));
-                    // candidates: float d2 not above (sqrt(best) + error)^2
-                    {
-                        const float4 Pme = st.P[lane];
-                        float bs = (float)sqrt(best);
-                        float e = 1.7320508f * (Pme.w + eqmax) + 4.f * U1 * bs + 1e-30f;
-                        float t = (bs + e) * (1.f + 4.f * U1);
-                        st.thr[lane] = isinf(best) ? INFINITY : t * t;
-                    }
-                    __syncwarp();
-                    const float4 Q = st.Q[lane < cnt ? lane : 0];
-                    for (unsigned pp = parts; pp; pp &= pp - 1) {
-                        const int s = __ffs(pp) - 1;
-                        const float4 P = st.P[s];
-                        const float thr = st.thr[s];
-                        float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
-                        bool c = (lane < cnt) && (dx * dx + dy * dy + dz * dz <= thr);
-                        unsigned b = __ballot_sync(PSB_FULL, c);
-                        if (lane == s) cand = b;
-                    }
-                    for (; cand; cand &= cand - 1) {
-                        const int64_t li = lo + __ffs(cand) - 1;
-                        double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                        if (better(d2, li)) { best = d2; bidx = li; }
-                    }
-                } else {
-                    st.best[lane] = (T)best;
-                    __syncwarp();
-                    const int j = lane < cnt ? lane : 0;
-                    const T xj = st.x[j], yj = st.y[j], zj = st.z[j];
-                    for (unsigned pp = parts; pp; pp &= pp - 1) {
-                        const int s = __ffs(pp) - 1;
-                        const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
-                        bool c = (lane < cnt) && (ex_d2_pp<T>(ps, xj, yj, zj) <= st.best[s]);
-                        unsigned b = __ballot_sync(PSB_FULL, c);
-                        if (lane == s) cand = b;
-                    }
-                    for (; cand; cand &= cand - 1) {
-                        const int jj = __ffs(cand) - 1;
-                        double d2 = (double)ex_d2_pp<T>(p, st.x[jj], st.y[jj], st.z[jj]);
-                        if (better(d2, lo + jj)) { best = d2; bidx = lo + jj; }
-                    }
-                }
-            };
-            ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
-            if (valid) ha = (bidx >= 0) ? tv.h[bidx] : qnan<T>();
+            ha = nearest_h_pass<T, BAND>(tv, st, stage_span, lane, valid, p, pf, pem, start, steps, ok);
         } else if (valid) {
             ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
         }
@@ -628,48 +694,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         } else if (WHAT == WHAT_DENSITY) {
             A.out[0][k] = (T)dens;
         } else {
-            const double s1 = S1.get();
-            const int L = A.rec.L;
-            if (s1 == 0.0) {
-                for (int o = 0; o < L; ++o) A.out[o][k] = qnan<T>();
-            } else {
-                // sums of (A - A0) w and (A - A0) g; gradients, divergences and
-                // curls are invariant under the shift, scalars add A0 back.
-                double sw[MAX_KC], sg[MAX_KC][3], sh[MAX_KC];
-#pragma unroll
-                for (int c = 0; c < KC; ++c) {
-                    sw[c] = Sw[c].get();
-                    sh[c] = (double)a0[c];
-#pragma unroll
-                    for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
-                }
-                const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
-                const double inv = 1.0 / s1;
-                for (int o = 0; o < L; ++o) {
-                    const int op = A.rec.op[o];
-                    const int a0i = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
-                    double v;
-                    if (op == OP_SCALAR) {
-                        v = a1 ? sw[a0i] * inv + sh[a0i] : sw[a0i] + sh[a0i] * s1;
-                    } else if (op == OP_GRADC) {
-                        v = sg[a0i][a1] - g[a1] * (sw[a0i] * inv);
-                    } else if (op == OP_GRADD) {
-                        v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
-                    } else if (op == OP_DIV) {
-                        double f = sg[a0i][0] + sg[a1][1] + sg[a2][2];
-                        double b = (sw[a0i] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
-                        v = f - b;
-                    } else {  // OP_CURL, component a3
-                        double Ax = sw[a0i] * inv, Ay = sw[a1] * inv, Az = sw[a2] * inv;
-                        double f, b;
-                        if (a3 == 0) { f = sg[a1][2] - sg[a2][1]; b = Ay * g[2] - Az * g[1]; }
-                        else if (a3 == 1) { f = sg[a2][0] - sg[a0i][2]; b = Az * g[0] - Ax * g[2]; }
-                        else { f = sg[a0i][1] - sg[a1][0]; b = Ax * g[1] - Ay * g[0]; }
-                        v = -(f - b);
-                    }
-                    A.out[o][k] = (T)v;
-                }
-            }
+            write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
         }
     }
     // ---- statistics and errors ----

@@ -1,0 +1,439 @@
+// k_split.cuh -- the two-kernel point path.
+//
+// k_collect walks the LBVH for a tile of 32 samples (one warp, the same walk,
+// spans and inclusion decisions as k_points) and records, per sample, the
+// accepted leaves as (first leaf, 32-bit mask) entries plus the sample's
+// smoothing length.  It keeps no accumulators, so it runs with few registers.
+// k_bodies then evaluates the kernel weights and sums of every recorded pair:
+// each lane runs through its own sample's list in one flattened loop, so a
+// warp iteration does 32 pair bodies until the shortest lists run out, instead
+// of idling lanes once per span.  Pairs are visited in the same order as in
+// k_points (span order, then leaf order), with the same arithmetic.
+#pragma once
+
+#include "k_points.cuh"
+
+namespace psb {
+
+template <class T, bool BAND> struct CStage {
+    T x[SPAN], y[SPAN], z[SPAN], h[SPAN];
+    T px[SPAN], py[SPAN], pz[SPAN], ra2[SPAN], best[SPAN];
+};
+template <class T> struct CStage<T, true> {
+    float4 Q[SPAN];   // leaf position relative to the warp anchor, h
+    float eq[SPAN];   // error bound of Q
+    float4 P[SPAN];   // sample position relative to the warp anchor, error bound
+    float2 R[SPAN];   // sample radius bounds
+    float2 AB[SPAN];  // per-span squared thresholds of each sample
+    float thr[SPAN];  // nearest search: candidate threshold
+};
+
+template <class T, int PREC, int ST>
+__global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
+    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
+    __shared__ CStage<T, BAND> stage_all[4];
+    const TreeView<T>& tv = A.tv;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    auto& st = stage_all[wib];
+    const int64_t bt = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (bt >= A.sp.ntiles) return;  // warp-uniform
+    const int64_t tile = A.sp.tile0 + bt;
+
+    const int64_t k = sample_of(A.src, tile, lane);
+    const bool valid = k >= 0;
+    T p[3] = {T(0), T(0), T(0)}, dd[3];
+    if (valid) sample_coords(A.src, k, p, dd);
+    const float pf[3] = {(float)p[0], (float)p[1], (float)p[2]};
+    const float pem = U1 * fmaxf(fmaxf(fabsf(pf[0]), fabsf(pf[1])), fabsf(pf[2])) + 1e-30f;
+    const int32_t start = (tv.root == 0) ? (int32_t)tv.n : tv.root;
+    unsigned long long n_pairs = 0, n_retest = 0, n_spans = 0, n_parts = 0;
+    int64_t steps = 0;
+    bool ok = true;
+
+    const unsigned vmask = __ballot_sync(PSB_FULL, valid);
+    const int first = vmask ? __ffs(vmask) - 1 : 0;
+    const double cw[3] = {__shfl_sync(PSB_FULL, (double)p[0], first), __shfl_sync(PSB_FULL, (double)p[1], first),
+                          __shfl_sync(PSB_FULL, (double)p[2], first)};
+    if constexpr (BAND) {
+        float sr[3] = {(float)((double)p[0] - cw[0]), (float)((double)p[1] - cw[1]), (float)((double)p[2] - cw[2])};
+        float es = U1 * (fabsf(sr[0]) + fabsf(sr[1]) + fabsf(sr[2])) + 1e-30f;
+        st.P[lane] = make_float4(sr[0], sr[1], sr[2], es);
+    } else {
+        st.px[lane] = p[0]; st.py[lane] = p[1]; st.pz[lane] = p[2];
+    }
+
+    // positions of leaves [lo, lo+cnt): lane j takes leaf lo+j (all lanes call)
+    auto stage_span = [&](int64_t lo, int cnt, bool) -> float {
+        __syncwarp();
+        float eqmax = 0.f;
+        if (lane < cnt) {
+            const int64_t li = lo + lane;
+            if constexpr (BAND) {
+                const float4 L = __ldg(&tv.leaf4[li]);
+                const int64_t t = li >> 5;
+                float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
+                float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
+                float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
+                st.Q[lane] = make_float4(q0, q1, q2, L.w);
+                eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
+                              fabsf(q0) + fabsf(q1) + fabsf(q2));
+                st.eq[lane] = eqmax;
+            } else {
+                st.x[lane] = __ldg(&tv.x[li]); st.y[lane] = __ldg(&tv.y[li]); st.z[lane] = __ldg(&tv.z[li]);
+                st.h[lane] = __ldg(&tv.h[li]);
+            }
+        }
+        __syncwarp();
+        return eqmax;
+    };
+
+    T ha = T(0);
+    if (ST != ST_SCATTER) {
+        if (A.hmode == PSB_H_NEAREST) {
+            ha = nearest_h_pass<T, BAND>(tv, st, stage_span, lane, valid, p, pf, pem, start, steps, ok);
+        } else if (valid) {
+            ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
+        }
+    }
+    const T ra = X<T>::mul(T(2), ha);
+    const T ra2 = X<T>::mul(ra, ra);
+    float ra2_hi = 0.f;
+    if constexpr (BAND) {
+        float ralo = 0.f, rahi = 0.f;
+        if (ST != ST_SCATTER) {
+            ralo = __double2float_rd((double)ra) * (1.f - 2.f * U1);
+            rahi = __double2float_ru((double)ra) * (1.f + 2.f * U1);
+            ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
+        }
+        st.R[lane] = make_float2(ralo, rahi);
+    } else {
+        st.ra2[lane] = ra2;
+    }
+
+    // this lane's pair list
+    uint2* ent = A.sp.ent + (size_t)bt * RCAP * 32 + lane;
+    int nent = 0;
+    bool ovf = false;
+    auto emit = [&](int64_t lo, unsigned acc) {
+        if (!acc) return;
+        n_pairs += __popc(acc);
+        if (nent < RCAP) {
+            ent[(size_t)nent * 32] = make_uint2((unsigned)lo, acc);
+            ++nent;
+        } else {
+            ovf = true;
+        }
+    };
+
+    auto node_fn = [&](int ni) -> bool {
+        if constexpr (BAND) {
+            float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
+            float lb = lb_d2_pbox(pf, pem, lo, hi);
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+        } else {
+            T d2n = ex_d2_pbox<T>(p, tv, ni);
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            return !(d2n > r2);
+        }
+    };
+
+    if constexpr (BAND) {
+        const float4 Pme = st.P[lane];
+        const float2 Rme = st.R[lane];
+        float esmax = Pme.w, rahimax = Rme.y;  // tile-wide maxima (sample error, sample radius)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            esmax = fmaxf(esmax, __shfl_xor_sync(PSB_FULL, esmax, o));
+            rahimax = fmaxf(rahimax, __shfl_xor_sync(PSB_FULL, rahimax, o));
+        }
+        auto span_fn = [&](int64_t lo, int cnt, bool part) {
+            const unsigned parts = __ballot_sync(PSB_FULL, part);
+            if (!parts) return;
+            float eq = 0.f, Aj = 0.f, Bj = 0.f, hb = 0.f;
+            __syncwarp();
+            if (lane < cnt) {
+                const int64_t li = lo + lane;
+                const float4 L = __ldg(&tv.leaf4[li]);
+                const int64_t t = li >> 5;
+                const float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
+                const float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
+                const float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                const float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
+                hb = L.w;
+                st.Q[lane] = make_float4(q0, q1, q2, hb);
+                eq = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
+                           fabsf(q0) + fabsf(q1) + fabsf(q2));
+            }
+            // error bound of float distances for this span, the same for every pair
+            float eqm = eq;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) eqm = fmaxf(eqm, __shfl_xor_sync(PSB_FULL, eqm, o));
+            const float rbhi = 2.f * hb * (1.f + 2.f * U1), rblo = 2.f * hb * (1.f - 2.f * U1);
+            float rmax = rahimax;
+            if (ST != ST_GATHER) {
+                float rb = rbhi;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) rb = fmaxf(rb, __shfl_xor_sync(PSB_FULL, rb, o));
+                rmax = fmaxf(rmax, rb);
+            }
+            const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
+            if (ST != ST_GATHER && lane < cnt) {
+                const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
+                Aj = il * il;
+                Bj = ih2 * ih2;
+            }
+            {
+                float As = 0.f, Bs = 0.f;
+                if (ST != ST_SCATTER) {
+                    const float il = fmaxf((Rme.x - E) * (1.f - 4.f * U1), 0.f), ih2 = (Rme.y + E) * (1.f + 4.f * U1);
+                    As = il * il;
+                    Bs = ih2 * ih2;
+                }
+                st.AB[lane] = make_float2(As, Bs);
+            }
+            __syncwarp();
+            const float4 Q = st.Q[lane < cnt ? lane : 0];
+            unsigned myacc = 0, myunc = 0;
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const float4 P = st.P[s];
+                const float2 AB = st.AB[s];
+                const float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                const bool in = (lane < cnt) && d2 < fmaxf(AB.x, Aj);
+                const bool un = (lane < cnt) && !in && !(d2 > fmaxf(AB.y, Bj));
+                const unsigned bi = __ballot_sync(PSB_FULL, in), bu = __ballot_sync(PSB_FULL, un);
+                if (lane == s) { myacc = bi; myunc = bu; }
+            }
+            // undecided pairs: the reference's double test
+            for (unsigned u = myunc; u; u &= u - 1) {
+                const int jj = __ffs(u) - 1;
+                const int64_t li = lo + jj;
+                ++n_retest;
+                T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
+                if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) myacc |= 1u << jj;
+            }
+            emit(lo, myacc);
+            ++n_spans;
+            n_parts += __popc(parts);
+        };
+        ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+    } else {
+        auto span_fn = [&](int64_t lo, int cnt, bool part) {
+            stage_span(lo, cnt, false);
+            const unsigned parts = __ballot_sync(PSB_FULL, part);
+            if (!parts) return;
+            ++n_spans;
+            n_parts += __popc(parts);
+            unsigned acc = 0;
+            const int j = lane < cnt ? lane : 0;
+            const T xj = st.x[j], yj = st.y[j], zj = st.z[j], hj = st.h[j];
+            const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj);  // (2 hb)^2
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
+                const T ra2s = st.ra2[s];
+                T e2 = ex_d2_pp<T>(ps, xj, yj, zj);
+                T r2 = (ST == ST_GATHER) ? ra2s : ((ST == ST_SCATTER) ? r2b : jmax(ra2s, r2b));
+                bool in = (lane < cnt) && (e2 <= r2);
+                unsigned bi = __ballot_sync(PSB_FULL, in);
+                if (lane == s) acc = bi;
+            }
+            emit(lo, acc);
+        };
+        ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps) && ok;
+    }
+
+    const bool tovf = __any_sync(PSB_FULL, ovf);
+    A.sp.cnt[bt * 32 + lane] = tovf ? (uint8_t)0xFF : (uint8_t)nent;
+    ((T*)A.sp.ha)[bt * 32 + lane] = ha;
+    if (tovf && lane == 0) {
+        const unsigned slot = atomicAdd(A.sp.ovf_count, 1u);
+        A.sp.ovf_tiles[slot] = (int32_t)tile;
+    }
+    // the single-kernel pass counts the pairs of an overflowed tile
+    if (tovf) n_pairs = 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+        n_retest += __shfl_xor_sync(PSB_FULL, n_retest, o);
+    }
+    if (lane == 0 && A.stats) {
+        atomicAdd(&A.stats[0], n_pairs);
+        atomicAdd(&A.stats[1], n_retest);
+        atomicAdd(&A.stats[2], (unsigned long long)steps);
+        atomicAdd(&A.stats[3], n_spans);
+        atomicAdd(&A.stats[4], n_parts);
+    }
+    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+template <class T, int PREC, int ST, int KC>
+__global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
+    using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
+    using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
+    constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
+    constexpr bool SHIFT = (PREC == PREC_FP32C);
+    const TreeView<T>& tv = A.tv;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int64_t bt = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (bt >= A.sp.ntiles) return;  // warp-uniform
+    const int n = A.sp.cnt[bt * 32 + lane];
+    if (n == 0xFF) return;  // overflowed tile (every lane): the single-kernel pass owns it
+    const int64_t tile = A.sp.tile0 + bt;
+    const int64_t k = sample_of(A.src, tile, lane);
+    const bool valid = k >= 0;
+    T p[3] = {T(0), T(0), T(0)}, dd[3];
+    if (valid) sample_coords(A.src, k, p, dd);
+    const T ha = ((const T*)A.sp.ha)[bt * 32 + lane];
+    const int kc = A.rec.kc;
+    const bool need_dg = A.rec.need_dg != 0;
+
+    const CT sig = inv_pi<CT>();
+    CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
+    if (ST != ST_SCATTER) {
+        ia = CT(1) / (CT)ha;
+        sa3 = sig * ia * ia * ia;
+        sa4 = sa3 * ia;
+    }
+    Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
+    CT a0[KC];
+    bool have0 = false;
+    S1.zero(); Dm.zero();
+#pragma unroll
+    for (int d = 0; d < 3; ++d) { G[d].zero(); Dg[d].zero(); }
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+        Sw[c].zero();
+        a0[c] = CT(0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) Sg[c][d].zero();
+    }
+
+    // Kernel weights and sums of one pair; weights as in k_points.
+    auto accumulate = [&](int64_t li, CT dx, CT dy, CT dz, CT Wsum, CT csum, CT mr, CT mb) {
+        const CT w = mr * Wsum;
+        const CT gc = mr * csum;
+        const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
+        S1.add(w);
+        G[0].add(gx); G[1].add(gy); G[2].add(gz);
+        if (SHIFT && !have0) {
+            have0 = true;
+#pragma unroll
+            for (int c = 0; c < KC; ++c)
+                if (c < kc) a0[c] = BAND ? (CT)__ldg(&A.colF[c][li]) : (CT)__ldg(&A.colT[c][li]);
+        }
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                CT a = BAND ? (CT)__ldg(&A.colF[c][li]) : (CT)__ldg(&A.colT[c][li]);
+                if (SHIFT) a -= a0[c];
+                Sw[c].add(a * w);
+                Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+            }
+        }
+        if (need_dg) {
+            Dm.add(mb * Wsum);
+            const CT mc = mb * csum;
+            Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+        }
+    };
+
+    const uint2* ent = A.sp.ent + (size_t)bt * RCAP * 32 + lane;
+    int e = 0;
+    unsigned m = 0;
+    int64_t lo = 0;
+    float R0[3] = {0.f, 0.f, 0.f}, R1[3] = {0.f, 0.f, 0.f};
+    int64_t rt0 = 0;
+    unsigned long long n_bodyit = 0;
+    while (true) {
+        if (m == 0 && e < n) {
+            const uint2 q = ent[(size_t)e * 32];
+            ++e;
+            lo = (int64_t)q.x;
+            m = q.y;
+            if constexpr (BAND) {
+                // the sample relative to the anchors of the (at most two)
+                // 32-leaf tiles of this entry, in double then rounded
+                const int64_t t0 = lo >> 5;
+                const int64_t t1 = (lo + 31 - __clz(m)) >> 5;
+                rt0 = t0;
+                R0[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t0]));
+                R0[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t0 + 1]));
+                R0[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t0 + 2]));
+                R1[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t1]));
+                R1[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t1 + 1]));
+                R1[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t1 + 2]));
+            }
+        }
+        if (!__any_sync(PSB_FULL, m != 0)) break;
+        ++n_bodyit;
+        if (m) {
+            const int j = __ffs(m) - 1;
+            m &= m - 1;
+            const int64_t li = lo + j;
+            if constexpr (BAND) {
+                const float4 Lj = __ldg(&tv.leaf4[li]);
+                const float4 K = __ldg(&tv.leafK[li]);
+                const bool first_tile = (li >> 5) == rt0;
+                const float dx = (first_tile ? R0[0] : R1[0]) - Lj.x;
+                const float dy = (first_tile ? R0[1] : R1[1]) - Lj.y;
+                const float dz = (first_tile ? R0[2] : R1[2]) - Lj.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
+                const float r = d2 * invr;
+                float Wsum = 0.f, csum = 0.f;
+                if (ST != ST_SCATTER) {
+                    float f, df;
+                    m4_fdf<float>(r * (float)ia, f, df);
+                    Wsum = (float)sa3 * f;
+                    csum = (float)sa4 * df;
+                }
+                if (ST != ST_GATHER) {
+                    float f, df;
+                    m4_fdf<float>(r * K.x, f, df);
+                    if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
+                    else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
+                }
+                csum *= invr;
+                const float mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
+                accumulate(li, dx, dy, dz, Wsum, csum, K.w, mb);
+            } else {
+                const T xb = __ldg(&tv.x[li]), yb = __ldg(&tv.y[li]), zb = __ldg(&tv.z[li]);
+                const T e2 = ex_d2_pp<T>(p, xb, yb, zb);
+                const CT d2 = (CT)e2;
+                const CT r = sqrt(d2);
+                const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
+                CT Wsum = CT(0), csum = CT(0);
+                if (ST != ST_SCATTER) {
+                    CT f, df;
+                    m4_fdf<CT>(r * ia, f, df);
+                    Wsum = sa3 * f;
+                    csum = sa4 * df * invr;
+                }
+                if (ST != ST_GATHER) {
+                    const CT hb = (CT)__ldg(&tv.h[li]);
+                    CT ib = CT(1) / hb;
+                    CT sb3 = sig * ib * ib * ib;
+                    CT f, df;
+                    m4_fdf<CT>(r * ib, f, df);
+                    CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
+                    if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
+                    else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
+                }
+                const T mT = __ldg(&tv.m[li]);
+                const CT mb = (CT)mT;
+                const CT mr = (CT)((double)mT / (double)__ldg(&tv.rho[li]));
+                accumulate(li, (CT)(p[0] - xb), (CT)(p[1] - yb), (CT)(p[2] - zb), Wsum, csum, mr, mb);
+            }
+        }
+    }
+
+    if (valid) write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
+    if (lane == 0 && A.stats) atomicAdd(&A.stats[5], n_bodyit);
+}
+
+}  // namespace psb

@@ -2,7 +2,7 @@
 // instantiations are split over inst_*.cu so that they compile in parallel.
 #pragma once
 
-#include "k_points.cuh"
+#include "k_split.cuh"
 
 namespace psb {
 
@@ -62,8 +62,39 @@ static cudaError_t dispatch_lines_p(const Args<T>& a, int st, int kc, int what, 
     return cudaGetLastError();
 }
 
+// two-kernel point path: k_collect (bodies = false) or k_bodies (bodies = true)
+// over the batch a.sp
+template <class T, int P, int S>
+static void dispatch_bodies_k(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
+    if (kc <= 1) k_bodies<T, P, S, 1><<<g, 128, 0, s>>>(a);
+    else if (kc <= 2) k_bodies<T, P, S, 2><<<g, 128, 0, s>>>(a);
+    else if (kc <= 4) k_bodies<T, P, S, 4><<<g, 128, 0, s>>>(a);
+    else k_bodies<T, P, S, 8><<<g, 128, 0, s>>>(a);
+}
+
+template <class T, int P>
+static cudaError_t dispatch_split_p(const Args<T>& a, int st, int kc, bool bodies, cudaStream_t s) {
+    unsigned g = (unsigned)((a.sp.ntiles + 3) / 4);
+    if (g == 0) return cudaSuccess;
+    if (!bodies) {
+        if (st == ST_GATHER) k_collect<T, P, ST_GATHER><<<g, 128, 0, s>>>(a);
+        else if (st == ST_SCATTER) k_collect<T, P, ST_SCATTER><<<g, 128, 0, s>>>(a);
+        else k_collect<T, P, ST_SYMMETRIC><<<g, 128, 0, s>>>(a);
+    } else {
+        if (st == ST_GATHER) dispatch_bodies_k<T, P, ST_GATHER>(a, kc, g, s);
+        else if (st == ST_SCATTER) dispatch_bodies_k<T, P, ST_SCATTER>(a, kc, g, s);
+        else dispatch_bodies_k<T, P, ST_SYMMETRIC>(a, kc, g, s);
+    }
+    return cudaGetLastError();
+}
+
 // defined in inst_*.cu
 template <class T> cudaError_t launch_points(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
+cudaError_t launch_split_d0(const Args<double>& a, int st, int kc, bool bodies, cudaStream_t s);
+cudaError_t launch_split_d1(const Args<double>& a, int st, int kc, bool bodies, cudaStream_t s);
+inline cudaError_t launch_split(const Args<double>& a, int prec, int st, int kc, bool bodies, cudaStream_t s) {
+    return prec == PREC_FP64 ? launch_split_d0(a, st, kc, bodies, s) : launch_split_d1(a, st, kc, bodies, s);
+}
 template <class T> cudaError_t launch_lines(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
 
 }  // namespace psb

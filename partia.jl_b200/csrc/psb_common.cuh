@@ -101,6 +101,7 @@ template <class T> struct TreeView {
     const double* anchor;    // 3 per 32-leaf tile (x, y, z)
     const float* mrho;       // m / rho (float)
     const float* mf;         // m (float)
+    const float4* leafK;     // (1/h, sigma/h^3, sigma/h^4, m/rho) in float
     float coord_err;         // bound on |float coordinate - exact| for node tests
 };
 

@@ -39,6 +39,7 @@ struct psb_ctx {
     void* nscale = nullptr;
     float4* node_lo = nullptr; float4* node_hi = nullptr; float4* leaf4 = nullptr;
     double* anchor = nullptr; float* mrho = nullptr; float* mf = nullptr;
+    float4* leafK = nullptr;  // per leaf (1/h, sigma/h^3, sigma/h^4, m/rho), float
     float* colsf = nullptr;  // float copies of the columns (double inputs), ncol x n
     float coord_err = 0.f;
     double bbox[6] = {0, 0, 0, 0, 0, 0};  // particle min x,y,z, max x,y,z
@@ -49,7 +50,7 @@ struct psb_ctx {
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };
-    Slot scratch[16];
+    Slot scratch[24];
 
     cudaEvent_t ev[8] = {};
 };

@@ -62,6 +62,8 @@ class Context:
         if rc != 0:
             raise L.PsbError(rc, "psb_create failed (is a CUDA device visible?)")
         self.h = h
+        # OR-ed into the flags of the interpolation calls (e.g. PSB_FLAG_SINGLE_KERNEL)
+        self.extra_flags = 0
         self.dtype = np.dtype(np.float64)
         self.n = 0
         self.ncol = 0
@@ -151,7 +153,7 @@ class Context:
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_points(self.h, ns, _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy,
                                              C.byref(cat.c), prec, _ptr_array(outs),
-                                             L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                             (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return outs
 
     def interp_grid(self, ax, ay, az, cat: CatalogC, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, hs=None,
@@ -163,7 +165,7 @@ class Context:
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_grid(self.h, ax.ctypes.data, len(ax), ay.ctypes.data, len(ay),
                                            az.ctypes.data, len(az), hmode, _ptr(hsa), strategy, C.byref(cat.c), prec,
-                                           _ptr_array(outs), L.PSB_FLAG_DEVICE_PTRS if dev else 0,
+                                           _ptr_array(outs), (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags,
                                            C.byref(self.last_stats)))
         return outs
 
@@ -177,7 +179,7 @@ class Context:
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_box(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, nz, hmode, _ptr(hsa),
                                           strategy, C.byref(cat.c), prec, _ptr_array(outs),
-                                          L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                          (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return outs
 
     def interp_lines(self, o, d, cat: CatalogC, strategy=L.PSB_SCATTER, hmode=L.PSB_H_PER_SAMPLE, hs=None,
@@ -189,7 +191,7 @@ class Context:
         outs = self._outs(nl, cat.L, dev, out)
         self._chk(self.lib.psb_interp_lines(self.h, nl, *[_ptr(a) for a in arrs], hmode, _ptr(hsa), strategy,
                                             C.byref(cat.c), prec, _ptr_array(outs),
-                                            L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                            (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return outs
 
     def interp_beam(self, frame, params, nx, ny, cat: CatalogC, strategy=L.PSB_SCATTER, hmode=L.PSB_H_PER_SAMPLE,
@@ -201,7 +203,7 @@ class Context:
         outs = self._outs(nx * ny, cat.L, dev, out)
         self._chk(self.lib.psb_interp_beam(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, hmode, _ptr(hsa), strategy,
                                            C.byref(cat.c), prec, _ptr_array(outs),
-                                           L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                           (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return outs
 
     def density(self, sx, sy, sz, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=None, prec=L.PSB_PREC_FP64,
@@ -211,7 +213,7 @@ class Context:
         hsa = self._hs(hmode, hs)
         o = out if out is not None else self._outs(len(sx), 1, dev)[0]
         self._chk(self.lib.psb_density(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy, prec,
-                                       _ptr(o), L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                       _ptr(o), (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return o
 
     def digest(self, a, d=None, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, hs=None, fp32c=False):

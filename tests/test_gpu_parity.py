@@ -188,6 +188,49 @@ def test_point_fields_float32_inputs():
             assert rel_err(g[k], ref[k]) <= 2e-4, (prec, k)
 
 
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+@pytest.mark.parametrize("strategy", [L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC])
+def test_two_kernel_path_matches_single_kernel(prec, strategy):
+    """The pair-list + pair-sum kernels visit the same pairs in the same order
+    with the same arithmetic as the single kernel."""
+    arrs, cols = make_particles(30_000, 71)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build(want_perm=False)
+    s = _samples(6000, 72)
+    cat = CatalogC(**CATALOGS["all"])
+    two = ctx.interp_points(*s, cat, strategy=strategy, hmode=L.PSB_H_NEAREST, prec=prec)
+    st2 = ctx.last_stats.as_dict()
+    ctx.extra_flags = L.PSB_FLAG_SINGLE_KERNEL
+    one = ctx.interp_points(*s, cat, strategy=strategy, hmode=L.PSB_H_NEAREST, prec=prec)
+    st1 = ctx.last_stats.as_dict()
+    assert st2["pairs"] == st1["pairs"] > 0
+    assert st2["launches"] >= 3
+    tol = 1e-14 if prec == L.PSB_PREC_FP64 else 1e-6
+    for k in range(cat.L):
+        assert rel_err(two[k], one[k]) <= tol, (k, rel_err(two[k], one[k]))
+
+
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+def test_two_kernel_path_overflow_tiles(prec):
+    """Samples with very large h accept more leaf spans than a pair list holds;
+    their tiles go to the single-kernel pass, the others stay on the lists."""
+    arrs, cols = make_particles(20_000, 73)
+    orc, ctx, _, _ = pair(arrs, cols)
+    rng = np.random.default_rng(74)
+    ns = 3000
+    s = tuple(rng.random(ns) for _ in range(3))
+    hs = np.where(rng.random(ns) < 0.01, 0.3, 0.01)
+    spec = CATALOGS["all"]
+    ref = orc.interp_points(*s, O.Catalog(**spec), strategy=O.GATHER, hmode=O.H_PER_SAMPLE, hs=hs)
+    g = ctx.interp_points(*s, CatalogC(**spec), strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=hs, prec=prec)
+    tol = FP64_TOL if prec == L.PSB_PREC_FP64 else FP32C_TOL
+    for k in range(len(ref)):
+        assert rel_err(g[k], ref[k]) <= tol, (k, rel_err(g[k], ref[k]))
+    co, _, _ = orc.digest(s, strategy=O.GATHER, hmode=O.H_PER_SAMPLE, hs=hs)
+    assert ctx.last_stats.pairs == int(co.sum())
+
+
 def test_empty_neighbourhood_gives_nan_and_zero_density():
     arrs, cols = make_particles(2000, 61)
     orc, ctx, _, _ = pair(arrs, cols)

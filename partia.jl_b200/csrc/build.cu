@@ -279,19 +279,40 @@ __global__ void k_pack_nodes(int64_t nint, const T* mnx, const T* mny, const T* 
     hi[t] = b;
 }
 
-// Leaf records.  For double inputs the coordinates are stored relative to the
-// first particle of their 32-leaf tile, so that float differences to a sample
-// carry only the rounding of the (small) offset.  For float inputs they are
-// the exact coordinates (anchor 0).
-template <class T>
-__global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, const T* h, const T* m, const T* rho,
-                              float4* leaf4, double* anchor, float* mrho, float* mf, float4* leafK) {
+// First leaf (0-based) of the span of every leaf: the leaf's highest
+// ancestor holding at most SPAN_LEAVES leaves, or the leaf itself when its
+// parent holds more.  The traversals hand exactly these subtrees to their
+// span handlers, so every span shares one anchor.  Unified ids: leaf i is
+// n + i; parent[id - 1] (0 above the root).
+__global__ void k_span_roots(int64_t n, const int32_t* parent, const int32_t* rlo, const int32_t* rhi,
+                             int32_t* sfirst) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int64_t t0 = i & ~(int64_t)31;
+    int32_t first = (int32_t)i;
+    int32_t p = parent[n + i - 1];
+    for (int guard = 0; p > 0 && guard < 2 * SPAN_LEAVES; ++guard) {  // a span is at most 31 levels deep
+        const int32_t lo = rlo[p - 1], hi = rhi[p - 1];
+        if (hi - lo + 1 > SPAN_LEAVES) break;
+        first = lo - 1;
+        p = parent[p - 1];
+    }
+    sfirst[i] = first;
+}
+
+// Leaf records.  For double inputs the coordinates are stored relative to the
+// first leaf of the leaf's span, so that float differences to a sample carry
+// only the rounding of the (small) offset.  For float inputs they are the
+// exact coordinates (anchor 0).
+template <class T>
+__global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, const T* h, const T* m, const T* rho,
+                              const int32_t* sfirst, float4* leaf4, float* mrho, float* mf, float4* leafK) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
     double ax = 0, ay = 0, az = 0;
-    if (sizeof(T) == 8) { ax = (double)x[t0]; ay = (double)y[t0]; az = (double)z[t0]; }
-    if (i == t0) { anchor[3 * (i >> 5) + 0] = ax; anchor[3 * (i >> 5) + 1] = ay; anchor[3 * (i >> 5) + 2] = az; }
+    if (sizeof(T) == 8) {
+        const int32_t a = sfirst[i];
+        ax = (double)x[a]; ay = (double)y[a]; az = (double)z[a];
+    }
     float4 r;
     if (sizeof(T) == 8) {
         r = make_float4((float)((double)x[i] - ax), (float)((double)y[i] - ay), (float)((double)z[i] - az),
@@ -402,13 +423,11 @@ static int build_typed(psb_ctx* c) {
     }
 
     // float traversal records
-    const int64_t ntile = (n + 31) / 32;
     PSB_CUDA_TRY(c, cudaMalloc(&c->links, sizeof(int4) * nalloc), "cudaMalloc links");
     if (nint > 0) k_pack_links<<<grid_for(nint), BT, 0, s>>>(nint, c->left, c->escape, c->range_lo, c->range_hi, c->links);
     PSB_CUDA_TRY(c, cudaMalloc(&c->node_lo, sizeof(float4) * nalloc), "cudaMalloc node_lo");
     PSB_CUDA_TRY(c, cudaMalloc(&c->node_hi, sizeof(float4) * nalloc), "cudaMalloc node_hi");
     PSB_CUDA_TRY(c, cudaMalloc(&c->leaf4, sizeof(float4) * n), "cudaMalloc leaf4");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->anchor, sizeof(double) * 3 * ntile), "cudaMalloc anchor");
     PSB_CUDA_TRY(c, cudaMalloc(&c->mrho, sizeof(float) * n), "cudaMalloc mrho");
     PSB_CUDA_TRY(c, cudaMalloc(&c->mf, sizeof(float) * n), "cudaMalloc mf");
     PSB_CUDA_TRY(c, cudaMalloc(&c->leafK, sizeof(float4) * n), "cudaMalloc leafK");
@@ -416,8 +435,12 @@ static int build_typed(psb_ctx* c) {
         k_pack_nodes<T><<<grid_for(nint), BT, 0, s>>>(nint, (const T*)c->nmin[0], (const T*)c->nmin[1],
                                                       (const T*)c->nmin[2], (const T*)c->nmax[0], (const T*)c->nmax[1],
                                                       (const T*)c->nmax[2], (const T*)c->nscale, c->node_lo, c->node_hi);
+    int32_t* sfirst = (int32_t*)scratch(c, 2, sizeof(int32_t) * n);  // visit counters consumed
+    if (!sfirst) return fail(c, PSB_ENOMEM, "scratch allocation failed (span roots)");
+    k_span_roots<<<grid_for(n), BT, 0, s>>>(n, c->parent, c->range_lo, c->range_hi, sfirst);
     k_pack_leaves<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->x, (const T*)c->y, (const T*)c->z, (const T*)c->h,
-                                                (const T*)c->m, (const T*)c->rho, c->leaf4, c->anchor, c->mrho, c->mf, c->leafK);
+                                                (const T*)c->m, (const T*)c->rho, sfirst, c->leaf4, c->mrho, c->mf,
+                                                c->leafK);
     if (sizeof(T) == 8 && c->ncol > 0) {
         PSB_CUDA_TRY(c, cudaMalloc(&c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
         for (int k = 0; k < c->ncol; ++k)

@@ -210,7 +210,7 @@ __device__ __forceinline__ bool warp_traverse(int32_t start, int64_t n, const in
 // so skipping the pruning tests inside a span cannot add or lose a neighbour,
 // and leaves are still visited in increasing index (DFS) order.
 // ---------------------------------------------------------------------------
-constexpr int SPAN = 32;
+constexpr int SPAN = SPAN_LEAVES;
 
 template <class NodeFn, class SpanFn>
 __device__ __forceinline__ bool warp_traverse_spans(int32_t start, int64_t n, const int4* __restrict__ links,

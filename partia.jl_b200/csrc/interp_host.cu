@@ -29,7 +29,7 @@ template <class T> TreeView<T> tree_view(psb_ctx* c) {
     v.cols = (const T* const*)c->d_cols;
     v.ncol = c->ncol;
     v.node_lo = c->node_lo; v.node_hi = c->node_hi; v.leaf4 = c->leaf4;
-    v.anchor = c->anchor; v.mrho = c->mrho; v.mf = c->mf; v.leafK = c->leafK;
+    v.mrho = c->mrho; v.mf = c->mf; v.leafK = c->leafK;
     v.coord_err = c->coord_err;
     return v;
 }
@@ -103,24 +103,25 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
 // Two-kernel point path over batches of tiles: k_collect writes the pair
 // lists of a batch, k_bodies sums them, and k_points takes the tiles whose
 // lists overflowed.  A batch holds at most SPLIT_BATCH tiles, which bounds the
-// list memory at SPLIT_BATCH * RCAP * 32 * 8 bytes (256 MiB).
+// list memory at SPLIT_BATCH * RCAP * 32 * 20 bytes (640 MiB).
 constexpr int64_t SPLIT_BATCH = 32768;
 
 static int run_split(psb_ctx* c, Args<double>& A, int prec, int st, int* launches) {
     cudaStream_t s = c->stream;
     const int64_t nt = A.src.ntiles;
     const int64_t B = std::min<int64_t>(nt, SPLIT_BATCH);
-    uint2* ent = (uint2*)scratch(c, 16, sizeof(uint2) * (size_t)RCAP * 32 * B);
+    float4* ent4 = (float4*)scratch(c, 16, sizeof(float4) * (size_t)RCAP * 32 * B);
+    uint32_t* emask = (uint32_t*)scratch(c, 20, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
     uint8_t* cnt = (uint8_t*)scratch(c, 17, (size_t)32 * B);
     void* hab = scratch(c, 18, sizeof(double) * 32 * (size_t)B);
     char* ovf = (char*)scratch(c, 19, 256 + sizeof(int32_t) * (size_t)B);
-    if (!ent || !cnt || !hab || !ovf) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
+    if (!ent4 || !emask || !cnt || !hab || !ovf) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
     unsigned* ovf_count = (unsigned*)ovf;
     int32_t* ovf_tiles = (int32_t*)(ovf + 256);
     for (int64_t t0 = 0; t0 < nt; t0 += B) {
         const int64_t nb = std::min<int64_t>(B, nt - t0);
         PSB_CUDA_TRY(c, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned), s), "memset overflow count");
-        A.sp.ent = ent; A.sp.cnt = cnt; A.sp.ha = hab;
+        A.sp.ent4 = ent4; A.sp.emask = emask; A.sp.cnt = cnt; A.sp.ha = hab;
         A.sp.ovf_tiles = ovf_tiles; A.sp.ovf_count = ovf_count;
         A.sp.tile0 = t0; A.sp.ntiles = nb;
         PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, false, s), "pair-list kernel launch");

@@ -16,8 +16,9 @@
 //    outward (a conservative superset); a leaf is accepted or rejected in
 //    float only when it lies outside an error band around the support
 //    radius, otherwise the reference's double test decides.  Neighbour sets
-//    are therefore identical too.  Float differences use coordinates relative
-//    to a per-32-leaf anchor, so their error is relative to the separation.
+//    are therefore identical too.  Float differences use leaf coordinates
+//    relative to the first leaf of their span, so their error is relative to
+//    the separation.
 #pragma once
 #include <type_traits>
 #include "interp.cuh"
@@ -25,14 +26,16 @@
 namespace psb {
 
 // Buffers of the two-kernel point path (one batch of tiles): the collect
-// kernel writes, for every sample, its accepted leaves as (first leaf, mask)
-// entries of up to 32 consecutive leaves, and its smoothing length; the body
-// kernel reads them.  A tile with a sample of more than RCAP entries is
-// marked (cnt = 0xFF for all its lanes) and listed in ovf_tiles; the
-// single-kernel path computes those tiles instead.
+// kernel writes, for every sample, its accepted leaves as one entry per span
+// (the span's first leaf, a mask over its <= 32 leaves, and the sample's
+// position relative to that first leaf, rounded to float from double), and
+// its smoothing length; the body kernel reads them.  A tile with a sample of
+// more than RCAP entries is marked (cnt = 0xFF for all its lanes) and listed
+// in ovf_tiles; the single-kernel path computes those tiles instead.
 constexpr int RCAP = 32;
 struct SplitBufs {
-    uint2* ent;          // [tile][RCAP][32]
+    float4* ent4;        // [tile][RCAP][32]: (rx, ry, rz, first leaf as int bits)
+    uint32_t* emask;     // [tile][RCAP][32]
     uint8_t* cnt;        // [tile][32]
     void* ha;            // [tile][32], element type T
     int32_t* ovf_tiles;  // absolute tile ids
@@ -314,11 +317,12 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
             float lb = lb_d2_line_box(of, mf3, el, lo, hi);
             return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
         };
-        // perpendicular offset of a tile anchor from the line, in double
-        auto perp_anchor = [&](int64_t t, float c[3], float& cerr) {
-            double q0 = __ldg(&tv.anchor[3 * t]) - (double)o[0];
-            double q1 = __ldg(&tv.anchor[3 * t + 1]) - (double)o[1];
-            double q2 = __ldg(&tv.anchor[3 * t + 2]) - (double)o[2];
+        // perpendicular offset of a span's anchor (its first leaf) from the
+        // line, in double
+        auto perp_anchor = [&](int64_t a, float c[3], float& cerr) {
+            double q0 = (double)__ldg(&tv.x[a]) - (double)o[0];
+            double q1 = (double)__ldg(&tv.y[a]) - (double)o[1];
+            double q2 = (double)__ldg(&tv.z[a]) - (double)o[2];
             double t0 = q0 * (double)m[0] + q1 * (double)m[1] + q2 * (double)m[2];
             c[0] = (float)(q0 - t0 * (double)m[0]);
             c[1] = (float)(q1 - t0 * (double)m[1]);
@@ -339,14 +343,9 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
             }
             __syncwarp();
             if (!part) return;
-            const int64_t t0 = lo >> 5;
-            float c0[3], c1[3] = {0.f, 0.f, 0.f}, ce0, ce1 = 0.f;
-            perp_anchor(t0, c0, ce0);
-            if (((lo + cnt - 1) >> 5) != t0) perp_anchor(t0 + 1, c1, ce1);
+            float cf[3], cerr;
+            perp_anchor(lo, cf, cerr);
             for (int j = 0; j < cnt; ++j) {
-                const bool second = ((lo + j) >> 5) != t0;
-                const float* cf = second ? c1 : c0;
-                const float cerr = second ? ce1 : ce0;
                 const float4 L = st.L[j];
                 float v0 = L.x + cf[0], v1 = L.y + cf[1], v2 = L.z + cf[2];
                 float vm = v0 * mf3[0] + v1 * mf3[1] + v2 * mf3[2];

@@ -31,7 +31,7 @@ template <class T, int KC> struct PStage<T, true, KC> {
     static constexpr int SB = NB * SPAN;
     // leaves of up to NB spans (slot b*32 + j = leaf j of batched span b)
     float4 Q[SB];       // position relative to the warp anchor, h (inclusion tests)
-    float4 Lr[SB];      // position relative to the leaf's own 32-leaf tile anchor (pair bodies)
+    float4 Lr[SB];      // position relative to the span's first leaf (pair bodies)
     float4 K[SB];       // 1/h, sigma/h^3, sigma/h^4, m/rho
     float mf[SB];       // m
     float col[KC][SB];
@@ -248,10 +248,10 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const int64_t li = lo + lane;
             if constexpr (BAND) {
                 const float4 L = __ldg(&tv.leaf4[li]);
-                const int64_t t = li >> 5;
-                float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
-                float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
-                float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                // the span's leaves are stored relative to its first leaf
+                float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+                float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+                float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
                 float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
                 st.Q[lane] = make_float4(q0, q1, q2, L.w);
                 eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
@@ -409,8 +409,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         unsigned unc0 = 0, unc1 = 0, unc2 = 0, unc3 = 0;
         const float4 Pme = st.P[lane];
         const float2 Rme = st.R[lane];
-        float R0[3] = {0.f, 0.f, 0.f}, R1[3] = {0.f, 0.f, 0.f};
-        int64_t rt0 = 0;
+        float R0[3] = {0.f, 0.f, 0.f};  // the sample relative to the current span's first leaf
         float esmax = Pme.w, rahimax = Rme.y;  // tile-wide maxima (sample error, sample radius)
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -428,10 +427,9 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             }
             const float4 Lj = st.Lr[slot];
             const float4 K = st.K[slot];
-            const bool first_tile = ((st.lo[b] + j) >> 5) == rt0;
-            const float dx = (first_tile ? R0[0] : R1[0]) - Lj.x;
-            const float dy = (first_tile ? R0[1] : R1[1]) - Lj.y;
-            const float dz = (first_tile ? R0[2] : R1[2]) - Lj.z;
+            const float dx = R0[0] - Lj.x;
+            const float dy = R0[1] - Lj.y;
+            const float dz = R0[2] - Lj.z;
             const float d2 = dx * dx + dy * dy + dz * dz;
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
             const float r = d2 * invr;
@@ -522,10 +520,9 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             if (lane < cnt) {
                 const int64_t li = lo + lane;
                 const float4 L = __ldg(&tv.leaf4[li]);
-                const int64_t t = li >> 5;
-                const float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
-                const float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
-                const float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+                const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+                const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
                 const float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
                 hb = L.w;
                 st.Q[slot] = make_float4(q0, q1, q2, hb);
@@ -543,20 +540,12 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
                 }
             }
             if (lane == 0) st.lo[b] = lo;
-            // this lane's sample relative to the anchors of the span's (at most
-            // two) 32-leaf tiles, in double then rounded: the pair separation
-            // R - L then carries only the rounding of two small vectors
-            {
-                const int64_t t0 = lo >> 5;
-                const int64_t t1 = (lo + cnt - 1) >> 5;
-                rt0 = t0;
-                R0[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t0]));
-                R0[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t0 + 1]));
-                R0[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t0 + 2]));
-                R1[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t1]));
-                R1[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t1 + 1]));
-                R1[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t1 + 2]));
-            }
+            // this lane's sample relative to the span's first leaf, in double
+            // then rounded: the pair separation R - L then carries only the
+            // rounding of two small vectors
+            R0[0] = (float)((double)p[0] - (double)__ldg(&tv.x[lo]));
+            R0[1] = (float)((double)p[1] - (double)__ldg(&tv.y[lo]));
+            R0[2] = (float)((double)p[2] - (double)__ldg(&tv.z[lo]));
             // error bound of float distances for this span, the same for every pair
             float eqm = eq;
 #pragma unroll

@@ -2,8 +2,8 @@
 //
 // k_collect walks the LBVH for a tile of 32 samples (one warp, the same walk,
 // spans and inclusion decisions as k_points) and records, per sample, the
-// accepted leaves as (first leaf, 32-bit mask) entries plus the sample's
-// smoothing length.  It keeps no accumulators, so it runs with few registers.
+// accepted leaves as one entry per span (first leaf, 32-bit mask, the sample's
+// offset from the first leaf) plus the sample's smoothing length.  It keeps no accumulators, so it runs with few registers.
 // k_bodies then evaluates the kernel weights and sums of every recorded pair:
 // each lane runs through its own sample's list in one flattened loop, so a
 // warp iteration does 32 pair bodies until the shortest lists run out, instead
@@ -71,10 +71,10 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
             const int64_t li = lo + lane;
             if constexpr (BAND) {
                 const float4 L = __ldg(&tv.leaf4[li]);
-                const int64_t t = li >> 5;
-                float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
-                float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
-                float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                // the span's leaves are stored relative to its first leaf
+                float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+                float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+                float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
                 float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
                 st.Q[lane] = make_float4(q0, q1, q2, L.w);
                 eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
@@ -113,14 +113,25 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
     }
 
     // this lane's pair list
-    uint2* ent = A.sp.ent + (size_t)bt * RCAP * 32 + lane;
+    float4* ent4 = A.sp.ent4 + (size_t)bt * RCAP * 32 + lane;
+    uint32_t* emask = A.sp.emask + (size_t)bt * RCAP * 32 + lane;
     int nent = 0;
     bool ovf = false;
     auto emit = [&](int64_t lo, unsigned acc) {
         if (!acc) return;
         n_pairs += __popc(acc);
         if (nent < RCAP) {
-            ent[(size_t)nent * 32] = make_uint2((unsigned)lo, acc);
+            // the sample relative to the span's first leaf, in double then
+            // rounded: the pair separation R - L carries only the rounding of
+            // two small vectors
+            float r0 = 0.f, r1 = 0.f, r2 = 0.f;
+            if (BAND) {
+                r0 = (float)((double)p[0] - (double)__ldg(&tv.x[lo]));
+                r1 = (float)((double)p[1] - (double)__ldg(&tv.y[lo]));
+                r2 = (float)((double)p[2] - (double)__ldg(&tv.z[lo]));
+            }
+            ent4[(size_t)nent * 32] = make_float4(r0, r1, r2, __int_as_float((int)lo));
+            emask[(size_t)nent * 32] = acc;
             ++nent;
         } else {
             ovf = true;
@@ -156,10 +167,9 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
             if (lane < cnt) {
                 const int64_t li = lo + lane;
                 const float4 L = __ldg(&tv.leaf4[li]);
-                const int64_t t = li >> 5;
-                const float o0 = (float)(__ldg(&tv.anchor[3 * t]) - cw[0]);
-                const float o1 = (float)(__ldg(&tv.anchor[3 * t + 1]) - cw[1]);
-                const float o2 = (float)(__ldg(&tv.anchor[3 * t + 2]) - cw[2]);
+                const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+                const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+                const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
                 const float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
                 hb = L.w;
                 st.Q[lane] = make_float4(q0, q1, q2, hb);
@@ -270,6 +280,35 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
     if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
 }
 
+// The data of one pair for k_bodies: float records for the FP32C path of
+// double inputs, the exact particle values otherwise.
+template <class T, bool BAND, int KC> struct PairData {
+    T x, y, z, h, m, rho;
+    T col[KC];
+    __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool,
+                                         const float*) {
+        x = __ldg(&tv.x[li]); y = __ldg(&tv.y[li]); z = __ldg(&tv.z[li]);
+        h = __ldg(&tv.h[li]); m = __ldg(&tv.m[li]); rho = __ldg(&tv.rho[li]);
+#pragma unroll
+        for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&A.colT[c][li]) : T(0);
+    }
+};
+template <class T, int KC> struct PairData<T, true, KC> {
+    float4 L, K;      // leaf4 and leafK of the particle
+    float col[KC];
+    float mb;         // mass (density gradient only)
+    float r[3];       // the sample relative to the span's first leaf
+    __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool need_dg,
+                                         const float* Rs) {
+        L = __ldg(&tv.leaf4[li]);
+        K = __ldg(&tv.leafK[li]);
+#pragma unroll
+        for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&A.colF[c][li]) : 0.f;
+        mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
+        r[0] = Rs[0]; r[1] = Rs[1]; r[2] = Rs[2];
+    }
+};
+
 template <class T, int PREC, int ST, int KC>
 __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
@@ -314,7 +353,7 @@ __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
     }
 
     // Kernel weights and sums of one pair; weights as in k_points.
-    auto accumulate = [&](int64_t li, CT dx, CT dy, CT dz, CT Wsum, CT csum, CT mr, CT mb) {
+    auto accumulate = [&](const auto& col, CT dx, CT dy, CT dz, CT Wsum, CT csum, CT mr, CT mb) {
         const CT w = mr * Wsum;
         const CT gc = mr * csum;
         const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
@@ -324,12 +363,12 @@ __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
             have0 = true;
 #pragma unroll
             for (int c = 0; c < KC; ++c)
-                if (c < kc) a0[c] = BAND ? (CT)__ldg(&A.colF[c][li]) : (CT)__ldg(&A.colT[c][li]);
+                if (c < kc) a0[c] = (CT)col[c];
         }
 #pragma unroll
         for (int c = 0; c < KC; ++c) {
             if (c < kc) {
-                CT a = BAND ? (CT)__ldg(&A.colF[c][li]) : (CT)__ldg(&A.colT[c][li]);
+                CT a = (CT)col[c];
                 if (SHIFT) a -= a0[c];
                 Sw[c].add(a * w);
                 Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
@@ -342,93 +381,89 @@ __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
         }
     };
 
-    const uint2* ent = A.sp.ent + (size_t)bt * RCAP * 32 + lane;
+    // The pairs of this lane's list, one ahead: the loads of the next pair are
+    // in flight while the current pair is summed.
+    const float4* ent4 = A.sp.ent4 + (size_t)bt * RCAP * 32 + lane;
+    const uint32_t* emask = A.sp.emask + (size_t)bt * RCAP * 32 + lane;
     int e = 0;
     unsigned m = 0;
     int64_t lo = 0;
-    float R0[3] = {0.f, 0.f, 0.f}, R1[3] = {0.f, 0.f, 0.f};
-    int64_t rt0 = 0;
-    unsigned long long n_bodyit = 0;
-    while (true) {
+    float Rs[3] = {0.f, 0.f, 0.f};
+    PairData<T, BAND, KC> nx;
+    bool hn = false;
+    auto fetch = [&]() {
         if (m == 0 && e < n) {
-            const uint2 q = ent[(size_t)e * 32];
+            const float4 q = ent4[(size_t)e * 32];
+            m = emask[(size_t)e * 32];
             ++e;
-            lo = (int64_t)q.x;
-            m = q.y;
-            if constexpr (BAND) {
-                // the sample relative to the anchors of the (at most two)
-                // 32-leaf tiles of this entry, in double then rounded
-                const int64_t t0 = lo >> 5;
-                const int64_t t1 = (lo + 31 - __clz(m)) >> 5;
-                rt0 = t0;
-                R0[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t0]));
-                R0[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t0 + 1]));
-                R0[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t0 + 2]));
-                R1[0] = (float)((double)p[0] - __ldg(&tv.anchor[3 * t1]));
-                R1[1] = (float)((double)p[1] - __ldg(&tv.anchor[3 * t1 + 1]));
-                R1[2] = (float)((double)p[2] - __ldg(&tv.anchor[3 * t1 + 2]));
-            }
+            lo = (int64_t)__float_as_int(q.w);
+            Rs[0] = q.x; Rs[1] = q.y; Rs[2] = q.z;
         }
-        if (!__any_sync(PSB_FULL, m != 0)) break;
-        ++n_bodyit;
-        if (m) {
+        hn = m != 0;
+        if (hn) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
-            const int64_t li = lo + j;
-            if constexpr (BAND) {
-                const float4 Lj = __ldg(&tv.leaf4[li]);
-                const float4 K = __ldg(&tv.leafK[li]);
-                const bool first_tile = (li >> 5) == rt0;
-                const float dx = (first_tile ? R0[0] : R1[0]) - Lj.x;
-                const float dy = (first_tile ? R0[1] : R1[1]) - Lj.y;
-                const float dz = (first_tile ? R0[2] : R1[2]) - Lj.z;
-                const float d2 = dx * dx + dy * dy + dz * dz;
-                const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-                const float r = d2 * invr;
-                float Wsum = 0.f, csum = 0.f;
-                if (ST != ST_SCATTER) {
-                    float f, df;
-                    m4_fdf<float>(r * (float)ia, f, df);
-                    Wsum = (float)sa3 * f;
-                    csum = (float)sa4 * df;
-                }
-                if (ST != ST_GATHER) {
-                    float f, df;
-                    m4_fdf<float>(r * K.x, f, df);
-                    if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
-                    else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
-                }
-                csum *= invr;
-                const float mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
-                accumulate(li, dx, dy, dz, Wsum, csum, K.w, mb);
-            } else {
-                const T xb = __ldg(&tv.x[li]), yb = __ldg(&tv.y[li]), zb = __ldg(&tv.z[li]);
-                const T e2 = ex_d2_pp<T>(p, xb, yb, zb);
-                const CT d2 = (CT)e2;
-                const CT r = sqrt(d2);
-                const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
-                CT Wsum = CT(0), csum = CT(0);
-                if (ST != ST_SCATTER) {
-                    CT f, df;
-                    m4_fdf<CT>(r * ia, f, df);
-                    Wsum = sa3 * f;
-                    csum = sa4 * df * invr;
-                }
-                if (ST != ST_GATHER) {
-                    const CT hb = (CT)__ldg(&tv.h[li]);
-                    CT ib = CT(1) / hb;
-                    CT sb3 = sig * ib * ib * ib;
-                    CT f, df;
-                    m4_fdf<CT>(r * ib, f, df);
-                    CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
-                    if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
-                    else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
-                }
-                const T mT = __ldg(&tv.m[li]);
-                const CT mb = (CT)mT;
-                const CT mr = (CT)((double)mT / (double)__ldg(&tv.rho[li]));
-                accumulate(li, (CT)(p[0] - xb), (CT)(p[1] - yb), (CT)(p[2] - zb), Wsum, csum, mr, mb);
+            nx.load(tv, A, lo + j, kc, need_dg, Rs);
+        }
+    };
+    unsigned long long n_bodyit = 0;
+    fetch();
+    while (__any_sync(PSB_FULL, hn)) {
+        const bool hc = hn;
+        const PairData<T, BAND, KC> cur = nx;
+        fetch();
+        ++n_bodyit;
+        if (!hc) continue;
+        if constexpr (BAND) {
+            const float dx = cur.r[0] - cur.L.x;
+            const float dy = cur.r[1] - cur.L.y;
+            const float dz = cur.r[2] - cur.L.z;
+            const float d2 = dx * dx + dy * dy + dz * dz;
+            const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
+            const float r = d2 * invr;
+            float Wsum = 0.f, csum = 0.f;
+            if (ST != ST_SCATTER) {
+                float f, df;
+                m4_fdf<float>(r * (float)ia, f, df);
+                Wsum = (float)sa3 * f;
+                csum = (float)sa4 * df;
             }
+            if (ST != ST_GATHER) {
+                float f, df;
+                m4_fdf<float>(r * cur.K.x, f, df);
+                if (ST == ST_SCATTER) { Wsum = cur.K.y * f; csum = cur.K.z * df; }
+                else { Wsum = 0.5f * (Wsum + cur.K.y * f); csum = 0.5f * (csum + cur.K.z * df); }
+            }
+            csum *= invr;
+            accumulate(cur.col, dx, dy, dz, Wsum, csum, cur.K.w, cur.mb);
+        } else {
+            const T e2 = ex_d2_pp<T>(p, cur.x, cur.y, cur.z);
+            const CT d2 = (CT)e2;
+            const CT r = sqrt(d2);
+            const CT invr = (d2 > CT(0)) ? CT(1) / r : CT(0);
+            CT Wsum = CT(0), csum = CT(0);
+            if (ST != ST_SCATTER) {
+                CT f, df;
+                m4_fdf<CT>(r * ia, f, df);
+                Wsum = sa3 * f;
+                csum = sa4 * df * invr;
+            }
+            if (ST != ST_GATHER) {
+                const CT hb = (CT)cur.h;
+                CT ib = CT(1) / hb;
+                CT sb3 = sig * ib * ib * ib;
+                CT f, df;
+                m4_fdf<CT>(r * ib, f, df);
+                CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
+                if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
+                else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
+            }
+            const CT mb = (CT)cur.m;
+            const CT mr = (CT)((double)cur.m / (double)cur.rho);
+            CT cc[KC];
+#pragma unroll
+            for (int c = 0; c < KC; ++c) cc[c] = (CT)cur.col[c];
+            accumulate(cc, (CT)(p[0] - cur.x), (CT)(p[1] - cur.y), (CT)(p[2] - cur.z), Wsum, csum, mr, mb);
         }
     }
 

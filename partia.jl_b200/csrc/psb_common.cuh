@@ -21,6 +21,10 @@
 
 namespace psb {
 
+// A subtree of at most SPAN_LEAVES leaves is handled as one unit ("span") by
+// the traversals; its root is the highest node with at most that many leaves.
+constexpr int SPAN_LEAVES = 32;
+
 // ---------------------------------------------------------------------------
 // Exactly rounded arithmetic.  Parity-critical steps (Morton quantisation,
 // squared distances, radii, the neighbour inclusion test, the nearest-particle
@@ -97,8 +101,9 @@ template <class T> struct TreeView {
     // float traversal records (used by the FP32C path of double inputs)
     const float4* node_lo;   // (minx, miny, minz, node_scale) rounded outward / up
     const float4* node_hi;   // (maxx, maxy, maxz, 0) rounded outward
-    const float4* leaf4;     // (x - ax, y - ay, z - az, h) relative to the tile anchor
-    const double* anchor;    // 3 per 32-leaf tile (x, y, z)
+    // (x - ax, y - ay, z - az, h): position relative to the first leaf of the
+    // leaf's span (the leaf's highest ancestor with <= SPAN_LEAVES leaves)
+    const float4* leaf4;
     const float* mrho;       // m / rho (float)
     const float* mf;         // m (float)
     const float4* leafK;     // (1/h, sigma/h^3, sigma/h^4, m/rho) in float

@@ -38,7 +38,7 @@ struct psb_ctx {
     void* nmax[3] = {nullptr, nullptr, nullptr};
     void* nscale = nullptr;
     float4* node_lo = nullptr; float4* node_hi = nullptr; float4* leaf4 = nullptr;
-    double* anchor = nullptr; float* mrho = nullptr; float* mf = nullptr;
+    float* mrho = nullptr; float* mf = nullptr;
     float4* leafK = nullptr;  // per leaf (1/h, sigma/h^3, sigma/h^4, m/rho), float
     float* colsf = nullptr;  // float copies of the columns (double inputs), ncol x n
     float coord_err = 0.f;

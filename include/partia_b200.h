@@ -263,6 +263,47 @@ int psb_neighbor_digest(psb_ctx* ctx, int32_t kind, int64_t ns,
                         int64_t* count_out, uint64_t* hash_out, void* ha_out,
                         uint32_t flags);
 
+/* ---- adjoint ------------------------------------------------------------------ */
+
+/* Vector-Jacobian products of the interpolation (no counterpart in the
+ * reference, which has no derivatives; they serve a ChainRulesCore.rrule of
+ * PointSamples_interpolation / StructuredGrid_interpolation /
+ * LineSamples_interpolation).  For the loss
+ *   L = sum_k sum_s gout[k][s] * out_k(s)
+ * with out_k the field k (catalog order) that the matching forward call
+ * returns, they write dL/dm (gm), dL/dA (gcols[c] for particle column c; the
+ * columns the catalog does not use get zeros; gcols and its entries may be
+ * NULL) and dL/dx, dL/dy, dL/dz per particle, in the order the particles were
+ * given to psb_set_particles.  Densities, smoothing lengths and the sample h
+ * (hs, or the nearest particle's h, which is piecewise constant in the
+ * positions) are held fixed.  Double particle data only (else
+ * PSB_EUNSUPPORTED); the forward sums are recomputed in PSB_PREC_FP64.  The
+ * pair terms are summed per particle by a traversal of an LBVH over the
+ * samples (points, grids), or of the pixel lattice (beams), with the forward's
+ * inclusion arithmetic: no float atomics.  gout, hs and the gradient arrays
+ * are device pointers with PSB_FLAG_DEVICE_PTRS, host pointers otherwise;
+ * grid axes, frame and params are host pointers. */
+int psb_adjoint_points(psb_ctx* ctx, int64_t ns,
+                       const void* sx, const void* sy, const void* sz,
+                       psb_hmode hmode, const void* hs, psb_strategy strategy,
+                       const psb_catalog* cat, const void* const* gout,
+                       double* gm, double* const* gcols, double* gx, double* gy, double* gz,
+                       uint32_t flags, psb_stats* stats);
+int psb_adjoint_grid(psb_ctx* ctx,
+                     const void* ax, int64_t nx, const void* ay, int64_t ny,
+                     const void* az, int64_t nz,
+                     psb_hmode hmode, const void* hs, psb_strategy strategy,
+                     const psb_catalog* cat, const void* const* gout,
+                     double* gm, double* const* gcols, double* gx, double* gy, double* gz,
+                     uint32_t flags, psb_stats* stats);
+/* Parallel-beam lines (psb_interp_beam; the frame axes must be orthonormal). */
+int psb_adjoint_beam(psb_ctx* ctx, const void* frame, const void* params,
+                     int64_t nx, int64_t ny,
+                     psb_hmode hmode, const void* hs, psb_strategy strategy,
+                     const psb_catalog* cat, const void* const* gout,
+                     double* gm, double* const* gcols, double* gx, double* gy, double* gz,
+                     uint32_t flags, psb_stats* stats);
+
 /* ---- interpolation without device allocation -------------------------------- */
 
 /* No counterpart in the reference: an addition of this library.

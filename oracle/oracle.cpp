@@ -725,6 +725,246 @@ static bool density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3
     return ok;
 }
 
+// ---------------------------------------------------------------------------
+// Adjoint (vector-Jacobian product) of the point and line interpolation for a
+// loss L = sum_s sum_k gout_k(s) out_k(s), with respect to particle masses,
+// columns and positions.  Densities and smoothing lengths are held fixed, and
+// so is h_a: the nearest-particle h is piecewise constant in the positions.
+// Written with the per-sample sums S1 = sum w, G = sum g, Sw_c = sum A_c w,
+// Sg_c = sum A_c g, Dm = sum m W, Dg = sum m gradW (w = m/rho W,
+// g = m/rho gradW), whose finalisation is the algebra of
+// general_interpolation.jl:128-214 (and
+// line_integrated_scalar_interpolation.jl:154-166 for lines).  The reference
+// has no adjoint; this is the checker of the GPU adjoint and is itself checked
+// against central finite differences of the forward restatement.
+// ---------------------------------------------------------------------------
+
+// M4 in terms of delta = p - x, r = |delta|, q = r/h (kernels/M4_spline.jl:13-36):
+// gradW = sigma/h^5 g1(q) delta and Hessian = sigma/h^5 (g1 I + g2 q n n^T),
+// with g1 = f'(q)/q, g2 = d g1/dq and n = delta/r.
+template <class T> static inline void m4_g12(T q, T& g1, T& g2) {
+    if (q < T(1)) {
+        g1 = T(2.25) * q - T(3);
+        g2 = T(2.25);
+    } else if (q < T(2)) {
+        T a = T(2) - q;
+        g1 = T(-0.75) * a * a / q;
+        g2 = T(0.75) * a * (q + T(2)) / (q * q);
+    } else {
+        g1 = T(0);
+        g2 = T(0);
+    }
+}
+
+// W, gradW and the Hessian (xx, yy, zz, xy, xz, yz) with respect to delta
+template <class T> static inline void kernel_whess(T dx, T dy, T dz, T h, T& W, T g[3], T H[6]) {
+    T r2 = dx * dx + dy * dy + dz * dz;
+    T r = std::sqrt(r2);
+    W = kernel_W(r, h);
+    kernel_gradW(dx, dy, dz, h, g[0], g[1], g[2]);
+    T g1, g2;
+    m4_g12(r / h, g1, g2);
+    T s5 = m4_norm3<T>() / (h * h * h * h * h);
+    T c = s5 * g1;
+    T e = (r2 > T(0)) ? s5 * g2 * (r / h) / r2 : T(0);
+    H[0] = c + e * dx * dx; H[1] = c + e * dy * dy; H[2] = c + e * dz * dz;
+    H[3] = e * dx * dy; H[4] = e * dx * dz; H[5] = e * dy * dz;
+}
+
+template <class T> static inline void hess_mul(const T H[6], const T v[3], T out[3]) {
+    out[0] = H[0] * v[0] + H[3] * v[1] + H[4] * v[2];
+    out[1] = H[3] * v[0] + H[1] * v[1] + H[5] * v[2];
+    out[2] = H[4] * v[0] + H[5] * v[1] + H[2] * v[2];
+}
+
+// Per-particle accumulator layout (Morton index li): [m, x, y, z, col 0, ...]
+template <class T>
+static bool adjoint_point(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T pa[3], T ha, int mode,
+                          const T* gout, T* acc) {
+    const T K = m4_support<T>();
+    const T radius = K * ha;
+    const T radius2 = radius * radius;
+    const int nc = (int)P.cols.size();
+    const int stride = 4 + nc;
+    struct Nb { int64_t li; T hb; };
+    std::vector<Nb> nb;
+    bool ok = traverse<T, false>(tr, pa, pa, mode, K, [&]() { return radius2; },
+                                 [&](int64_t li, T, T hb) { nb.push_back({li, hb}); });
+    auto eval = [&](const Nb& b, T& W, T g[3], T H[6]) {
+        T dx = pa[0] - P.x[b.li], dy = pa[1] - P.y[b.li], dz = pa[2] - P.z[b.li];
+        if (mode == GATHER) { kernel_whess(dx, dy, dz, ha, W, g, H); return; }
+        if (mode == SCATTER) { kernel_whess(dx, dy, dz, b.hb, W, g, H); return; }
+        T Wa, ga[3], Ha[6], Wb, gb[3], Hb[6];
+        kernel_whess(dx, dy, dz, ha, Wa, ga, Ha);
+        kernel_whess(dx, dy, dz, b.hb, Wb, gb, Hb);
+        W = T(0.5) * (Wa + Wb);
+        for (int d = 0; d < 3; ++d) g[d] = T(0.5) * (ga[d] + gb[d]);
+        for (int d = 0; d < 6; ++d) H[d] = T(0.5) * (Ha[d] + Hb[d]);
+    };
+    // sums
+    T S1 = 0, G[3] = {0, 0, 0}, Dm = 0, Dg[3] = {0, 0, 0};
+    std::vector<T> Sw(nc, T(0)), Sg(3 * nc, T(0));
+    for (const Nb& b : nb) {
+        T W, g[3], H[6];
+        eval(b, W, g, H);
+        const T m = P.m[b.li], mr = m / P.rho[b.li];
+        S1 += mr * W;
+        Dm += m * W;
+        for (int d = 0; d < 3; ++d) { G[d] += mr * g[d]; Dg[d] += m * g[d]; }
+        for (int c = 0; c < nc; ++c) {
+            const T A = P.cols[c][b.li];
+            Sw[c] += A * mr * W;
+            for (int d = 0; d < 3; ++d) Sg[3 * c + d] += A * mr * g[d];
+        }
+    }
+    if (S1 == T(0)) return ok;  // every output NaN, nothing flows back
+    // cotangents of the sums
+    const T inv = T(1) / S1, inv2 = inv * inv;
+    T lS1 = 0, lG[3] = {0, 0, 0}, lDm = 0, lDg[3] = {0, 0, 0};
+    std::vector<T> lSw(nc, T(0)), lSg(3 * nc, T(0));
+    int o = 0;
+    for (int j = 0; j < cat.ns; ++j) {
+        const int c = cat.sslot[j];
+        const T go = gout[o++];
+        if (cat.shep[j]) { lSw[c] += go * inv; lS1 -= go * Sw[c] * inv2; }
+        else lSw[c] += go;
+    }
+    for (int j = 0; j < cat.ng; ++j) {
+        const int c = cat.gslot[j];
+        for (int d = 0; d < 3; ++d) {
+            const T go = gout[o++];
+            if (c < 0) {  // Dg - G Dm / S1
+                lDg[d] += go; lG[d] -= go * Dm * inv; lDm -= go * G[d] * inv; lS1 += go * G[d] * Dm * inv2;
+            } else {      // Sg_c - G Sw_c / S1
+                lSg[3 * c + d] += go; lG[d] -= go * Sw[c] * inv; lSw[c] -= go * G[d] * inv;
+                lS1 += go * G[d] * Sw[c] * inv2;
+            }
+        }
+    }
+    for (int j = 0; j < cat.nd; ++j) {  // sum_d Sg_{c_d}[d] - sum_d Sw_{c_d}/S1 G[d]
+        const T go = gout[o++];
+        for (int d = 0; d < 3; ++d) {
+            const int c = cat.dslot[3 * j + d];
+            lSg[3 * c + d] += go; lG[d] -= go * Sw[c] * inv; lSw[c] -= go * G[d] * inv;
+            lS1 += go * Sw[c] * G[d] * inv2;
+        }
+    }
+    for (int j = 0; j < cat.nc; ++j) {
+        const int cx = cat.cslot[3 * j], cy = cat.cslot[3 * j + 1], cz = cat.cslot[3 * j + 2];
+        // component = -Sg_a[ka] + Sg_b[kb] + Sw_a/S1 G[ka] - Sw_b/S1 G[kb]
+        const int a_[3] = {cy, cz, cx}, ka_[3] = {2, 0, 1}, b_[3] = {cz, cx, cy}, kb_[3] = {1, 2, 0};
+        for (int d = 0; d < 3; ++d) {
+            const T go = gout[o++];
+            const int a = a_[d], ka = ka_[d], b = b_[d], kb = kb_[d];
+            lSg[3 * a + ka] -= go; lSg[3 * b + kb] += go;
+            lG[ka] += go * Sw[a] * inv; lG[kb] -= go * Sw[b] * inv;
+            lSw[a] += go * G[ka] * inv; lSw[b] -= go * G[kb] * inv;
+            lS1 -= go * (Sw[a] * G[ka] - Sw[b] * G[kb]) * inv2;
+        }
+    }
+    // pair terms
+    for (const Nb& b : nb) {
+        T W, g[3], H[6];
+        eval(b, W, g, H);
+        const T m = P.m[b.li], rho = P.rho[b.li], mr = m / rho;
+        T aS = lS1, aG[3] = {lG[0], lG[1], lG[2]};
+        for (int c = 0; c < nc; ++c) {
+            const T A = P.cols[c][b.li];
+            aS += lSw[c] * A;
+            for (int d = 0; d < 3; ++d) aG[d] += A * lSg[3 * c + d];
+        }
+        T* a = acc + b.li * stride;
+        a[0] += (aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2]) / rho + lDm * W +
+                lDg[0] * g[0] + lDg[1] * g[1] + lDg[2] * g[2];
+        for (int c = 0; c < nc; ++c)
+            a[4 + c] += mr * (lSw[c] * W + lSg[3 * c] * g[0] + lSg[3 * c + 1] * g[1] + lSg[3 * c + 2] * g[2]);
+        T Ha[3], Hd[3];
+        hess_mul(H, aG, Ha);
+        hess_mul(H, lDg, Hd);
+        for (int d = 0; d < 3; ++d)  // delta = p - x_b
+            a[1 + d] -= mr * (aS * g[d] + Ha[d]) + m * (lDm * g[d] + Hd[d]);
+    }
+    return ok;
+}
+
+// line_integrated_kernel_function and its derivative in r: the slope of the
+// table segment that lin_lut interpolates on (line_integrated_kernel.jl:13-19)
+template <class T> static inline void line_kernel_d(T r, T h, T& W, T& dW) {
+    const T invh = T(1) / h;
+    const T q = r * invh;
+    if (q >= m4_support<T>()) { W = T(0); dW = T(0); return; }
+    const T* Q = lut_Q<T>();
+    const T* I = lut_I<T>();
+    const T dq = Q[1] - Q[0];
+    const T idxf = q / dq + T(1);
+    int32_t i = (int32_t)idxf;
+    if (i < 1) i = 1;
+    if (i > LUT_N - 1) i = LUT_N - 1;
+    const T t = idxf - T(i);
+    W = invh * (I[i - 1] * (T(1) - t) + I[i] * t);
+    dW = invh * invh * (I[i] - I[i - 1]) / dq;
+}
+
+template <class T>
+static bool adjoint_line(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T o[3], const T dir[3],
+                         T ha, int mode, const T* gout, T* acc) {
+    const T K = m4_support<T>();
+    const T radius = K * ha;
+    const T radius2 = radius * radius;
+    const int nc = (int)P.cols.size();
+    const int stride = 4 + nc;
+    struct Nb { int64_t li; T d2, hb; };
+    std::vector<Nb> nb;
+    bool ok = traverse<T, true>(tr, o, dir, mode, K, [&]() { return radius2; },
+                                [&](int64_t li, T d2, T hb) { nb.push_back({li, d2, hb}); });
+    auto eval = [&](const Nb& b, T& W, T& dW) {
+        const T dr = std::sqrt(b.d2 < T(0) ? T(0) : b.d2);
+        if (mode == GATHER) { line_kernel_d(dr, ha, W, dW); return; }
+        if (mode == SCATTER) { line_kernel_d(dr, b.hb, W, dW); return; }
+        T Wa, da, Wb, db;
+        line_kernel_d(dr, ha, Wa, da);
+        line_kernel_d(dr, b.hb, Wb, db);
+        W = T(0.5) * (Wa + Wb);
+        dW = T(0.5) * (da + db);
+    };
+    T S1 = 0;
+    std::vector<T> Sw(nc, T(0));
+    for (const Nb& b : nb) {
+        T W, dW;
+        eval(b, W, dW);
+        const T mr = P.m[b.li] / P.rho[b.li];
+        S1 += mr * W;
+        for (int c = 0; c < nc; ++c) Sw[c] += P.cols[c][b.li] * mr * W;
+    }
+    if (S1 == T(0)) return ok;
+    const T inv = T(1) / S1;
+    T lS1 = 0;
+    std::vector<T> lSw(nc, T(0));
+    for (int j = 0; j < cat.ns; ++j) {
+        const int c = cat.sslot[j];
+        const T go = gout[j];
+        if (cat.shep[j]) { lSw[c] += go * inv; lS1 -= go * Sw[c] * inv * inv; }
+        else lSw[c] += go;
+    }
+    for (const Nb& b : nb) {
+        T W, dW;
+        eval(b, W, dW);
+        const T rho = P.rho[b.li], mr = P.m[b.li] / rho;
+        T aS = lS1;
+        for (int c = 0; c < nc; ++c) aS += lSw[c] * P.cols[c][b.li];
+        T* a = acc + b.li * stride;
+        a[0] += aS * W / rho;
+        for (int c = 0; c < nc; ++c) a[4 + c] += mr * lSw[c] * W;
+        // d r_perp / d x_b = (D - (D.m) m) / r_perp with D = x_b - o
+        const T D[3] = {P.x[b.li] - o[0], P.y[b.li] - o[1], P.z[b.li] - o[2]};
+        const T Dm = D[0] * dir[0] + D[1] * dir[1] + D[2] * dir[2];
+        const T dr = std::sqrt(b.d2 < T(0) ? T(0) : b.d2);
+        if (dr > T(0))
+            for (int d = 0; d < 3; ++d) a[1 + d] += mr * aS * dW * (D[d] - Dm * dir[d]) / dr;
+    }
+    return ok;
+}
+
 }  // namespace orc
 
 // ===========================================================================
@@ -1047,3 +1287,77 @@ ORC_API int orc_morton_codes(int64_t n, int dtype, const void* x, const void* y,
     return 0;
 }
 
+
+// Adjoint of orc_interp_points / orc_interp_lines (double particles only):
+// gout[k] holds the cotangent of output field k per sample; gm, gcols[c], gx,
+// gy, gz receive dL/dm, dL/dA_c, dL/dx.. per particle in the order the
+// particles were given to orc_create.
+template <class F>
+static int adjoint_impl(orc_ctx* c, int64_t ns, F per_sample, void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
+    Particles<double>& P = c->Pd;
+    Tree<double>& tr = c->Td;
+    const int nc = (int)P.cols.size();
+    const int stride = 4 + nc;
+    std::vector<double> acc((size_t)P.n * stride, 0.0);
+    std::atomic<int> bad(0);
+    #pragma omp parallel
+    {
+        std::vector<double> mine((size_t)P.n * stride, 0.0);
+        #pragma omp for schedule(dynamic, 16)
+        for (int64_t i = 0; i < ns; ++i)
+            if (!per_sample(i, mine.data())) bad = 1;
+        #pragma omp critical
+        for (size_t k = 0; k < mine.size(); ++k) acc[k] += mine[k];
+    }
+    for (int64_t i = 0; i < P.n; ++i) {
+        const int64_t j = tr.order[i];  // original index of Morton position i
+        const double* a = acc.data() + (size_t)i * stride;
+        if (gm) ((double*)gm)[j] = a[0];
+        if (gx) ((double*)gx)[j] = a[1];
+        if (gy) ((double*)gy)[j] = a[2];
+        if (gz) ((double*)gz)[j] = a[3];
+        for (int k = 0; k < nc; ++k)
+            if (gcols && gcols[k]) ((double*)gcols[k])[j] = a[4 + k];
+    }
+    return bad ? -5 : 0;
+}
+
+ORC_API int orc_adjoint_points(orc_ctx* c, int64_t ns, const void* sx, const void* sy, const void* sz,
+                               int hmode, const void* hs, int mode,
+                               int nsc, const int32_t* ss, const uint8_t* sh, int ng, const int32_t* gs,
+                               int nd, const int32_t* ds, int nc, const int32_t* cs, const void* const* gout,
+                               void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
+    if (!c->built) return -7;
+    if (c->dtype != 0) return -6;
+    Catalog cat = make_cat(nsc, ss, sh, ng, gs, nd, ds, nc, cs);
+    const int L = cat.L();
+    const double* X = (const double*)sx; const double* Y = (const double*)sy; const double* Z = (const double*)sz;
+    const double* const* GO = (const double* const*)gout;
+    return adjoint_impl(c, ns, [&](int64_t i, double* acc) {
+        double p[3] = {X[i], Y[i], Z[i]};
+        bool ok1 = true;
+        double ha = (mode == SCATTER) ? 0.0 : sample_h(c->Td, p, hmode, (const double*)hs, i, ok1);
+        std::vector<double> go(L > 0 ? L : 1);
+        for (int k = 0; k < L; ++k) go[k] = GO[k][i];
+        return adjoint_point(c->Pd, c->Td, cat, p, ha, mode, go.data(), acc) && ok1;
+    }, gm, gcols, gx, gy, gz);
+}
+
+ORC_API int orc_adjoint_lines(orc_ctx* c, int64_t nl, const void* const* od, int hmode, const void* hs, int mode,
+                              int nsc, const int32_t* ss, const uint8_t* sh, const void* const* gout,
+                              void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
+    if (!c->built) return -7;
+    if (c->dtype != 0) return -6;
+    if (mode != SCATTER && hmode == 0) return -1;
+    Catalog cat = make_cat(nsc, ss, sh, 0, nullptr, 0, nullptr, 0, nullptr);
+    const double* const* A = (const double* const*)od;
+    const double* const* GO = (const double* const*)gout;
+    return adjoint_impl(c, nl, [&](int64_t i, double* acc) {
+        double o[3] = {A[0][i], A[1][i], A[2][i]}, d[3] = {A[3][i], A[4][i], A[5][i]};
+        double ha = 0.0;
+        if (mode != SCATTER) ha = (hmode == 1) ? ((const double*)hs)[i] : ((const double*)hs)[0];
+        std::vector<double> go(cat.ns > 0 ? cat.ns : 1);
+        for (int k = 0; k < cat.ns; ++k) go[k] = GO[k][i];
+        return adjoint_line(c->Pd, c->Td, cat, o, d, ha, mode, go.data(), acc);
+    }, gm, gcols, gx, gy, gz);
+}

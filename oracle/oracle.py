@@ -75,6 +75,13 @@ def lib():
         L.orc_brute_nearest.restype = C.c_int
         L.orc_morton_codes.argtypes = [_i64, C.c_int, _vp, _vp, _vp, _vp]
         L.orc_morton_codes.restype = C.c_int
+        L.orc_adjoint_points.argtypes = [_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int,
+                                         C.c_int, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp,
+                                         _vp, _vp, _vp, _vp, _vp]
+        L.orc_adjoint_points.restype = C.c_int
+        L.orc_adjoint_lines.argtypes = [_vp, _i64, _vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp,
+                                        _vp, _vp, _vp, _vp, _vp]
+        L.orc_adjoint_lines.restype = C.c_int
         _lib = L
     return _lib
 
@@ -214,6 +221,40 @@ class Oracle:
         if rc != 0:
             raise RuntimeError(f"oracle interp_lines failed ({rc})")
         return outs
+
+    def _grad_bufs(self):
+        g = dict(m=np.zeros(self.n), x=np.zeros(self.n), y=np.zeros(self.n), z=np.zeros(self.n),
+                 cols=[np.zeros(self.n) for _ in self._cols])
+        return g, _ptr_array(g["cols"])
+
+    def adjoint_points(self, sx, sy, sz, cat: Catalog, gout, strategy=SYMMETRIC, hmode=H_NEAREST, hs=None):
+        """dL/dm, dL/dA_c, dL/dx for L = sum_k sum_s gout[k][s] out_k(s) (double particles), in the
+        order the particles were given."""
+        sx, sy, sz = self._s(sx), self._s(sy), self._s(sz)
+        hsa = None if hs is None else self._s(np.atleast_1d(hs))
+        go = [np.ascontiguousarray(g, dtype=np.float64) for g in gout]
+        g, cptr = self._grad_bufs()
+        rc = lib().orc_adjoint_points(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy,
+                                      len(cat.scalars), _p(cat.scalars), _p(cat.shepard),
+                                      len(cat.grads), _p(cat.grads), len(cat.divs) // 3, _p(cat.divs),
+                                      len(cat.curls) // 3, _p(cat.curls), _ptr_array(go),
+                                      _p(g["m"]), cptr, _p(g["x"]), _p(g["y"]), _p(g["z"]))
+        if rc != 0:
+            raise RuntimeError(f"oracle adjoint_points failed ({rc})")
+        return g
+
+    def adjoint_lines(self, o, d, scalars, gout, shepard=None, strategy=SCATTER, hmode=H_PER_SAMPLE, hs=None):
+        arrs = [self._s(a) for a in (*o, *d)]
+        cat = Catalog(scalars=scalars, shepard=shepard)
+        hsa = None if hs is None else self._s(np.atleast_1d(hs))
+        go = [np.ascontiguousarray(g, dtype=np.float64) for g in gout]
+        g, cptr = self._grad_bufs()
+        rc = lib().orc_adjoint_lines(self.ctx, len(arrs[0]), _ptr_array(arrs), hmode, _p(hsa), strategy,
+                                     len(cat.scalars), _p(cat.scalars), _p(cat.shepard), _ptr_array(go),
+                                     _p(g["m"]), cptr, _p(g["x"]), _p(g["y"]), _p(g["z"]))
+        if rc != 0:
+            raise RuntimeError(f"oracle adjoint_lines failed ({rc})")
+        return g
 
     def density(self, sx, sy, sz, strategy=GATHER, hmode=H_PER_SAMPLE, hs=None):
         sx, sy, sz = self._s(sx), self._s(sy), self._s(sz)

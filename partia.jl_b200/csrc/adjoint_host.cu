@@ -1,0 +1,297 @@
+// adjoint_host.cu -- host drivers of the adjoint entry points: stage the
+// samples and the output cotangents, run the FP64 forward pass in its
+// sum-cotangent mode, build the LBVH over the samples (points) and run the
+// particle-centric kernels, then return dL/dm, dL/dA_c and dL/dx per particle
+// in the order the particles were given to psb_set_particles.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "k_adjoint.cuh"
+#include "psb_ctx.hpp"
+#include "psb_host.hpp"
+
+extern "C" int psb_create(psb_ctx** out, int device);
+extern "C" int psb_set_stream(psb_ctx* c, void* stream);
+extern "C" int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x, const void* y, const void* z,
+                                 const void* m, const void* h, const void* rho, int32_t ncol, const void* const* cols,
+                                 psb_kernel kernel, uint32_t flags);
+
+namespace psb {
+
+int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu);
+
+template <int KC>
+static void launch_adj_points_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
+    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC><<<g, 128, 0, s>>>(a);
+    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC><<<g, 128, 0, s>>>(a);
+    else k_adj_points<ST_SYMMETRIC, KC><<<g, 128, 0, s>>>(a);
+}
+template <int KC>
+static void launch_adj_beam_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
+    if (st == ST_GATHER) k_adj_beam<ST_GATHER, KC><<<g, 128, 0, s>>>(a);
+    else if (st == ST_SCATTER) k_adj_beam<ST_SCATTER, KC><<<g, 128, 0, s>>>(a);
+    else k_adj_beam<ST_SYMMETRIC, KC><<<g, 128, 0, s>>>(a);
+}
+
+// clears the adjoint hook of the context on every exit path
+struct AdjHook {
+    psb_ctx* c;
+    ~AdjHook() {
+        c->adj_gout = nullptr;
+        c->adj_lam = nullptr;
+        c->adj_lam_stride = 0;
+        c->adj_ha = nullptr;
+    }
+};
+
+int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int st, const psb_catalog* cat,
+                const void* const* gout, double* gm, double* const* gcols, double* gx, double* gy, double* gz,
+                uint32_t flags, psb_stats* stats) {
+    if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before the adjoint");
+    if (c->dt != PSB_F64) return fail(c, PSB_EUNSUPPORTED, "the adjoint needs double particle data");
+    if (st < 0 || st > 2) return fail(c, PSB_EINVAL, "unknown interpolation strategy");
+    if (hmode < 0 || hmode > 2) return fail(c, PSB_EINVAL, "unknown smoothing-length mode");
+    const bool line = rq0.line;
+    if (line && st != ST_SCATTER && hmode == PSB_H_NEAREST)
+        return fail(c, PSB_EINVAL, "line samples need hs for itpGather and itpSymmetric");
+    const bool dev = (flags & PSB_FLAG_DEVICE_PTRS) != 0;
+    cudaStream_t s = c->stream;
+    const int64_t n = c->n;
+    int64_t ns = rq0.ns;
+    if (rq0.kind == SRC_GRID) ns = rq0.nx * rq0.ny * rq0.nz;
+    if (rq0.kind == SRC_BEAM) ns = rq0.nx * rq0.ny;
+    if (ns < 0) return fail(c, PSB_EINVAL, "sample count must be non-negative");
+
+    Recipe rec;
+    std::vector<int> colu;
+    int rc = make_recipe(c, cat, line, rec, colu);
+    if (rc) return rc;
+    const int L = rec.L, kc = rec.kc;
+    if (L > 0 && ns > 0 && !gout) return fail(c, PSB_EINVAL, "gout must not be NULL");
+    for (int k = 0; ns > 0 && k < L; ++k)
+        if (!gout[k]) return fail(c, PSB_EINVAL, "a gout array is NULL");
+    if (!gm || !gx || !gy || !gz) return fail(c, PSB_EINVAL, "gradient outputs must not be NULL");
+    const bool need_h = st != ST_SCATTER && hmode != PSB_H_NEAREST;
+    if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+    if (rq0.kind == SRC_BEAM) {
+        if (rq0.nx < 2 || rq0.ny < 2) return fail(c, PSB_EUNSUPPORTED, "the beam adjoint needs nx, ny >= 2");
+        const double* f = (const double*)rq0.frame;
+        const double* pr = (const double*)rq0.params;
+        if (pr[1] == pr[0] || pr[3] == pr[2]) return fail(c, PSB_EINVAL, "degenerate beam extent");
+        auto dot = [&](int a, int b) { return f[a] * f[b] + f[a + 1] * f[b + 1] + f[a + 2] * f[b + 2]; };
+        if (std::fabs(dot(3, 3) - 1) > 1e-9 || std::fabs(dot(6, 6) - 1) > 1e-9 || std::fabs(dot(9, 9) - 1) > 1e-9 ||
+            std::fabs(dot(3, 6)) > 1e-9 || std::fabs(dot(3, 9)) > 1e-9 || std::fabs(dot(6, 9)) > 1e-9)
+            return fail(c, PSB_EUNSUPPORTED, "the beam adjoint needs an orthonormal frame");
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[0], s), "event");
+    int launches = 0;
+
+    // ---- gradient outputs (device) ----
+    const int ng = 4 + kc;
+    double* gdev = (double*)scratch(c, 27, sizeof(double) * (size_t)ng * (n > 0 ? n : 1));
+    if (!gdev) return fail(c, PSB_ENOMEM, "scratch allocation failed (gradients)");
+    double* g_m = dev ? gm : gdev;
+    double* g_x = dev ? gx : gdev + n;
+    double* g_y = dev ? gy : gdev + 2 * n;
+    double* g_z = dev ? gz : gdev + 3 * n;
+    double* g_c[MAX_KC] = {};
+    for (int q = 0; q < kc; ++q) g_c[q] = dev ? (gcols ? gcols[colu[q]] : nullptr) : gdev + (4 + q) * n;
+    PSB_CUDA_TRY(c, cudaMemsetAsync(gdev, 0, sizeof(double) * (size_t)ng * (n > 0 ? n : 1), s), "memset");
+    if (dev) {
+        for (double* p : {gm, gx, gy, gz}) PSB_CUDA_TRY(c, cudaMemsetAsync(p, 0, sizeof(double) * n, s), "memset");
+        for (int k = 0; gcols && k < c->ncol; ++k)
+            if (gcols[k]) PSB_CUDA_TRY(c, cudaMemsetAsync(gcols[k], 0, sizeof(double) * n, s), "memset");
+    }
+
+    if (ns > 0 && n > 0) {
+        // ---- samples, hs and gout on the device ----
+        SampleReq rq = rq0;
+        double* xyz = nullptr;
+        if (!line) {
+            xyz = (double*)scratch(c, 25, sizeof(double) * 3 * (size_t)ns);
+            if (!xyz) return fail(c, PSB_ENOMEM, "scratch allocation failed (samples)");
+            if (rq0.kind == SRC_ARRAYS) {
+                const cudaMemcpyKind kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+                for (int q = 0; q < 3; ++q)
+                    PSB_CUDA_TRY(c, cudaMemcpyAsync(xyz + q * ns, rq0.a[q], sizeof(double) * ns, kind, s), "sample copy");
+            } else {  // grid axes (host) -> coordinates of every sample
+                double* ax = (double*)scratch(c, 29, sizeof(double) * (rq0.nx + rq0.ny + rq0.nz));
+                if (!ax) return fail(c, PSB_ENOMEM, "scratch allocation failed (axes)");
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(ax, rq0.ax, sizeof(double) * rq0.nx, cudaMemcpyHostToDevice, s), "axis H2D");
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(ax + rq0.nx, rq0.ay, sizeof(double) * rq0.ny, cudaMemcpyHostToDevice, s), "axis H2D");
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(ax + rq0.nx + rq0.ny, rq0.az, sizeof(double) * rq0.nz, cudaMemcpyHostToDevice, s), "axis H2D");
+                SampleSrc<double> G;
+                memset((void*)&G, 0, sizeof(G));
+                G.kind = SRC_GRID;
+                G.ax = ax; G.ay = ax + rq0.nx; G.az = ax + rq0.nx + rq0.ny;
+                G.nx = rq0.nx; G.ny = rq0.ny; G.nz = rq0.nz;
+                k_sample_xyz<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(G, ns, xyz, xyz + ns, xyz + 2 * ns);
+                PSB_CUDA_TRY(c, cudaGetLastError(), "sample coordinate kernel");
+                ++launches;
+            }
+            rq = SampleReq();
+            rq.kind = SRC_ARRAYS;
+            rq.ns = ns;
+            rq.a[0] = xyz; rq.a[1] = xyz + ns; rq.a[2] = xyz + 2 * ns;
+        }
+        const int64_t nh = need_h ? (hmode == PSB_H_PER_SAMPLE ? ns : 1) : 0;
+        double* hsd = nullptr;
+        std::vector<double> hs_host;
+        if (need_h) {
+            hsd = (double*)scratch(c, 28, sizeof(double) * nh);
+            if (!hsd) return fail(c, PSB_ENOMEM, "scratch allocation failed (hs)");
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(hsd, hs, sizeof(double) * nh, dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s),
+                         "hs copy");
+            if (line) {
+                hs_host.resize(nh);
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(hs_host.data(), hsd, sizeof(double) * nh, cudaMemcpyDeviceToHost, s), "hs D2H");
+            }
+        }
+        double* god = (double*)scratch(c, 21, sizeof(double) * (size_t)(L > 0 ? L : 1) * ns);
+        const double** gptr = (const double**)scratch(c, 22, sizeof(void*) * (L > 0 ? L : 1));
+        const int nq = line ? 1 + kc : 8 + 4 * kc;
+        double* lam = (double*)scratch(c, 23, sizeof(double) * (size_t)nq * ns);
+        double* ha = (double*)scratch(c, 24, sizeof(double) * ns);
+        if (!god || !gptr || !lam || !ha) return fail(c, PSB_ENOMEM, "scratch allocation failed (cotangents)");
+        std::vector<const double*> gp(L > 0 ? L : 1);
+        for (int k = 0; k < L; ++k) {
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(god + (size_t)k * ns, gout[k], sizeof(double) * ns,
+                                            dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s), "gout copy");
+            gp[k] = god + (size_t)k * ns;
+        }
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(gptr, gp.data(), sizeof(void*) * (L > 0 ? L : 1), cudaMemcpyHostToDevice, s),
+                     "gout table copy");
+        PSB_CUDA_TRY(c, cudaMemsetAsync(ha, 0, sizeof(double) * ns, s), "memset");
+        PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");  // host staging buffers are released below
+
+        // ---- forward pass in FP64 writing the sum cotangents ----
+        {
+            AdjHook hook{c};
+            c->adj_gout = gptr;
+            c->adj_lam = lam;
+            c->adj_lam_stride = ns;
+            c->adj_ha = ha;
+            psb_stats fst;
+            memset(&fst, 0, sizeof(fst));
+            rc = run(c, rq, hmode, need_h ? (const void*)hsd : nullptr, st, cat, PREC_FP64, nullptr,
+                     PSB_FLAG_DEVICE_PTRS, &fst, WHAT_INTERP, nullptr, nullptr, nullptr);
+            if (rc) return rc;
+            launches += fst.launches;
+        }
+
+        AdjArgs J;
+        memset((void*)&J, 0, sizeof(J));
+        J.pt = tree_view<double>(c);
+        for (int q = 0; q < kc; ++q) J.colT[q] = (const double*)c->cols[colu[q]];
+        J.kc = kc;
+        J.lam_stride = ns;
+        J.porder = c->order;
+        J.gm = g_m; J.gx = g_x; J.gy = g_y; J.gz = g_z;
+        for (int q = 0; q < kc; ++q) J.gcol[q] = g_c[q];
+        J.err = c->d_err;
+        unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 8 * sizeof(unsigned long long));
+        if (!dstats) return fail(c, PSB_ENOMEM, "scratch allocation failed (stats)");
+        PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), s), "memset stats");
+        J.stats = dstats;
+        const int kcl = kc <= 1 ? 1 : (kc <= 2 ? 2 : (kc <= 4 ? 4 : 8));
+        PSB_CUDA_TRY(c, cudaEventRecord(c->ev[1], s), "event");
+        if (!line) {
+            // ---- LBVH over the samples, h = h_a ----
+            if (!c->sctx) {
+                psb_ctx* sc = nullptr;
+                int r2 = psb_create(&sc, c->device);
+                if (r2) return fail(c, r2, "could not create the sample-tree context");
+                c->sctx = sc;
+            }
+            psb_set_stream(c->sctx, (void*)s);
+            rc = psb_set_particles(c->sctx, ns, PSB_F64, xyz, xyz + ns, xyz + 2 * ns, ha, ha, ha, 0, nullptr,
+                                   PSB_KERNEL_M4, PSB_FLAG_DEVICE_PTRS);
+            if (!rc) rc = build_lbvh(c->sctx);
+            if (rc) return fail(c, rc, std::string("sample tree: ") + c->sctx->err);
+            double* lams = (double*)scratch(c, 26, sizeof(double) * (size_t)nq * ns);
+            if (!lams) return fail(c, PSB_ENOMEM, "scratch allocation failed (cotangents)");
+            k_gather_rows<<<(unsigned)((ns + 255) / 256), 256, 0, s>>>(lam, c->sctx->order, ns, nq, lams);
+            PSB_CUDA_TRY(c, cudaGetLastError(), "cotangent gather");
+            J.sv = tree_view<double>(c->sctx);
+            J.lam = lams;
+            const unsigned g = (unsigned)((n + 127) / 128);
+            if (kcl == 1) launch_adj_points_k<1>(J, st, g, s);
+            else if (kcl == 2) launch_adj_points_k<2>(J, st, g, s);
+            else if (kcl == 4) launch_adj_points_k<4>(J, st, g, s);
+            else launch_adj_points_k<8>(J, st, g, s);
+            PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
+            launches += 2;
+        } else {
+            J.lam = lam;
+            SampleSrc<double>& B = J.beam;
+            B.kind = SRC_BEAM;
+            B.ns = ns;
+            memcpy(B.frame, rq0.frame, sizeof(double) * 12);
+            memcpy(B.params, rq0.params, sizeof(double) * 4);
+            B.nx = rq0.nx; B.ny = rq0.ny; B.nz = 1;
+            J.hmode = hmode;
+            J.hs = hsd;
+            double hmax = 0.0;
+            for (double v : hs_host) hmax = std::max(hmax, v);
+            J.ha_max = hmax;
+            J.lut = c->lut_d;
+            const unsigned g = (unsigned)((n + 127) / 128);
+            if (kcl == 1) launch_adj_beam_k<1>(J, st, g, s);
+            else if (kcl == 2) launch_adj_beam_k<2>(J, st, g, s);
+            else if (kcl == 4) launch_adj_beam_k<4>(J, st, g, s);
+            else launch_adj_beam_k<8>(J, st, g, s);
+            PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
+            launches += 1;
+        }
+        PSB_CUDA_TRY(c, cudaEventRecord(c->ev[2], s), "event");
+        unsigned long long hst[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(hst, dstats, sizeof(hst), cudaMemcpyDeviceToHost, s), "stats D2H");
+        unsigned herr = 0;
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(&herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, s), "error D2H");
+        PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+        if (herr) {
+            cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
+            cudaStreamSynchronize(s);
+            return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+        }
+        if (stats) {
+            memset(stats, 0, sizeof(*stats));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
+            stats->interp_ms = ms;
+            stats->pairs = (int64_t)hst[0];
+            stats->warp_steps = (int64_t)hst[2];
+        }
+    }
+    // ---- gradients to the caller ----
+    if (!dev && n > 0) {
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(gm, g_m, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gradient D2H");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(gx, g_x, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gradient D2H");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(gy, g_y, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gradient D2H");
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(gz, g_z, sizeof(double) * n, cudaMemcpyDeviceToHost, s), "gradient D2H");
+        for (int k = 0; gcols && k < c->ncol; ++k) {
+            if (!gcols[k]) continue;
+            int q = -1;
+            for (int t = 0; t < kc; ++t)
+                if (colu[t] == k) q = t;
+            if (q >= 0)
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(gcols[k], g_c[q], sizeof(double) * n, cudaMemcpyDeviceToHost, s),
+                             "gradient D2H");
+            else
+                memset(gcols[k], 0, sizeof(double) * n);
+        }
+    }
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[3], s), "event");
+    PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+    if (stats) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev[0], c->ev[3]);
+        stats->total_ms = ms;
+        stats->launches = launches;
+    }
+    return PSB_OK;
+}
+
+}  // namespace psb

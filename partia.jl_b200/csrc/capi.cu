@@ -173,6 +173,8 @@ PSB_API int psb_destroy(psb_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     free_particles(c);
+    if (c->sctx) psb_destroy(c->sctx);
+    c->sctx = nullptr;
     for (auto& sl : c->scratch) {
         if (sl.p) cudaFree(sl.p);
         sl.p = nullptr;
@@ -424,4 +426,59 @@ PSB_API int psb_neighbor_digest(psb_ctx* c, int32_t kind, int64_t ns, const void
     int prec = (flags & 0x100u) ? PREC_FP32C : PREC_FP64;
     return run(c, r, hmode, hs, strategy, nullptr, prec, nullptr, flags & PSB_FLAG_DEVICE_PTRS, nullptr, WHAT_DIGEST,
                count_out, hash_out, ha_out);
+}
+
+// ---- adjoint --------------------------------------------------------------
+namespace psb {
+int run_adjoint(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, const psb_catalog* cat,
+                const void* const* gout, double* gm, double* const* gcols, double* gx, double* gy, double* gz,
+                uint32_t flags, psb_stats* stats);
+}
+
+PSB_API int psb_adjoint_points(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const void* sz,
+                               psb_hmode hmode, const void* hs, psb_strategy strategy, const psb_catalog* cat,
+                               const void* const* gout, double* gm, double* const* gcols, double* gx, double* gy,
+                               double* gz, uint32_t flags, psb_stats* stats) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    cudaSetDevice(c->device);
+    int rc = check_samples(c, ns, sx, sy, sz);
+    if (rc) return rc;
+    return run_adjoint(c, points_req(ns, sx, sy, sz), hmode, hs, strategy, cat, gout, gm, gcols, gx, gy, gz, flags,
+                       stats);
+}
+
+PSB_API int psb_adjoint_grid(psb_ctx* c, const void* ax, int64_t nx, const void* ay, int64_t ny, const void* az,
+                             int64_t nz, psb_hmode hmode, const void* hs, psb_strategy strategy,
+                             const psb_catalog* cat, const void* const* gout, double* gm, double* const* gcols,
+                             double* gx, double* gy, double* gz, uint32_t flags, psb_stats* stats) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    cudaSetDevice(c->device);
+    if (nx < 0 || ny < 0 || nz < 0) return fail(c, PSB_EINVAL, "grid sizes must be non-negative");
+    if ((nx > 0 && !ax) || (ny > 0 && !ay) || (nz > 0 && !az)) return fail(c, PSB_EINVAL, "axis arrays must not be NULL");
+    SampleReq r;
+    r.kind = SRC_GRID;
+    r.ns = nx * ny * nz;
+    r.ax = ax; r.ay = ay; r.az = az;
+    r.nx = nx; r.ny = ny; r.nz = nz;
+    return run_adjoint(c, r, hmode, hs, strategy, cat, gout, gm, gcols, gx, gy, gz, flags, stats);
+}
+
+PSB_API int psb_adjoint_beam(psb_ctx* c, const void* frame, const void* params, int64_t nx, int64_t ny,
+                             psb_hmode hmode, const void* hs, psb_strategy strategy, const psb_catalog* cat,
+                             const void* const* gout, double* gm, double* const* gcols, double* gx, double* gy,
+                             double* gz, uint32_t flags, psb_stats* stats) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    cudaSetDevice(c->device);
+    int rc = check_frame(c, frame, params, nx, ny, 1, false);
+    if (rc) return rc;
+    SampleReq r;
+    r.kind = SRC_BEAM;
+    r.line = true;
+    r.ns = nx * ny;
+    r.frame = frame; r.params = params;
+    r.nx = nx; r.ny = ny; r.nz = 1;
+    return run_adjoint(c, r, hmode, hs, strategy, cat, gout, gm, gcols, gx, gy, gz, flags, stats);
 }

@@ -156,8 +156,9 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
         A.rec.L = (what == WHAT_DENSITY) ? 1 : 0;
     }
     const int L = A.rec.L;
-    if (what == WHAT_INTERP && L > 0 && !out) return fail(c, PSB_EINVAL, "output pointer array must not be NULL");
-    for (int k = 0; what == WHAT_INTERP && k < L && ns > 0; ++k)
+    const bool adj = (what == WHAT_INTERP) && c->adj_lam;  // adjoint sum-cotangent pass: no fields written
+    if (what == WHAT_INTERP && !adj && L > 0 && !out) return fail(c, PSB_EINVAL, "output pointer array must not be NULL");
+    for (int k = 0; what == WHAT_INTERP && !adj && k < L && ns > 0; ++k)
         if (!out[k]) return fail(c, PSB_EINVAL, "output pointer " + std::to_string(k) + " is NULL");
     if (what == WHAT_DENSITY && ns > 0 && (!out || !out[0])) return fail(c, PSB_EINVAL, "density output is NULL");
     if (what == WHAT_DIGEST && ns > 0 && (!dcount || !dhash)) return fail(c, PSB_EINVAL, "digest outputs are NULL");
@@ -169,6 +170,12 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     A.err = c->d_err;
     A.lut_d = c->lut_d;
     A.lut_f = c->lut_f;
+    if (adj) {
+        A.gout = c->adj_gout;
+        A.lam = c->adj_lam;
+        A.lam_stride = c->adj_lam_stride;
+        A.ha_out = (T*)c->adj_ha;
+    }
     for (size_t q = 0; q < colu.size(); ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
@@ -252,7 +259,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
             A.dig_hash = (uint64_t*)(obuf + 8 * ns);
             A.ha_out = (T*)(obuf + 16 * ns);
         }
-    } else {
+    } else if (!adj) {
         if (dev) {
             for (int q = 0; ns > 0 && q < L; ++q) A.out[q] = (T*)out[q];
         } else if (ns > 0 && L > 0) {
@@ -286,7 +293,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[3], s), "event");
 
     // ---- copy back ----
-    if (!dev && ns > 0) {
+    if (!dev && !adj && ns > 0) {
         if (what == WHAT_DIGEST) {
             PSB_CUDA_TRY(c, cudaMemcpyAsync(dcount, A.dig_count, 8 * ns, cudaMemcpyDeviceToHost, s), "digest D2H");
             PSB_CUDA_TRY(c, cudaMemcpyAsync(dhash, A.dig_hash, 8 * ns, cudaMemcpyDeviceToHost, s), "digest D2H");

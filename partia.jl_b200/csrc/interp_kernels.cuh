@@ -61,6 +61,12 @@ template <class T> struct Args {
     unsigned* err;
     unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests, [2] traversal steps
     SplitBufs sp;
+    // adjoint (FP64 interpolation only): with lam set, the output stage
+    // writes the cotangents of the per-sample sums, from the output
+    // cotangents gout[L][ns], to lam[q * lam_stride + k] instead of fields
+    const double* const* gout;
+    double* lam;
+    int64_t lam_stride;
     // single-kernel path over a device list of tiles (nullptr: every tile)
     const int32_t* tile_list;
     const unsigned* tile_count;
@@ -402,6 +408,30 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
             A.dig_count[k] = hcount;
             A.dig_hash[k] = hsum;
             if (A.ha_out) A.ha_out[k] = ha;
+        } else if (A.lam) {
+            // adjoint: cotangents of S1 (q = 0) and Sw_c (q = 1 + c), zero where S1 = 0
+            const double s1 = S1.get();
+            double l[1 + MAX_KC];
+            for (int q = 0; q <= kc; ++q) l[q] = 0.0;
+            if (s1 != 0.0) {
+                const double inv = 1.0 / s1;
+                for (int q = 0; q < A.rec.L; ++q) {
+                    const double go = A.gout[q][k];
+                    const int c = A.rec.a0[q];
+                    l[1 + c] += A.rec.a1[q] ? go * inv : go;
+                }
+                // Shepard terms: d(Sw_c/S1)/dS1 = -Sw_c/S1^2
+                for (int q = 0; q < A.rec.L; ++q) {
+                    if (!A.rec.a1[q]) continue;
+                    const int c = A.rec.a0[q];
+                    double swc = 0.0;
+#pragma unroll
+                    for (int cc = 0; cc < KC; ++cc)
+                        if (cc == c) swc = Sw[cc].get();
+                    l[0] -= A.gout[q][k] * swc * inv * inv;
+                }
+            }
+            for (int q = 0; q <= kc; ++q) A.lam[q * A.lam_stride + k] = l[q];
         } else {
             const double s1 = S1.get();
             const int L = A.rec.L;

@@ -1,0 +1,355 @@
+// k_adjoint.cuh -- adjoint (vector-Jacobian product) kernels.
+//
+// For a loss L = sum_s sum_k gout_k(s) out_k(s) the forward pass in FP64 first
+// writes, per sample, the cotangents lambda of its sums (S1, G, Dm, Dg, Sw_c,
+// Sg_c; write_sum_cotangents).  The kernels here then sum the pair terms per
+// PARTICLE, so that every gradient is accumulated by one thread and no float
+// atomics are needed:
+//   dL/dm_b   = sum_s (aS W + aG.gradW) / rho_b + lDm W + lDg.gradW
+//   dL/dA_c,b = sum_s m_b/rho_b (lSw_c W + lSg_c.gradW)
+//   dL/dx_b   = -sum_s m_b/rho_b (aS gradW + H aG) + m_b (lDm gradW + H lDg)
+// with aS = lS1 + sum_c lSw_c A_c,b, aG = lG + sum_c A_c,b lSg_c, W, gradW and
+// the Hessian H of the kernel at delta = x_s - x_b (averaged over h_a and h_b
+// in the symmetric strategy).  Densities and smoothing lengths are held fixed
+// (h_a from the nearest particle is piecewise constant in the positions).
+//
+// Point samples: one warp per 32 Morton-consecutive particles walks a second
+// LBVH built over the samples (node scale = subtree max of h_a) with the
+// forward's radius rules seen from the particle, and re-decides every pair
+// with the forward's exact arithmetic, so the pair set is the forward's.
+// Parallel-beam lines: one thread per particle visits the pixels whose lines
+// can pass within its support (the particle projected onto the frame plane)
+// and re-decides each pair with the forward's line distance.
+#pragma once
+
+#include "k_points.cuh"
+
+namespace psb {
+
+struct AdjArgs {
+    TreeView<double> pt;          // particles (Morton order)
+    TreeView<double> sv;          // samples, in the order of their own LBVH; h = h_a
+    const double* colT[MAX_KC];   // the catalog's distinct columns (particle Morton order)
+    int kc;
+    const double* lam;            // sum cotangents [q][sample] (sample-tree order for points)
+    int64_t lam_stride;
+    const int64_t* porder;        // particle Morton position -> caller's index
+    double* gm;
+    double* gx;
+    double* gy;
+    double* gz;
+    double* gcol[MAX_KC];         // gradient of catalog column c (caller's order), may be null
+    // parallel-beam lines
+    SampleSrc<double> beam;
+    int hmode;
+    const double* hs;
+    double ha_max;
+    const double* lut;
+    unsigned* err;
+    unsigned long long* stats;    // [0] pairs, [2] walk steps
+};
+
+// M4 at delta = x_s - x_b: W, gradW = sigma/h^5 g1(q) delta and the Hessian
+// (xx, yy, zz, xy, xz, yz) = sigma/h^5 (g1 I + g2 q delta delta^T / r^2), with
+// g1 = f'(q)/q and g2 = d g1/dq (kernels/M4_spline.jl:13-36).
+__device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r, double h, double& W, double g[3],
+                                         double H[6]) {
+    const double invh = 1.0 / h;
+    const double q = r * invh;
+    const double sig = inv_pi<double>();
+    const double ih3 = invh * invh * invh, ih5 = ih3 * invh * invh;
+    double f, g1, g2;
+    if (q < 1.0) {
+        f = 1.0 + q * q * (0.75 * q - 1.5);
+        g1 = 2.25 * q - 3.0;
+        g2 = 2.25;
+    } else if (q < 2.0) {
+        const double a = 2.0 - q;
+        f = 0.25 * a * a * a;
+        g1 = -0.75 * a * a / q;
+        g2 = 0.75 * a * (q + 2.0) / (q * q);
+    } else {
+        f = 0.0; g1 = 0.0; g2 = 0.0;
+    }
+    W = sig * ih3 * f;
+    const double c = sig * ih5 * g1;
+    const double e = (r2 > 0.0) ? sig * ih5 * g2 * q / r2 : 0.0;
+    g[0] = c * dl[0]; g[1] = c * dl[1]; g[2] = c * dl[2];
+    H[0] = c + e * dl[0] * dl[0]; H[1] = c + e * dl[1] * dl[1]; H[2] = c + e * dl[2] * dl[2];
+    H[3] = e * dl[0] * dl[1]; H[4] = e * dl[0] * dl[2]; H[5] = e * dl[1] * dl[2];
+}
+
+__device__ __forceinline__ void hmul(const double H[6], const double v[3], double o[3]) {
+    o[0] = H[0] * v[0] + H[3] * v[1] + H[4] * v[2];
+    o[1] = H[3] * v[0] + H[1] * v[1] + H[5] * v[2];
+    o[2] = H[4] * v[0] + H[5] * v[1] + H[2] * v[2];
+}
+
+struct AStage {
+    double sx[SPAN], sy[SPAN], sz[SPAN], sh[SPAN];  // samples of the span, h_a
+    double px[SPAN], py[SPAN], pz[SPAN], ph[SPAN];  // the warp's particles
+};
+
+template <int ST, int KC>
+__global__ void __launch_bounds__(128) k_adj_points(const AdjArgs A) {
+    __shared__ AStage stage_all[4];
+    const TreeView<double>& pt = A.pt;
+    const TreeView<double>& sv = A.sv;
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    AStage& st = stage_all[wib];
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (tile * 32 >= pt.n) return;  // warp-uniform
+    const int64_t b = tile * 32 + lane;
+    const bool valid = b < pt.n;
+    double xb[3] = {0.0, 0.0, 0.0}, hb = 0.0, mb = 0.0, rhob = 1.0, Ab[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) Ab[c] = 0.0;
+    if (valid) {
+        xb[0] = pt.x[b]; xb[1] = pt.y[b]; xb[2] = pt.z[b];
+        hb = pt.h[b]; mb = pt.m[b]; rhob = pt.rho[b];
+#pragma unroll
+        for (int c = 0; c < KC; ++c)
+            if (c < A.kc) Ab[c] = A.colT[c][b];
+    }
+    st.px[lane] = xb[0]; st.py[lane] = xb[1]; st.pz[lane] = xb[2]; st.ph[lane] = hb;
+    // this particle's own support radius^2, with the forward's operation order
+    const double rb = X<double>::mul(2.0, hb);
+    const double rb2 = X<double>::mul(rb, rb);
+    const double mr = mb / rhob;
+    double gm = 0.0, gx[3] = {0.0, 0.0, 0.0}, ga[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) ga[c] = 0.0;
+    const int kc = A.kc;
+    const int64_t L = A.lam_stride;
+    unsigned long long n_pairs = 0;
+    int64_t steps = 0;
+
+    auto pair = [&](int64_t li, double sxv, double syv, double szv, double ha) {
+        ++n_pairs;
+        const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
+        const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
+        const double r = sqrt(r2);
+        double W, g[3], H[6];
+        if (ST == ST_GATHER) {
+            m4_whess(dl, r2, r, ha, W, g, H);
+        } else if (ST == ST_SCATTER) {
+            m4_whess(dl, r2, r, hb, W, g, H);
+        } else {
+            double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
+            m4_whess(dl, r2, r, ha, Wa, ga3, Ha);
+            m4_whess(dl, r2, r, hb, Wb, gb3, Hb);
+            W = 0.5 * (Wa + Wb);
+            for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
+            for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
+        }
+        const double* lam = A.lam + li;
+        const double lS1 = __ldg(&lam[0]);
+        const double lG[3] = {__ldg(&lam[L]), __ldg(&lam[2 * L]), __ldg(&lam[3 * L])};
+        const double lDm = __ldg(&lam[4 * L]);
+        const double lDg[3] = {__ldg(&lam[5 * L]), __ldg(&lam[6 * L]), __ldg(&lam[7 * L])};
+        double aS = lS1, aG[3] = {lG[0], lG[1], lG[2]};
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                const double lsw = __ldg(&lam[(8 + c) * L]);
+                const double lsg[3] = {__ldg(&lam[(8 + kc + 3 * c) * L]), __ldg(&lam[(9 + kc + 3 * c) * L]),
+                                       __ldg(&lam[(10 + kc + 3 * c) * L])};
+                aS += lsw * Ab[c];
+                aG[0] += Ab[c] * lsg[0]; aG[1] += Ab[c] * lsg[1]; aG[2] += Ab[c] * lsg[2];
+                ga[c] += mr * (lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2]);
+            }
+        }
+        gm += (aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2]) / rhob + lDm * W + lDg[0] * g[0] +
+              lDg[1] * g[1] + lDg[2] * g[2];
+        double Ha[3], Hd[3];
+        hmul(H, aG, Ha);
+        hmul(H, lDg, Hd);
+        for (int d = 0; d < 3; ++d) gx[d] -= mr * (aS * g[d] + Ha[d]) + mb * (lDm * g[d] + Hd[d]);
+    };
+
+    // node test seen from the particle: the largest sample radius in the node
+    // (node scale = max h_a) for gather, the particle's own for scatter
+    auto node_fn = [&](int ni) -> bool {
+        const double d2n = ex_d2_pbox<double>(xb, sv, ni);
+        double r2;
+        if (ST == ST_SCATTER) {
+            r2 = rb2;
+        } else {
+            const double rs = X<double>::mul(2.0, __ldg(&sv.nscale[ni]));
+            const double rs2 = X<double>::mul(rs, rs);
+            r2 = (ST == ST_GATHER) ? rs2 : jmax(rs2, rb2);
+        }
+        return !(d2n > r2);
+    };
+    auto span_fn = [&](int64_t lo, int cnt, bool part) {
+        __syncwarp();
+        if (lane < cnt) {
+            st.sx[lane] = __ldg(&sv.x[lo + lane]); st.sy[lane] = __ldg(&sv.y[lo + lane]);
+            st.sz[lane] = __ldg(&sv.z[lo + lane]); st.sh[lane] = __ldg(&sv.h[lo + lane]);
+        }
+        __syncwarp();
+        const unsigned parts = __ballot_sync(PSB_FULL, part);
+        if (!parts) return;
+        // lane j holds sample j; the forward's pair test for every participating particle
+        const int j = lane < cnt ? lane : 0;
+        const double ps[3] = {st.sx[j], st.sy[j], st.sz[j]};
+        const double ra = X<double>::mul(2.0, st.sh[j]);
+        const double ra2 = X<double>::mul(ra, ra);
+        unsigned acc = 0;
+        for (unsigned pp = parts; pp; pp &= pp - 1) {
+            const int s = __ffs(pp) - 1;
+            const double e2 = ex_d2_pp<double>(ps, st.px[s], st.py[s], st.pz[s]);
+            const bool in = (lane < cnt) && (e2 <= ex_r2<ST, double>(ra2, st.ph[s]));
+            const unsigned bi = __ballot_sync(PSB_FULL, in);
+            if (lane == s) acc = bi;
+        }
+        for (; acc; acc &= acc - 1) {
+            const int jj = __ffs(acc) - 1;
+            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj]);
+        }
+    };
+    const int32_t start = (sv.root == 0) ? (int32_t)sv.n : sv.root;
+    const bool ok = warp_traverse_spans(start, sv.n, sv.links, sv.escape, valid, node_fn, span_fn, steps);
+
+    if (valid) {
+        const int64_t o = A.porder[b];
+        A.gm[o] = gm;
+        A.gx[o] = gx[0]; A.gy[o] = gx[1]; A.gz[o] = gx[2];
+#pragma unroll
+        for (int c = 0; c < KC; ++c)
+            if (c < kc && A.gcol[c]) A.gcol[c][o] = ga[c];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+    if (lane == 0 && A.stats) {
+        atomicAdd(&A.stats[0], n_pairs);
+        atomicAdd(&A.stats[2], (unsigned long long)steps);
+    }
+    if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+// line-integrated kernel and its r-derivative: the slope of the table segment
+// that line_W interpolates on
+__device__ __forceinline__ void line_Wd(double r, double h, const double* lut, double& W, double& dW) {
+    const double invh = 1.0 / h;
+    const double q = r * invh;
+    if (q >= 2.0) { W = 0.0; dW = 0.0; return; }
+    const double dq = 2.0 / 4095.0;
+    const double idxf = q / dq + 1.0;
+    int i = (int)idxf;
+    i = i < 1 ? 1 : (i > LUT_N - 1 ? LUT_N - 1 : i);
+    const double t = idxf - (double)i;
+    W = invh * (lut[i - 1] * (1.0 - t) + lut[i] * t);
+    dW = invh * invh * (lut[i] - lut[i - 1]) / dq;
+}
+
+template <int ST, int KC>
+__global__ void __launch_bounds__(128) k_adj_beam(const AdjArgs A) {
+    const TreeView<double>& pt = A.pt;
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= pt.n) return;
+    const double xb[3] = {pt.x[b], pt.y[b], pt.z[b]};
+    const double hb = pt.h[b], mb = pt.m[b], rhob = pt.rho[b], mr = mb / rhob;
+    const int kc = A.kc;
+    double Ab[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) Ab[c] = (c < kc) ? A.colT[c][b] : 0.0;
+    const SampleSrc<double>& B = A.beam;
+    const double* f = B.frame;
+    // the particle on the frame plane (frame axes orthonormal)
+    const double v[3] = {xb[0] - f[0], xb[1] - f[1], xb[2] - f[2]};
+    const double xi = v[0] * f[3] + v[1] * f[4] + v[2] * f[5];
+    const double eta = v[0] * f[6] + v[1] * f[7] + v[2] * f[8];
+    const double R = 2.0 * fmax(hb, A.ha_max) * (1.0 + 1e-9) + 1e-300;
+    const double dxi = (B.params[1] - B.params[0]) / (double)(B.nx - 1);
+    const double deta = (B.params[3] - B.params[2]) / (double)(B.ny - 1);
+    auto range = [](double c, double R, double lo0, double d, int64_t n, int64_t& a, int64_t& z) {
+        double u0 = (c - R - lo0) / d, u1 = (c + R - lo0) / d;
+        if (u0 > u1) { double t = u0; u0 = u1; u1 = t; }
+        u0 = floor(u0) - 1.0;
+        u1 = ceil(u1) + 1.0;
+        a = u0 < 0.0 ? 0 : (u0 > (double)(n - 1) ? n : (int64_t)u0);
+        z = u1 > (double)(n - 1) ? n - 1 : (u1 < 0.0 ? -1 : (int64_t)u1);
+    };
+    int64_t i0, i1, j0, j1;
+    range(xi, R, B.params[0], dxi, B.nx, i0, i1);
+    range(eta, R, B.params[2], deta, B.ny, j0, j1);
+    const double rb = X<double>::mul(2.0, hb);
+    (void)rb;
+    double gm = 0.0, gx[3] = {0.0, 0.0, 0.0}, ga[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) ga[c] = 0.0;
+    const int64_t L = A.lam_stride;
+    unsigned long long n_pairs = 0;
+    for (int64_t j = j0; j <= j1; ++j) {
+        for (int64_t i = i0; i <= i1; ++i) {
+            const int64_t k = i + B.nx * j;
+            double o[3], m[3];
+            sample_coords(B, k, o, m);
+            double ha = 0.0;
+            if (ST != ST_SCATTER) ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
+            const double ra = X<double>::mul(2.0, ha);
+            const double ra2 = X<double>::mul(ra, ra);
+            const double e2 = ex_d2_line<double>(o, m, xb[0], xb[1], xb[2]);
+            if (!(e2 <= ex_r2<ST, double>(ra2, hb))) continue;
+            ++n_pairs;
+            const double dr = sqrt(e2 < 0.0 ? 0.0 : e2);
+            double W, dW;
+            if (ST == ST_GATHER) {
+                line_Wd(dr, ha, A.lut, W, dW);
+            } else if (ST == ST_SCATTER) {
+                line_Wd(dr, hb, A.lut, W, dW);
+            } else {
+                double Wa, da, Wb, db;
+                line_Wd(dr, ha, A.lut, Wa, da);
+                line_Wd(dr, hb, A.lut, Wb, db);
+                W = 0.5 * (Wa + Wb);
+                dW = 0.5 * (da + db);
+            }
+            double aS = __ldg(&A.lam[k]);
+#pragma unroll
+            for (int c = 0; c < KC; ++c) {
+                if (c < kc) {
+                    const double lsw = __ldg(&A.lam[(1 + c) * L + k]);
+                    aS += lsw * Ab[c];
+                    ga[c] += mr * lsw * W;
+                }
+            }
+            gm += aS * W / rhob;
+            if (dr > 0.0) {
+                // d r_perp / d x_b = (D - (D.m) m) / r_perp, D = x_b - o
+                const double D[3] = {xb[0] - o[0], xb[1] - o[1], xb[2] - o[2]};
+                const double Dm = D[0] * m[0] + D[1] * m[1] + D[2] * m[2];
+                const double s = mr * aS * dW / dr;
+                for (int d = 0; d < 3; ++d) gx[d] += s * (D[d] - Dm * m[d]);
+            }
+        }
+    }
+    const int64_t ob = A.porder[b];
+    A.gm[ob] = gm;
+    A.gx[ob] = gx[0]; A.gy[ob] = gx[1]; A.gz[ob] = gx[2];
+#pragma unroll
+    for (int c = 0; c < KC; ++c)
+        if (c < kc && A.gcol[c]) A.gcol[c][ob] = ga[c];
+    if (A.stats && n_pairs) atomicAdd(&A.stats[0], n_pairs);
+}
+
+// sample coordinates of every sample of a source (grid, box) as arrays
+__global__ void k_sample_xyz(const SampleSrc<double> S, int64_t ns, double* x, double* y, double* z) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    double p[3], d[3];
+    sample_coords(S, k, p, d);
+    x[k] = p[0]; y[k] = p[1]; z[k] = p[2];
+}
+
+// lam_out[q][i] = lam_in[q][order[i]]: sum cotangents in the sample tree's order
+__global__ void k_gather_rows(const double* in, const int64_t* order, int64_t n, int nq, double* out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t s = order[i];
+    for (int q = 0; q < nq; ++q) out[q * n + i] = in[q * n + s];
+}
+
+}  // namespace psb

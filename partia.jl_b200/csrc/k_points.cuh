@@ -44,12 +44,83 @@ template <class T, int KC> struct PStage<T, true, KC> {
     float thr[SPAN];    // nearest search: candidate threshold on the float d2
 };
 
+// Adjoint: cotangents of the per-sample sums S1, G, Dm, Dg, Sw_c, Sg_c for a
+// loss sum_o gout[o][k] out_o(k), i.e. the derivative of the output recipes
+// below.  Layout q: 0 S1 | 1-3 G | 4 Dm | 5-7 Dg | 8+c Sw_c | 8+kc+3c+d Sg_c.
+// Sums shifted by a0 (FP32C) are shifted back first.  All zero where S1 = 0
+// (every output NaN, nothing flows back).
+template <class T, class Acc, class CT, int KC>
+__device__ __forceinline__ void write_sum_cotangents(const Args<T>& A, int64_t k, const Acc& S1, const Acc (&G)[3],
+                                                     const Acc (&Sw)[KC], const Acc (&Sg)[KC][3], const Acc& Dm,
+                                                     const Acc (&Dg)[3], const CT (&a0)[KC]) {
+    const int kc = A.rec.kc;
+    const double s1 = S1.get();
+    const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
+    double sw[MAX_KC], sg[MAX_KC][3];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+        sw[c] = Sw[c].get() + (double)a0[c] * s1;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get() + (double)a0[c] * g[d];
+    }
+    const double dm = Dm.get();
+    double l[8 + 4 * MAX_KC];
+    for (int q = 0; q < 8 + 4 * kc; ++q) l[q] = 0.0;
+    double* lS1 = &l[0];
+    double* lG = &l[1];
+    double* lDm = &l[4];
+    double* lDg = &l[5];
+    double* lSw = &l[8];
+    double* lSg = &l[8 + kc];
+    if (s1 != 0.0) {
+        const double inv = 1.0 / s1, inv2 = inv * inv;
+        for (int o = 0; o < A.rec.L; ++o) {
+            const double go = A.gout[o][k];
+            const int op = A.rec.op[o];
+            const int a0i = A.rec.a0[o], a1 = A.rec.a1[o], a2 = A.rec.a2[o], a3 = A.rec.a3[o];
+            if (op == OP_SCALAR) {
+                if (a1) { lSw[a0i] += go * inv; *lS1 -= go * sw[a0i] * inv2; }
+                else lSw[a0i] += go;
+            } else if (op == OP_GRADC) {  // Sg_c[d] - G[d] Sw_c / S1
+                lSg[3 * a0i + a1] += go; lG[a1] -= go * sw[a0i] * inv; lSw[a0i] -= go * g[a1] * inv;
+                *lS1 += go * g[a1] * sw[a0i] * inv2;
+            } else if (op == OP_GRADD) {  // Dg[d] - G[d] Dm / S1
+                lDg[a1] += go; lG[a1] -= go * dm * inv; *lDm -= go * g[a1] * inv;
+                *lS1 += go * g[a1] * dm * inv2;
+            } else if (op == OP_DIV) {
+                const int cs[3] = {a0i, a1, a2};
+                for (int d = 0; d < 3; ++d) {
+                    const int c = cs[d];
+                    lSg[3 * c + d] += go; lG[d] -= go * sw[c] * inv; lSw[c] -= go * g[d] * inv;
+                    *lS1 += go * sw[c] * g[d] * inv2;
+                }
+            } else {  // OP_CURL: -Sg_a[ka] + Sg_b[kb] + Sw_a/S1 G[ka] - Sw_b/S1 G[kb]
+                int a, ka, b, kb;
+                if (a3 == 0) { a = a1; ka = 2; b = a2; kb = 1; }
+                else if (a3 == 1) { a = a2; ka = 0; b = a0i; kb = 2; }
+                else { a = a0i; ka = 1; b = a1; kb = 0; }
+                lSg[3 * a + ka] -= go; lSg[3 * b + kb] += go;
+                lG[ka] += go * sw[a] * inv; lG[kb] -= go * sw[b] * inv;
+                lSw[a] += go * g[ka] * inv; lSw[b] -= go * g[kb] * inv;
+                *lS1 -= go * (sw[a] * g[ka] - sw[b] * g[kb]) * inv2;
+            }
+        }
+    }
+    for (int q = 0; q < 8 + 4 * kc; ++q) A.lam[q * A.lam_stride + k] = l[q];
+    (void)dm;
+    (void)Dg;
+}
+
 // Output fields of one sample from its sums (general_interpolation.jl:128-214):
 // NaN everywhere when S1 = 0, then each recipe op in catalog order.
 template <class T, class Acc, class CT, int KC>
 __device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k, const Acc& S1, const Acc (&G)[3],
                                                      const Acc (&Sw)[KC], const Acc (&Sg)[KC][3], const Acc& Dm,
                                                      const Acc (&Dg)[3], const CT (&a0)[KC]) {
+    if (A.lam) {
+        write_sum_cotangents<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
+        return;
+    }
     const double s1 = S1.get();
     const int L = A.rec.L;
     if (s1 == 0.0) {
@@ -676,6 +747,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
 
     // ---- outputs ----
     if (valid) {
+        if (WHAT != WHAT_DIGEST && A.ha_out) A.ha_out[k] = ha;
         if (WHAT == WHAT_DIGEST) {
             A.dig_count[k] = hcount;
             A.dig_hash[k] = hsum;

@@ -257,6 +257,7 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
     }
 
     const bool tovf = __any_sync(PSB_FULL, ovf);
+    if (valid && A.ha_out) A.ha_out[k] = ha;
     A.sp.cnt[bt * 32 + lane] = tovf ? (uint8_t)0xFF : (uint8_t)nent;
     ((T*)A.sp.ha)[bt * 32 + lane] = ha;
     if (tovf && lane == 0) {

@@ -50,7 +50,17 @@ struct psb_ctx {
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };
-    Slot scratch[24];
+    Slot scratch[32];
+
+    // adjoint: while adj_lam is set, an FP64 interpolation call writes the
+    // cotangents of its per-sample sums (from the output cotangents adj_gout,
+    // a device array of L device pointers) to adj_lam and h_a to adj_ha,
+    // instead of output fields
+    const double* const* adj_gout = nullptr;
+    double* adj_lam = nullptr;
+    int64_t adj_lam_stride = 0;
+    void* adj_ha = nullptr;
+    struct psb_ctx* sctx = nullptr;  // LBVH over the samples of the last adjoint call
 
     cudaEvent_t ev[8] = {};
 };

@@ -74,6 +74,12 @@ _SIGS = {
     "psb_build_lbvh": ([_vp, _vp, _vp], C.c_int),
     "psb_get_tree": ([_vp] * 9, C.c_int),
     "psb_interp_points": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp], C.c_int),
+    "psb_adjoint_points": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                            _u32, _vp], C.c_int),
+    "psb_adjoint_grid": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp,
+                          _vp, _vp, _u32, _vp], C.c_int),
+    "psb_adjoint_beam": ([_vp, _vp, _vp, _i64, _i64, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                          _u32, _vp], C.c_int),
     "psb_interp_points_noalloc": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _vp],
                                   C.c_int),
     "psb_interp_grid": ([_vp, _vp, _i64, _vp, _i64, _vp, _i64, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp],

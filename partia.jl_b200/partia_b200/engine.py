@@ -156,6 +156,62 @@ class Context:
                                              (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
         return outs
 
+    # ---- adjoint ----
+    def _grad_outs(self, like_dev):
+        n = self.n
+        if like_dev:
+            import torch
+            mk = lambda: torch.zeros(n, dtype=torch.float64, device="cuda")
+        else:
+            mk = lambda: np.zeros(n, dtype=np.float64)
+        g = dict(m=mk(), x=mk(), y=mk(), z=mk(), cols=[mk() for _ in range(self.ncol)])
+        return g
+
+    def _gout(self, gout, dev):
+        if dev:
+            return list(gout)
+        return [np.ascontiguousarray(np.asarray(g, dtype=np.float64)) for g in gout]
+
+    def adjoint_points(self, sx, sy, sz, cat: CatalogC, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                       hs=None):
+        """dL/dm, dL/dA_c, dL/dx.. for L = sum_k sum_s gout[k][s] out_k(s), in the particles' given order."""
+        sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
+        dev = _is_dev(sx)
+        hsa = self._hs(hmode, hs)
+        go = self._gout(gout, dev)
+        g = self._grad_outs(dev)
+        self._chk(self.lib.psb_adjoint_points(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa),
+                                              strategy, C.byref(cat.c), _ptr_array(go), _ptr(g["m"]),
+                                              _ptr_array(g["cols"]), _ptr(g["x"]), _ptr(g["y"]), _ptr(g["z"]),
+                                              L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+        return g
+
+    def adjoint_grid(self, ax, ay, az, cat: CatalogC, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                     hs=None, device=False):
+        ax, ay, az = (np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in (ax, ay, az))
+        hsa = self._hs(hmode, hs)
+        go = self._gout(gout, device)
+        g = self._grad_outs(device)
+        self._chk(self.lib.psb_adjoint_grid(self.h, ax.ctypes.data, len(ax), ay.ctypes.data, len(ay),
+                                            az.ctypes.data, len(az), hmode, _ptr(hsa), strategy, C.byref(cat.c),
+                                            _ptr_array(go), _ptr(g["m"]), _ptr_array(g["cols"]), _ptr(g["x"]),
+                                            _ptr(g["y"]), _ptr(g["z"]), L.PSB_FLAG_DEVICE_PTRS if device else 0,
+                                            C.byref(self.last_stats)))
+        return g
+
+    def adjoint_beam(self, frame, params, nx, ny, cat: CatalogC, gout, strategy=L.PSB_SCATTER,
+                     hmode=L.PSB_H_PER_SAMPLE, hs=None, device=False):
+        fr = np.ascontiguousarray(np.asarray(frame, dtype=np.float64).reshape(12))
+        pa = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(4))
+        hsa = self._hs(hmode, hs)
+        go = self._gout(gout, device)
+        g = self._grad_outs(device)
+        self._chk(self.lib.psb_adjoint_beam(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, hmode, _ptr(hsa),
+                                            strategy, C.byref(cat.c), _ptr_array(go), _ptr(g["m"]),
+                                            _ptr_array(g["cols"]), _ptr(g["x"]), _ptr(g["y"]), _ptr(g["z"]),
+                                            L.PSB_FLAG_DEVICE_PTRS if device else 0, C.byref(self.last_stats)))
+        return g
+
     def interp_grid(self, ax, ay, az, cat: CatalogC, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, hs=None,
                     prec=L.PSB_PREC_FP64, out=None, device_out=False):
         ax, ay, az = (np.ascontiguousarray(np.asarray(a, dtype=self.dtype)) for a in (ax, ay, az))

@@ -1,0 +1,146 @@
+"""GPU adjoint against the oracle's (finite-difference-pinned) adjoint.
+
+dL/dm, dL/dA_c and dL/dx for L = sum_k sum_s gout[k][s] out_k(s): point
+samples for every strategy and h mode, every output kind; structured grids;
+parallel-beam line-integrated samples.  The GPU sums the pair terms per
+particle over an LBVH of the samples (or the pixel lattice); the oracle sums
+them per sample.  Tolerance: 1e-10 of each gradient array's max |value| (the
+two sum in different orders).
+"""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+if not has_gpu():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+from partia_b200 import _lib as L  # noqa: E402
+from partia_b200.engine import CatalogC, Context  # noqa: E402
+
+TOL = 1e-10
+CAT = dict(scalars=[0, 1, 3], shepard=[0, 1, 1], grads=[-1, 1], divs=[1, 2, 3], curls=[3, 2, 1])
+
+
+def particles(n, seed):
+    rng = np.random.default_rng(seed)
+    x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    m = rng.uniform(0.5, 1.5, n) / n
+    h = 1.3 * (1.0 / n) ** (1 / 3) * rng.uniform(0.6, 1.6, n)
+    rho = rng.uniform(0.5, 2.0, n)
+    cols = [rho.copy(), np.sin(3 * x) + y, -y + 0.3 * z, x * x + 0.2 * rng.standard_normal(n)]
+    return [x, y, z, m, h, rho], cols
+
+
+def setup(n, seed):
+    arrs, cols = particles(n, seed)
+    orc = O.Oracle(*arrs, cols=cols)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build(want_perm=False)
+    return orc, ctx
+
+
+def close(a, b, tol=TOL):
+    a, b = np.asarray(a), np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def compare(g, r, ncol):
+    for key in ("m", "x", "y", "z"):
+        assert close(g[key], r[key]) <= TOL, (key, close(g[key], r[key]))
+    for c in range(ncol):
+        if np.abs(r["cols"][c]).max() == 0:
+            assert np.abs(g["cols"][c]).max() == 0, c
+        else:
+            assert close(g["cols"][c], r["cols"][c]) <= TOL, (c, close(g["cols"][c], r["cols"][c]))
+
+
+@pytest.mark.parametrize("strategy", [L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC])
+@pytest.mark.parametrize("hmode", [L.PSB_H_NEAREST, L.PSB_H_PER_SAMPLE])
+def test_point_adjoint_matches_oracle(strategy, hmode):
+    orc, ctx = setup(6000, 101)
+    rng = np.random.default_rng(102)
+    ns = 3000
+    s = tuple(rng.uniform(-0.05, 1.05, ns) for _ in range(3))
+    hs = rng.uniform(0.02, 0.05, ns) if hmode == L.PSB_H_PER_SAMPLE else None
+    nl = O.Catalog(**CAT).L
+    gout = [rng.standard_normal(ns) for _ in range(nl)]
+    r = orc.adjoint_points(*s, O.Catalog(**CAT), gout, strategy=strategy, hmode=hmode, hs=hs)
+    g = ctx.adjoint_points(*s, CatalogC(**CAT), gout, strategy=strategy, hmode=hmode, hs=hs)
+    compare(g, r, 4)
+    assert ctx.last_stats.pairs > 0
+
+
+def test_point_adjoint_device_pointers_and_unused_column():
+    import torch
+    orc, ctx = setup(4000, 103)
+    rng = np.random.default_rng(104)
+    ns = 1500
+    s = tuple(rng.uniform(0.0, 1.0, ns) for _ in range(3))
+    spec = dict(scalars=[1], shepard=[1], grads=[1])  # columns 0, 2, 3 unused
+    gout = [rng.standard_normal(ns) for _ in range(4)]
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=O.SYMMETRIC)
+    ts = tuple(torch.from_numpy(a).cuda() for a in s)
+    tg = [torch.from_numpy(a).cuda() for a in gout]
+    g = ctx.adjoint_points(*ts, CatalogC(**spec), tg, strategy=L.PSB_SYMMETRIC)
+    g = {k: ([c.cpu().numpy() for c in v] if k == "cols" else v.cpu().numpy()) for k, v in g.items()}
+    compare(g, r, 4)
+    for c in (0, 2, 3):
+        assert np.abs(g["cols"][c]).max() == 0
+
+
+def test_grid_adjoint_matches_points():
+    orc, ctx = setup(5000, 105)
+    ax = np.linspace(0.05, 0.95, 14)
+    ay = np.linspace(0.1, 0.9, 11)
+    az = np.linspace(0.0, 1.0, 9)
+    ns = len(ax) * len(ay) * len(az)
+    rng = np.random.default_rng(106)
+    spec = dict(scalars=[0], shepard=[0], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])
+    gout = [rng.standard_normal(ns) for _ in range(8)]
+    X, Y, Z = np.meshgrid(ax, ay, az, indexing="ij")
+    s = (X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F"))
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=O.SYMMETRIC)
+    g = ctx.adjoint_grid(ax, ay, az, CatalogC(**spec), gout, strategy=L.PSB_SYMMETRIC)
+    compare(g, r, 4)
+
+
+@pytest.mark.parametrize("strategy", [L.PSB_SCATTER, L.PSB_GATHER, L.PSB_SYMMETRIC])
+def test_beam_adjoint_matches_oracle(strategy):
+    from partia_b200 import workloads as W
+    orc, ctx = setup(8000, 107)
+    fr = W.Frame((0.5, 0.5, 0.5), (0.3, -0.2, 1.0), (1.0, 0.0, -0.3))
+    fr.rotate(0.3, -0.2, 0.5)
+    farr = fr.as_array()
+    prm = np.array([-0.35, 0.3, -0.25, 0.3])
+    nx, ny = 40, 33
+    nl = nx * ny
+    rng = np.random.default_rng(108)
+    scal, shep = [0, 1], [0, 1]
+    gout = [rng.standard_normal(nl) for _ in scal]
+    hs = None if strategy == L.PSB_SCATTER else np.array([0.03])
+    hm = L.PSB_H_CONSTANT
+    ox = W.plane_coordinates(farr, (prm[0], prm[1], nx), (prm[2], prm[3], ny))
+    fw = tuple(np.full(nl, farr[9 + c]) for c in range(3))
+    r = orc.adjoint_lines(ox, fw, scal, gout, shepard=shep, strategy=strategy, hmode=O.H_CONSTANT, hs=hs)
+    g = ctx.adjoint_beam(farr, prm, nx, ny, CatalogC(scalars=scal, shepard=shep), gout, strategy=strategy,
+                         hmode=hm, hs=hs)
+    compare(g, r, 4)
+    assert ctx.last_stats.pairs > 0
+
+
+def test_adjoint_error_paths():
+    orc, ctx = setup(500, 109)
+    s = (np.array([0.5]), np.array([0.5]), np.array([0.5]))
+    with pytest.raises(L.PsbError):  # gather needs hs unless nearest
+        ctx.adjoint_points(*s, CatalogC(scalars=[0]), [np.ones(1)], strategy=L.PSB_GATHER,
+                           hmode=L.PSB_H_PER_SAMPLE, hs=None)
+    # a frame whose right and up axes coincide
+    bad = np.array([0, 0, 0, 1, 0, 0, 1, 0, 0, 0, 0, 1], dtype=float)
+    with pytest.raises(L.PsbError):
+        ctx.adjoint_beam(bad, np.array([0.0, 1.0, 0.0, 1.0]), 4, 4, CatalogC(scalars=[0]), [np.ones(16)])

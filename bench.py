@@ -146,6 +146,98 @@ def make_workload():
     return d, axis
 
 
+def timed_call(fn, stream, steps, warmup):
+    """Median device time (ms) of fn() over `steps` calls after `warmup`, CUDA events on `stream`."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(b))
+    return float(np.median(ms))
+
+
+def lines_and_adjoint(steps, warmup):
+    """The line-integrated configurations (clump particles, parallel beam through
+    the 30/45-degree frame over [0,1]^2, scatter, column density = plain scalar
+    rho): forward throughput of 8M particles x 1024^2 lines in FP32C and FP64,
+    and the adjoint of 0.5 ||Sigma - Sigma_target||^2 for 1M particles x 512^2
+    lines against its forward.  Particles and outputs stay on the device."""
+    import torch
+    from partia_b200 import _lib as L, workloads as W
+    from partia_b200.engine import CatalogC, Context
+    stream = torch.cuda.Stream()
+    fr = W.c3_frame().as_array()
+    prm = np.array([0.0, 1.0, 0.0, 1.0])
+    cat = CatalogC(scalars=[0], shepard=[0])
+    res = {}
+
+    def context(d, h, rho):
+        ctx = Context(0)
+        L.load().psb_set_stream(ctx.h, stream.cuda_stream)
+        ctx.set_particles(d["x"], d["y"], d["z"], d["m"], h, rho, [rho])
+        ctx.build(want_perm=False)
+        return ctx
+
+    # 8M particles, 1024^2 lines
+    d = W.clumps(8_000_000, 2)
+    h, rho = W.density_h(d)
+    ctx = context(d, h, rho)
+    npix = 1024
+    out32 = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
+    out64 = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
+    f32 = lambda: ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP32C, out=out32)
+    f64 = lambda: ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP64, out=out64)
+    t32 = timed_call(f32, stream, steps, warmup)
+    pairs = ctx.last_stats.pairs
+    t64 = timed_call(f64, stream, max(2, steps // 2), 1)
+    a, b = out32[0], out64[0]
+    fin = torch.isfinite(b)
+    err = ((a[fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
+    res["lines"] = {"workload": "clumps-8M column density, 1024^2 parallel beam, scatter", "N": 8_000_000,
+                    "lines": npix * npix, "pairs": int(pairs), "fp32c_ms": t32, "fp64_ms": t64,
+                    "lines_per_s": npix * npix / (t32 / 1e3), "fp64_lines_per_s": npix * npix / (t64 / 1e3),
+                    "speedup_fp32c_vs_fp64": t64 / t32, "fp32c_rel_err_vs_fp64": err}
+    ctx.close()
+    del out32, out64
+
+    # 1M particles, 512^2 lines: forward and adjoint
+    d = W.clumps(1_000_000, 3)
+    h, rho = W.density_h(d)
+    ctx = context(d, h, rho)
+    rng = np.random.default_rng(1003)
+    dt = dict(d)
+    dt["m"] = d["m"] * (1.0 + 0.1 * rng.standard_normal(len(d["m"])))
+    for k in ("x", "y", "z"):
+        dt[k] = d[k] + 0.002 * rng.standard_normal(len(d[k]))
+    npix = 512
+    tgt = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
+    ctx_t = context(dt, h, rho)
+    ctx_t.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP64, out=tgt)
+    ctx_t.close()
+    sig = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
+    fwd = lambda: ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP32C, out=sig)
+    tf = timed_call(fwd, stream, steps, warmup)
+    fwd64 = lambda: ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP64, out=sig)
+    tf64 = timed_call(fwd64, stream, max(2, steps // 2), 1)
+    gout = [torch.nan_to_num(sig[0] - tgt[0])]
+    bwd = lambda: ctx.adjoint_beam(fr, prm, npix, npix, cat, gout, strategy=L.PSB_SCATTER, device=True)
+    tb = timed_call(bwd, stream, steps, warmup)
+    res["adjoint"] = {"workload": "clumps-1M column density, 512^2 parallel beam, loss 0.5||Sigma - Sigma_target||^2",
+                      "N": 1_000_000, "lines": npix * npix, "pairs": int(ctx.last_stats.pairs),
+                      "forward_fp32c_ms": tf, "forward_fp64_ms": tf64, "backward_ms": tb,
+                      "grad_fwd_time_ratio": tb / tf, "grad_fwd_time_ratio_vs_fp64": tb / tf64,
+                      "gradients": "dL/dm, dL/drho-column, dL/dx (FP64)"}
+    ctx.close()
+    return res
+
+
 def cpu_reference(args, d, axis, steps, warmup, threads=None):
     """Oracle port on the host cores over a bounded random sample of grid points."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -210,6 +302,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=4.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-lines", action="store_true", help="skip the line-integrated and adjoint legs")
     args = ap.parse_args()
     NGRID = args.grid
     if args.impl == "reference":
@@ -348,6 +441,10 @@ def main():
     achieved = b_alg / (kern_ms / 1e3) / 1e9
     tr = ncu_traffic()
 
+    extra = None
+    if world == 1 and not args.no_lines:
+        extra = lines_and_adjoint(max(3, args.steps // 4), 2)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
@@ -373,7 +470,9 @@ def main():
                          "kernel": "k_points<double,FP32C,SYMMETRIC,4,INTERP>", "kernel_ms": kern_ms,
                          "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg),
                          "warp_steps_per_launch": int(ctx_steps)},
-            "fp64": fp64, "fp32c_rel_err_vs_fp64": errs, "grad_fwd_time_ratio": None,
+            "fp64": fp64, "fp32c_rel_err_vs_fp64": errs,
+            "grad_fwd_time_ratio": extra["adjoint"]["grad_fwd_time_ratio"] if extra else None,
+            "lines": extra["lines"] if extra else None, "adjoint": extra["adjoint"] if extra else None,
             "build_ms": build_ms,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

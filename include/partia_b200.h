@@ -277,7 +277,10 @@ int psb_neighbor_digest(psb_ctx* ctx, int32_t kind, int64_t ns,
  * given to psb_set_particles.  Densities, smoothing lengths and the sample h
  * (hs, or the nearest particle's h, which is piecewise constant in the
  * positions) are held fixed.  Double particle data only (else
- * PSB_EUNSUPPORTED); the forward sums are recomputed in PSB_PREC_FP64.  The
+ * PSB_EUNSUPPORTED).  The forward sums are recomputed in PSB_PREC_FP64 where
+ * the cotangents depend on them (Shepard ratios, gradients, divergences,
+ * curls, or a nearest-particle h); a catalog of plain scalars (e.g. column
+ * density) needs no forward pass.  The
  * pair terms are summed per particle by a traversal of an LBVH over the
  * samples (points, grids), or of the pixel lattice (beams), with the forward's
  * inclusion arithmetic: no float atomics.  gout, hs and the gradient arrays

@@ -1,7 +1,7 @@
 // adjoint_host.cu -- host drivers of the adjoint entry points: stage the
-// samples and the output cotangents, run the FP64 forward pass in its
-// sum-cotangent mode, build the LBVH over the samples (points) and run the
-// particle-centric kernels, then return dL/dm, dL/dA_c and dL/dx per particle
+// samples and the output cotangents, obtain the sum cotangents (directly, or
+// from the FP64 forward pass in its sum-cotangent mode), build the LBVH over
+// the samples (points) and run the particle-centric kernels, then return dL/dm, dL/dA_c and dL/dx per particle
 // in the order the particles were given to psb_set_particles.
 #include <algorithm>
 #include <cmath>
@@ -33,6 +33,24 @@ static void launch_adj_beam_k(const AdjArgs& a, int st, unsigned g, cudaStream_t
     if (st == ST_GATHER) k_adj_beam<ST_GATHER, KC><<<g, 128, 0, s>>>(a);
     else if (st == ST_SCATTER) k_adj_beam<ST_SCATTER, KC><<<g, 128, 0, s>>>(a);
     else k_adj_beam<ST_SYMMETRIC, KC><<<g, 128, 0, s>>>(a);
+}
+
+// Sum cotangents that do not depend on the forward sums: a catalog of
+// scalars without Shepard normalisation (lambda_Sw_c = the sum of the output
+// cotangents of column c, every other cotangent zero).
+__global__ void k_direct_cotangents(const Recipe rec, const double* const* gout, int64_t ns, int nq, bool line,
+                                    double* lam) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= ns) return;
+    for (int q = 0; q < nq; ++q) lam[q * ns + k] = 0.0;
+    const int base = line ? 1 : 8;  // Sw_c sits at q = 1 + c (lines) or 8 + c (points)
+    for (int o = 0; o < rec.L; ++o) lam[(base + rec.a0[o]) * ns + k] += gout[o][k];
+}
+
+// h_a of every sample from hs (per sample, or one constant)
+__global__ void k_fill_ha(const double* hs, bool per_sample, int64_t ns, double* ha) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < ns) ha[k] = per_sample ? hs[k] : hs[0];
 }
 
 // clears the adjoint hook of the context on every exit path
@@ -166,8 +184,19 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
         PSB_CUDA_TRY(c, cudaMemsetAsync(ha, 0, sizeof(double) * ns, s), "memset");
         PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");  // host staging buffers are released below
 
-        // ---- forward pass in FP64 writing the sum cotangents ----
-        {
+        // ---- sum cotangents: directly from gout when the catalog allows and
+        // h_a needs no nearest search, else a forward pass in FP64 ----
+        bool direct = true;
+        for (int o = 0; o < L; ++o)
+            if (rec.op[o] != OP_SCALAR || rec.a1[o]) direct = false;
+        if (!line && st != ST_SCATTER && hmode == PSB_H_NEAREST) direct = false;
+        if (direct) {
+            const unsigned gb = (unsigned)((ns + 255) / 256);
+            k_direct_cotangents<<<gb, 256, 0, s>>>(rec, gptr, ns, nq, line, lam);
+            if (need_h) k_fill_ha<<<gb, 256, 0, s>>>(hsd, hmode == PSB_H_PER_SAMPLE, ns, ha);
+            PSB_CUDA_TRY(c, cudaGetLastError(), "cotangent kernel");
+            launches += need_h ? 2 : 1;
+        } else {
             AdjHook hook{c};
             c->adj_gout = gptr;
             c->adj_lam = lam;

@@ -80,6 +80,31 @@ def clumps(n, seed, nclump=64, frac_clump=0.9):
                 z=np.ascontiguousarray(p[:, 2]), m=np.full(n, 1.0 / n))
 
 
+def density_h(d, iters=3, eta=1.2, device=0):
+    """Smoothing lengths and densities from the density sum (the clump
+    configurations' recipe): h0 = eta (m / rho0)^(1/3) with rho0 the mean
+    density (total mass over the unit cube), then `iters` rounds of
+    rho = sum_b m_b W(|x - x_b|, h) (gather at the particles, M4) and
+    h = eta (m / rho)^(1/3).  Runs on the GPU through the library; returns
+    (h, rho) with rho the last density sum."""
+    from . import _lib as L
+    from .engine import Context
+    x, y, z, m = d["x"], d["y"], d["z"], d["m"]
+    rho0 = float(np.sum(m))
+    h = eta * (m / rho0) ** (1.0 / 3.0)
+    ctx = Context(device)
+    rho = None
+    try:
+        for _ in range(iters):
+            ctx.set_particles(x, y, z, m, h, np.ones_like(m))
+            ctx.build(want_perm=False)
+            rho = ctx.density(x, y, z, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=h)
+            h = eta * (m / rho) ** (1.0 / 3.0)
+    finally:
+        ctx.close()
+    return h, rho
+
+
 def cell_centre_axis(n, lo=0.0, hi=1.0):
     d = (hi - lo) / n
     return (lo + 0.5 * d, hi - 0.5 * d, n)

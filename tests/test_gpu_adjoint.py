@@ -134,6 +134,38 @@ def test_beam_adjoint_matches_oracle(strategy):
     assert ctx.last_stats.pairs > 0
 
 
+@pytest.mark.parametrize("strategy,hmode", [(L.PSB_SCATTER, L.PSB_H_NEAREST), (L.PSB_GATHER, L.PSB_H_PER_SAMPLE),
+                                            (L.PSB_SYMMETRIC, L.PSB_H_CONSTANT)])
+def test_plain_scalar_adjoint_without_forward_pass(strategy, hmode):
+    """Plain (non-Shepard) scalars: the sum cotangents are the output
+    cotangents themselves, so no forward pass runs; points and beams."""
+    from partia_b200 import workloads as W
+    orc, ctx = setup(5000, 111)
+    rng = np.random.default_rng(112)
+    ns = 2000
+    s = tuple(rng.uniform(0.0, 1.0, ns) for _ in range(3))
+    hs = {L.PSB_H_NEAREST: None, L.PSB_H_PER_SAMPLE: rng.uniform(0.02, 0.05, ns),
+          L.PSB_H_CONSTANT: np.array([0.035])}[hmode]
+    spec = dict(scalars=[0, 2, 0], shepard=[0, 0, 0])
+    gout = [rng.standard_normal(ns) for _ in range(3)]
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=strategy, hmode=hmode, hs=hs)
+    g = ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy, hmode=hmode, hs=hs)
+    compare(g, r, 4)
+    if strategy != L.PSB_SCATTER and hmode == L.PSB_H_NEAREST:
+        return
+    fr = W.c3_frame().as_array()
+    prm = np.array([0.0, 1.0, 0.0, 1.0])
+    nx = ny = 37
+    gl = [rng.standard_normal(nx * ny)]
+    hl = None if strategy == L.PSB_SCATTER else np.array([0.03])
+    ox = W.plane_coordinates(fr, (0.0, 1.0, nx), (0.0, 1.0, ny))
+    fw = tuple(np.full(nx * ny, fr[9 + c]) for c in range(3))
+    r = orc.adjoint_lines(ox, fw, [0], gl, shepard=[0], strategy=strategy, hmode=O.H_CONSTANT, hs=hl)
+    g = ctx.adjoint_beam(fr, prm, nx, ny, CatalogC(scalars=[0], shepard=[0]), gl, strategy=strategy,
+                         hmode=L.PSB_H_CONSTANT, hs=hl)
+    compare(g, r, 4)
+
+
 def test_adjoint_error_paths():
     orc, ctx = setup(500, 109)
     s = (np.array([0.5]), np.array([0.5]), np.array([0.5]))

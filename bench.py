@@ -54,7 +54,7 @@ def peaks():
 def ncu_traffic():
     """DRAM bytes per launch of the point kernel from the committed ncu summary."""
     try:
-        with open(os.path.join(ROOT, "profiles", "k_points_c2_traffic.json")) as f:
+        with open(os.path.join(ROOT, "profiles", "split_c2_traffic.json")) as f:
             return json.load(f)
     except Exception:
         return None
@@ -467,7 +467,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind,
                          "traffic": (tr or {}).get("bytes_per_launch") if tr else None,
-                         "kernel": "k_points<double,FP32C,SYMMETRIC,4,INTERP>", "kernel_ms": kern_ms,
+                         "kernel": "k_collect + k_bodies <double,FP32C,SYMMETRIC,4> (pair lists, pair sums)", "kernel_ms": kern_ms,
                          "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg),
                          "warp_steps_per_launch": int(ctx_steps)},
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs,

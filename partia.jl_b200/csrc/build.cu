@@ -305,7 +305,8 @@ __global__ void k_span_roots(int64_t n, const int32_t* parent, const int32_t* rl
 // exact coordinates (anchor 0).
 template <class T>
 __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, const T* h, const T* m, const T* rho,
-                              const int32_t* sfirst, float4* leaf4, float* mrho, float* mf, float4* leafK) {
+                              const int32_t* sfirst, float4* leaf4, float* mrho, float* mf, float4* leafK,
+                              float2* spanb) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double ax = 0, ay = 0, az = 0;
@@ -328,6 +329,12 @@ __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, con
     const float ih = 1.f / r.w;
     const float s3 = 0.318309886183790671538f * ih * ih * ih;
     leafK[i] = make_float4(ih, s3, s3 * ih, mr);
+    // span bounds: max |offset|_1 and max h, rounded up (non-negative floats
+    // order like their bit patterns); spanb starts at zero
+    const float l1 = (fabsf(r.x) + fabsf(r.y) + fabsf(r.z)) * 1.0000005f;
+    const float hu = __double2float_ru((double)h[i]);
+    atomicMax((int*)&spanb[sfirst[i]].x, __float_as_int(l1));
+    atomicMax((int*)&spanb[sfirst[i]].y, __float_as_int(hu));
 }
 
 __global__ void k_to_float(const double* src, int64_t n, float* dst) {
@@ -431,6 +438,8 @@ static int build_typed(psb_ctx* c) {
     PSB_CUDA_TRY(c, cudaMalloc(&c->mrho, sizeof(float) * n), "cudaMalloc mrho");
     PSB_CUDA_TRY(c, cudaMalloc(&c->mf, sizeof(float) * n), "cudaMalloc mf");
     PSB_CUDA_TRY(c, cudaMalloc(&c->leafK, sizeof(float4) * n), "cudaMalloc leafK");
+    PSB_CUDA_TRY(c, cudaMalloc(&c->spanb, sizeof(float2) * n), "cudaMalloc span bounds");
+    PSB_CUDA_TRY(c, cudaMemsetAsync(c->spanb, 0, sizeof(float2) * n, s), "memset span bounds");
     if (nint > 0)
         k_pack_nodes<T><<<grid_for(nint), BT, 0, s>>>(nint, (const T*)c->nmin[0], (const T*)c->nmin[1],
                                                       (const T*)c->nmin[2], (const T*)c->nmax[0], (const T*)c->nmax[1],
@@ -440,7 +449,7 @@ static int build_typed(psb_ctx* c) {
     k_span_roots<<<grid_for(n), BT, 0, s>>>(n, c->parent, c->range_lo, c->range_hi, sfirst);
     k_pack_leaves<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->x, (const T*)c->y, (const T*)c->z, (const T*)c->h,
                                                 (const T*)c->m, (const T*)c->rho, sfirst, c->leaf4, c->mrho, c->mf,
-                                                c->leafK);
+                                                c->leafK, c->spanb);
     if (sizeof(T) == 8 && c->ncol > 0) {
         PSB_CUDA_TRY(c, cudaMalloc(&c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
         for (int k = 0; k < c->ncol; ++k)

@@ -54,7 +54,7 @@ void free_tree(psb_ctx* c) {
     for (int d = 0; d < 3; ++d) { dfree(c->nmin[d]); dfree(c->nmax[d]); }
     dfree(c->nscale);
     dfree_t(c->node_lo); dfree_t(c->node_hi); dfree_t(c->leaf4);
-    dfree_t(c->mrho); dfree_t(c->mf); dfree_t(c->leafK); dfree_t(c->colsf);
+    dfree_t(c->mrho); dfree_t(c->mf); dfree_t(c->leafK); dfree_t(c->spanb); dfree_t(c->colsf);
     c->built = false;
     c->root = 0;
 }

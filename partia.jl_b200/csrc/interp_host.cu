@@ -29,7 +29,7 @@ template <class T> TreeView<T> tree_view(psb_ctx* c) {
     v.cols = (const T* const*)c->d_cols;
     v.ncol = c->ncol;
     v.node_lo = c->node_lo; v.node_hi = c->node_hi; v.leaf4 = c->leaf4;
-    v.mrho = c->mrho; v.mf = c->mf; v.leafK = c->leafK;
+    v.mrho = c->mrho; v.mf = c->mf; v.leafK = c->leafK; v.spanb = c->spanb;
     v.coord_err = c->coord_err;
     return v;
 }

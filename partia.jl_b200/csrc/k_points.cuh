@@ -195,11 +195,14 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
             if (__ldg(&tv.codes[mid]) < code) lo = mid + 1;
             else hi = mid;
         }
-        const int64_t c0 = lo > 0 ? lo - 1 : 0;
-        const int64_t c1 = lo < tv.n ? lo : tv.n - 1;
-        const double d0 = (double)ex_d2_pp<T>(p, tv.x[c0], tv.y[c0], tv.z[c0]);
-        const double d1 = (double)ex_d2_pp<T>(p, tv.x[c1], tv.y[c1], tv.z[c1]);
-        if (d1 < d0) { best = d1; bidx = c1; } else { best = d0; bidx = c0; }
+        // the (up to) four particles around that position in Morton order, in
+        // increasing index: the first strict minimum keeps the smallest index
+        const int64_t c0 = lo >= 2 ? lo - 2 : 0;
+        const int64_t c1 = (lo + 2 <= tv.n) ? lo + 2 : tv.n;
+        for (int64_t ci = c0; ci < c1; ++ci) {
+            const double dc = (double)ex_d2_pp<T>(p, tv.x[ci], tv.y[ci], tv.z[ci]);
+            if (dc < best) { best = dc; bidx = ci; }
+        }
     }
     auto better = [&](double d2, int64_t li) { return d2 < best || (d2 == best && li < bidx); };
     auto node_fn = [&](int ni) -> bool {
@@ -216,9 +219,7 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
         if (!parts) return;
         unsigned cand = 0;
         if constexpr (BAND) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) eqmax = fmaxf(eqmax, __shfl_xor_sync(PSB_FULL, eqmax, o));
-            // candidates: float d2 not above (sqrt(best) + error)^2
+            // candidates: float d2 not above (sqrt(best) + error)^2 (eqmax is the span's bound)
             {
                 const float4 Pme = st.P[lane];
                 float bs = (float)sqrt(best);
@@ -311,24 +312,27 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         st.px[lane] = p[0]; st.py[lane] = p[1]; st.pz[lane] = p[2];
     }
 
-    // stage leaves [lo, lo+cnt): lane j takes leaf lo+j (all lanes call)
+    // stage leaves [lo, lo+cnt): lane j takes leaf lo+j (all lanes call).
+    // Returns the error bound of the float leaf positions Q (the same for the
+    // whole span): |Q - exact| <= U1 (|L|_1 + |o|_1 + |Q|_1) per leaf, and
+    // |Q|_1 <= (|L|_1 + |o|_1)(1 + U1), with max |L|_1 over the span stored.
     auto stage_span = [&](int64_t lo, int cnt, bool with_cols) -> float {
         __syncwarp();
         float eqmax = 0.f;
-        if (lane < cnt) {
+        if constexpr (BAND) {
+            // the span's leaves are stored relative to its first leaf
+            const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+            const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+            const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
+            const float lm = __ldg(&tv.spanb[lo]).x;
+            eqmax = U1 * (2.f * lm + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
+            if (lane < cnt) {
+                const float4 L = __ldg(&tv.leaf4[lo + lane]);
+                st.Q[lane] = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
+            }
+        } else if (lane < cnt) {
             const int64_t li = lo + lane;
-            if constexpr (BAND) {
-                const float4 L = __ldg(&tv.leaf4[li]);
-                // the span's leaves are stored relative to its first leaf
-                float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
-                float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
-                float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
-                float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
-                st.Q[lane] = make_float4(q0, q1, q2, L.w);
-                eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
-                              fabsf(q0) + fabsf(q1) + fabsf(q2));
-                st.eq[lane] = eqmax;
-            } else {
+            {
                 st.x[lane] = __ldg(&tv.x[li]); st.y[lane] = __ldg(&tv.y[li]); st.z[lane] = __ldg(&tv.z[li]);
                 st.h[lane] = __ldg(&tv.h[li]);
                 if (with_cols) {

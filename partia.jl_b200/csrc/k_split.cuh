@@ -20,8 +20,7 @@ template <class T, bool BAND> struct CStage {
     T px[SPAN], py[SPAN], pz[SPAN], ra2[SPAN], best[SPAN];
 };
 template <class T> struct CStage<T, true> {
-    float4 Q[SPAN];   // leaf position relative to the warp anchor, h
-    float eq[SPAN];   // error bound of Q
+    float4 Q[SPAN];   // leaf position relative to the warp anchor, h (nearest search)
     float4 P[SPAN];   // sample position relative to the warp anchor, error bound
     float2 R[SPAN];   // sample radius bounds
     float2 AB[SPAN];  // per-span squared thresholds of each sample
@@ -29,7 +28,7 @@ template <class T> struct CStage<T, true> {
 };
 
 template <class T, int PREC, int ST>
-__global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
+__global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
     constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
     __shared__ CStage<T, BAND> stage_all[4];
     const TreeView<T>& tv = A.tv;
@@ -64,26 +63,25 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
     }
 
     // positions of leaves [lo, lo+cnt): lane j takes leaf lo+j (all lanes call)
+    // (the span's float error bound is the same for every leaf; see k_points)
     auto stage_span = [&](int64_t lo, int cnt, bool) -> float {
         __syncwarp();
         float eqmax = 0.f;
-        if (lane < cnt) {
-            const int64_t li = lo + lane;
-            if constexpr (BAND) {
-                const float4 L = __ldg(&tv.leaf4[li]);
-                // the span's leaves are stored relative to its first leaf
-                float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
-                float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
-                float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
-                float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
-                st.Q[lane] = make_float4(q0, q1, q2, L.w);
-                eqmax = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
-                              fabsf(q0) + fabsf(q1) + fabsf(q2));
-                st.eq[lane] = eqmax;
-            } else {
-                st.x[lane] = __ldg(&tv.x[li]); st.y[lane] = __ldg(&tv.y[li]); st.z[lane] = __ldg(&tv.z[li]);
-                st.h[lane] = __ldg(&tv.h[li]);
+        if constexpr (BAND) {
+            // the span's leaves are stored relative to its first leaf
+            const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+            const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+            const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
+            const float lm = __ldg(&tv.spanb[lo]).x;
+            eqmax = U1 * (2.f * lm + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
+            if (lane < cnt) {
+                const float4 L = __ldg(&tv.leaf4[lo + lane]);
+                st.Q[lane] = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
             }
+        } else if (lane < cnt) {
+            const int64_t li = lo + lane;
+            st.x[lane] = __ldg(&tv.x[li]); st.y[lane] = __ldg(&tv.y[li]); st.z[lane] = __ldg(&tv.z[li]);
+            st.h[lane] = __ldg(&tv.h[li]);
         }
         __syncwarp();
         return eqmax;
@@ -162,38 +160,31 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
         auto span_fn = [&](int64_t lo, int cnt, bool part) {
             const unsigned parts = __ballot_sync(PSB_FULL, part);
             if (!parts) return;
-            float eq = 0.f, Aj = 0.f, Bj = 0.f, hb = 0.f;
-            __syncwarp();
-            if (lane < cnt) {
-                const int64_t li = lo + lane;
-                const float4 L = __ldg(&tv.leaf4[li]);
-                const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
-                const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
-                const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
-                const float q0 = L.x + o0, q1 = L.y + o1, q2 = L.z + o2;
-                hb = L.w;
-                st.Q[lane] = make_float4(q0, q1, q2, hb);
-                eq = U1 * (fabsf(L.x) + fabsf(L.y) + fabsf(L.z) + fabsf(o0) + fabsf(o1) + fabsf(o2) +
-                           fabsf(q0) + fabsf(q1) + fabsf(q2));
-            }
-            // error bound of float distances for this span, the same for every pair
-            float eqm = eq;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) eqm = fmaxf(eqm, __shfl_xor_sync(PSB_FULL, eqm, o));
-            const float rbhi = 2.f * hb * (1.f + 2.f * U1), rblo = 2.f * hb * (1.f - 2.f * U1);
+            // the span's anchor (first leaf) relative to the warp anchor and its
+            // bounds: one error bound E for every float distance of the span
+            const float o0 = (float)((double)__ldg(&tv.x[lo]) - cw[0]);
+            const float o1 = (float)((double)__ldg(&tv.y[lo]) - cw[1]);
+            const float o2 = (float)((double)__ldg(&tv.z[lo]) - cw[2]);
+            const float2 sb = __ldg(&tv.spanb[lo]);
+            const float eqm = U1 * (2.f * sb.x + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
+            // the rounding of r itself enters through 4 U1 r (r <= the larger radius)
             float rmax = rahimax;
-            if (ST != ST_GATHER) {
-                float rb = rbhi;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) rb = fmaxf(rb, __shfl_xor_sync(PSB_FULL, rb, o));
-                rmax = fmaxf(rmax, rb);
-            }
+            if (ST != ST_GATHER) rmax = fmaxf(rmax, 2.f * sb.y * (1.f + 2.f * U1));
             const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
-            if (ST != ST_GATHER && lane < cnt) {
-                const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
-                Aj = il * il;
-                Bj = ih2 * ih2;
+            // this lane's leaf (far away for lanes past the span: never in, never undecided)
+            float4 Q = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+            float Aj = 0.f, Bj = 0.f;
+            if (lane < cnt) {
+                const float4 L = __ldg(&tv.leaf4[lo + lane]);
+                Q = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
+                if (ST != ST_GATHER) {
+                    const float rbhi = 2.f * L.w * (1.f + 2.f * U1), rblo = 2.f * L.w * (1.f - 2.f * U1);
+                    const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
+                    Aj = il * il;
+                    Bj = ih2 * ih2;
+                }
             }
+            __syncwarp();
             {
                 float As = 0.f, Bs = 0.f;
                 if (ST != ST_SCATTER) {
@@ -204,19 +195,20 @@ __global__ void __launch_bounds__(128) k_collect(const Args<T> A) {
                 st.AB[lane] = make_float2(As, Bs);
             }
             __syncwarp();
-            const float4 Q = st.Q[lane < cnt ? lane : 0];
-            unsigned myacc = 0, myunc = 0;
+            // surely in: d2 < A; maybe in: d2 <= B (undecided = maybe and not surely)
+            unsigned myacc = 0, mymaybe = 0;
             for (unsigned pp = parts; pp; pp &= pp - 1) {
                 const int s = __ffs(pp) - 1;
                 const float4 P = st.P[s];
                 const float2 AB = st.AB[s];
                 const float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
                 const float d2 = dx * dx + dy * dy + dz * dz;
-                const bool in = (lane < cnt) && d2 < fmaxf(AB.x, Aj);
-                const bool un = (lane < cnt) && !in && !(d2 > fmaxf(AB.y, Bj));
-                const unsigned bi = __ballot_sync(PSB_FULL, in), bu = __ballot_sync(PSB_FULL, un);
-                if (lane == s) { myacc = bi; myunc = bu; }
+                const float At = (ST == ST_GATHER) ? AB.x : ((ST == ST_SCATTER) ? Aj : fmaxf(AB.x, Aj));
+                const float Bt = (ST == ST_GATHER) ? AB.y : ((ST == ST_SCATTER) ? Bj : fmaxf(AB.y, Bj));
+                const unsigned bi = __ballot_sync(PSB_FULL, d2 < At), bm = __ballot_sync(PSB_FULL, d2 <= Bt);
+                if (lane == s) { myacc = bi; mymaybe = bm; }
             }
+            const unsigned myunc = mymaybe & ~myacc;
             // undecided pairs: the reference's double test
             for (unsigned u = myunc; u; u &= u - 1) {
                 const int jj = __ffs(u) - 1;

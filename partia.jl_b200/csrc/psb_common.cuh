@@ -107,6 +107,9 @@ template <class T> struct TreeView {
     const float* mrho;       // m / rho (float)
     const float* mf;         // m (float)
     const float4* leafK;     // (1/h, sigma/h^3, sigma/h^4, m/rho) in float
+    // at the first leaf of every span: (max over the span of |leaf4.x| +
+    // |leaf4.y| + |leaf4.z|, max h), both rounded up (float error bounds)
+    const float2* spanb;
     float coord_err;         // bound on |float coordinate - exact| for node tests
 };
 

@@ -184,6 +184,10 @@ PSB_API int psb_destroy(psb_ctx* c) {
     if (c->lut_f) cudaFree(c->lut_f);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
+    for (auto& ev : c->pev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& cs : c->cstream)
+        if (cs) cudaStreamDestroy(cs);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return PSB_OK;

@@ -106,15 +106,15 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
 // list memory at SPLIT_BATCH * RCAP * 32 * 20 bytes (640 MiB).
 constexpr int64_t SPLIT_BATCH = 32768;
 
-static int run_split(psb_ctx* c, Args<double>& A, int prec, int st, int* launches) {
+static int run_split(psb_ctx* c, Args<double>& A, int prec, int st, int* launches, int slot_off = 0) {
     cudaStream_t s = c->stream;
     const int64_t nt = A.src.ntiles;
     const int64_t B = std::min<int64_t>(nt, SPLIT_BATCH);
-    float4* ent4 = (float4*)scratch(c, 16, sizeof(float4) * (size_t)RCAP * 32 * B);
-    uint32_t* emask = (uint32_t*)scratch(c, 20, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
-    uint8_t* cnt = (uint8_t*)scratch(c, 17, (size_t)32 * B);
-    void* hab = scratch(c, 18, sizeof(double) * 32 * (size_t)B);
-    char* ovf = (char*)scratch(c, 19, 256 + sizeof(int32_t) * (size_t)B);
+    float4* ent4 = (float4*)scratch(c, 16 + slot_off, sizeof(float4) * (size_t)RCAP * 32 * B);
+    uint32_t* emask = (uint32_t*)scratch(c, 20 + slot_off, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
+    uint8_t* cnt = (uint8_t*)scratch(c, 17 + slot_off, (size_t)32 * B);
+    void* hab = scratch(c, 18 + slot_off, sizeof(double) * 32 * (size_t)B);
+    char* ovf = (char*)scratch(c, 19 + slot_off, 256 + sizeof(int32_t) * (size_t)B);
     if (!ent4 || !emask || !cnt || !hab || !ovf) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
     unsigned* ovf_count = (unsigned*)ovf;
     int32_t* ovf_tiles = (int32_t*)(ovf + 256);
@@ -242,7 +242,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
                                                                     make_double3(sc[0], sc[1], sc[2]), codes, idx);
         PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
         ++launches;
-        PSB_CUDA_TRY(c, radix_sort_pairs(codes, idx, ns, c, 6, &launches), "sample sort");
+        PSB_CUDA_TRY(c, radix_sort_pairs(codes, idx, ns, c, 6, &launches, false), "sample sort");
         S.order = idx;
     }
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[2], s), "event");
@@ -332,6 +332,172 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     return PSB_OK;
 }
 
+// Point samples in host memory, in chunks of PIPE_CHUNK: chunk k+1 is copied
+// in on one copy stream and chunk k-1 copied out on another while chunk k
+// computes, so a large call costs about max(compute, copies) instead of their
+// sum.  Consecutive chunks compute on two streams with their own scratch, so
+// the tail of one chunk's kernels overlaps the start of the next.  Each chunk
+// is Morton-ordered on its own.  Buffers are double-buffered and guarded by
+// events.  (Copies from pageable memory still work, with less overlap.)
+constexpr int64_t PIPE_CHUNK = int64_t(1) << 19;
+
+template <class T>
+static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st,
+                                const psb_catalog* cat, int prec, void* const* out, uint32_t flags,
+                                psb_stats* stats) {
+    cudaStream_t s = c->stream;
+    const size_t es = sizeof(T);
+    const int64_t ns = rq.ns;
+    const int64_t CH = PIPE_CHUNK;
+    const int64_t nch = (ns + CH - 1) / CH;
+    int launches = 0;
+
+    Args<T> A;
+    memset((void*)&A, 0, sizeof(A));
+    std::vector<int> colu;
+    int rc = make_recipe(c, cat, false, A.rec, colu);
+    if (rc) return rc;
+    const int L = A.rec.L;
+    if (L > 0 && !out) return fail(c, PSB_EINVAL, "output pointer array must not be NULL");
+    for (int k = 0; k < L; ++k)
+        if (!out[k]) return fail(c, PSB_EINVAL, "output pointer " + std::to_string(k) + " is NULL");
+    const bool need_h = (st != ST_SCATTER) && hmode != PSB_H_NEAREST;
+    if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+    const bool ph = need_h && hmode == PSB_H_PER_SAMPLE;
+
+    for (int q = 0; q < 3; ++q)
+        if (!c->cstream[q]) PSB_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->cstream[q], cudaStreamNonBlocking), "stream");
+    for (int q = 0; q < 8; ++q)
+        if (!c->pev[q]) PSB_CUDA_TRY(c, cudaEventCreateWithFlags(&c->pev[q], cudaEventDisableTiming), "event");
+    cudaStream_t sin = c->cstream[0], sout = c->cstream[1];
+    const cudaStream_t cs[2] = {s, c->cstream[2]};
+    // the launch helpers use c->stream: point it at the chunk's compute stream, restore on exit
+    struct StreamRestore {
+        psb_ctx* c;
+        cudaStream_t s;
+        ~StreamRestore() { c->stream = s; }
+    } restore{c, s};
+    cudaEvent_t in_ready[2] = {c->pev[0], c->pev[1]}, in_free[2] = {c->pev[2], c->pev[3]};
+    cudaEvent_t done[2] = {c->pev[4], c->pev[5]}, out_free[2] = {c->pev[6], c->pev[7]};
+
+    A.tv = tree_view<T>(c);
+    A.hmode = hmode;
+    A.err = c->d_err;
+    A.lut_d = c->lut_d;
+    A.lut_f = c->lut_f;
+    for (size_t q = 0; q < colu.size(); ++q) {
+        A.colT[q] = (const T*)c->cols[colu[q]];
+        A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
+    }
+    const int nin = 3 + (ph ? 1 : 0);
+    char* inb = (char*)scratch(c, 0, es * CH * nin * 2);
+    char* outb = (char*)scratch(c, 2, es * CH * (L > 0 ? L : 1) * 2);
+    uint64_t* codes[2] = {(uint64_t*)scratch(c, 3, sizeof(uint64_t) * CH), (uint64_t*)scratch(c, 35, sizeof(uint64_t) * CH)};
+    uint32_t* idx[2] = {(uint32_t*)scratch(c, 4, sizeof(uint32_t) * CH), (uint32_t*)scratch(c, 36, sizeof(uint32_t) * CH)};
+    unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 8 * sizeof(unsigned long long));
+    T* hconst = (need_h && !ph) ? (T*)scratch(c, 1, es) : nullptr;
+    if (!inb || !outb || !codes[0] || !codes[1] || !idx[0] || !idx[1] || !dstats || (need_h && !ph && !hconst))
+        return fail(c, PSB_ENOMEM, "scratch allocation failed (chunked samples)");
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[0], s), "event");
+    PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), s), "memset stats");
+    if (hconst) PSB_CUDA_TRY(c, cudaMemcpyAsync(hconst, hs, es, cudaMemcpyHostToDevice, s), "hs H2D");
+    A.stats = dstats;
+    // the copy streams start after everything queued on the compute stream so far
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[1], s), "event");
+    PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, c->ev[1], 0), "stream wait");
+    PSB_CUDA_TRY(c, cudaStreamWaitEvent(sout, c->ev[1], 0), "stream wait");
+    PSB_CUDA_TRY(c, cudaStreamWaitEvent(cs[1], c->ev[1], 0), "stream wait");
+    double sc[3];
+    for (int d = 0; d < 3; ++d) {
+        double ext = c->bbox[3 + d] - c->bbox[d];
+        sc[d] = ext > 0 ? 2097151.0 / ext : 0.0;
+    }
+    const double3 lo3 = make_double3(c->bbox[0], c->bbox[1], c->bbox[2]);
+    const double3 sc3 = make_double3(sc[0], sc[1], sc[2]);
+
+    for (int64_t k = 0; k < nch; ++k) {
+        const int b = (int)(k & 1);
+        const int64_t off = k * CH, cn = std::min<int64_t>(CH, ns - off);
+        char* ib = inb + es * CH * nin * b;
+        // in
+        if (k >= 2) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, in_free[b], 0), "stream wait");
+        for (int q = 0; q < 3; ++q)
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(ib + es * CH * q, (const char*)rq.a[q] + es * off, es * cn,
+                                            cudaMemcpyHostToDevice, sin), "sample H2D");
+        if (ph)
+            PSB_CUDA_TRY(c, cudaMemcpyAsync(ib + es * CH * 3, (const char*)hs + es * off, es * cn,
+                                            cudaMemcpyHostToDevice, sin), "hs H2D");
+        PSB_CUDA_TRY(c, cudaEventRecord(in_ready[b], sin), "event");
+        // compute
+        const cudaStream_t sc_ = cs[b];
+        c->stream = sc_;
+        PSB_CUDA_TRY(c, cudaStreamWaitEvent(sc_, in_ready[b], 0), "stream wait");
+        if (k >= 2) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sc_, out_free[b], 0), "stream wait");
+        SampleSrc<T>& S = A.src;
+        S.kind = SRC_ARRAYS;
+        S.ns = cn;
+        for (int q = 0; q < 3; ++q) S.a[q] = (const T*)(ib + es * CH * q);
+        S.ntiles = (cn + 31) / 32;
+        S.order = nullptr;
+        A.hs = ph ? (const T*)(ib + es * CH * 3) : hconst;
+        for (int q = 0; q < L; ++q) A.out[q] = (T*)(outb + es * CH * ((size_t)L * b + q));
+        if (cn > 64) {
+            k_sample_codes<T><<<(unsigned)((cn + 255) / 256), 256, 0, sc_>>>(S.a[0], S.a[1], S.a[2], cn, lo3, sc3,
+                                                                          codes[b], idx[b]);
+            PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
+            ++launches;
+            PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, 6 + 32 * b, &launches, false), "sample sort");
+            S.order = idx[b];
+        }
+        bool split = false;
+        if constexpr (sizeof(T) == 8) split = !(flags & PSB_FLAG_SINGLE_KERNEL);
+        if (split) {
+            if constexpr (sizeof(T) == 8) {
+                rc = run_split(c, A, prec, st, &launches, 32 * b);
+                if (rc) return rc;
+            }
+        } else {
+            PSB_CUDA_TRY(c, launch_points<T>(A, prec, st, A.rec.kc, WHAT_INTERP, sc_), "interpolation kernel launch");
+            ++launches;
+        }
+        PSB_CUDA_TRY(c, cudaEventRecord(in_free[b], sc_), "event");
+        PSB_CUDA_TRY(c, cudaEventRecord(done[b], sc_), "event");
+        // out
+        PSB_CUDA_TRY(c, cudaStreamWaitEvent(sout, done[b], 0), "stream wait");
+        for (int q = 0; q < L; ++q)
+            PSB_CUDA_TRY(c, cudaMemcpyAsync((char*)out[q] + es * off, A.out[q], es * cn, cudaMemcpyDeviceToHost, sout),
+                         "output D2H");
+        PSB_CUDA_TRY(c, cudaEventRecord(out_free[b], sout), "event");
+    }
+    // join the copy streams and the second compute stream back into the compute stream
+    c->stream = s;
+    PSB_CUDA_TRY(c, cudaStreamWaitEvent(s, out_free[(nch - 1) & 1], 0), "stream wait");
+    PSB_CUDA_TRY(c, cudaEventRecord(c->ev[4], s), "event");
+    unsigned long long hst[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    unsigned herr = 0;
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(hst, dstats, sizeof(hst), cudaMemcpyDeviceToHost, s), "stats D2H");
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(&herr, c->d_err, sizeof(herr), cudaMemcpyDeviceToHost, s), "error D2H");
+    PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+    if (herr) {
+        cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
+        cudaStreamSynchronize(s);
+        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+    }
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->total_ms = ms_between(c->ev[0], c->ev[4]);
+        stats->interp_ms = stats->total_ms;
+        stats->pairs = (int64_t)hst[0];
+        stats->exact_retests = (int64_t)hst[1];
+        stats->warp_steps = (int64_t)hst[2];
+        stats->spans = (int64_t)hst[3];
+        stats->span_tests = (int64_t)hst[4];
+        stats->body_iters = (int64_t)hst[5];
+        stats->launches = launches;
+    }
+    return PSB_OK;
+}
+
 int run(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, const psb_catalog* cat, int prec,
         void* const* out, uint32_t flags, psb_stats* stats, int what, int64_t* dcount, uint64_t* dhash, void* ha_out) {
     if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before interpolation");
@@ -343,6 +509,11 @@ int run(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, cons
         return fail(c, PSB_EINVAL,
                     "LineSamples_interpolation only supports itpScatter. Line-integrated samples do not have a "
                     "well-defined query smoothing length ha, so itpGather and itpSymmetric are not supported.");
+    const bool pipelined = what == WHAT_INTERP && !(flags & PSB_FLAG_DEVICE_PTRS) && rq.kind == SRC_ARRAYS &&
+                           !rq.line && !c->adj_lam && rq.ns >= 2 * PIPE_CHUNK;
+    if (pipelined)
+        return c->dt == PSB_F64 ? run_points_pipelined<double>(c, rq, hmode, hs, st, cat, prec, out, flags, stats)
+                                : run_points_pipelined<float>(c, rq, hmode, hs, st, cat, prec, out, flags, stats);
     return c->dt == PSB_F64
                ? run_typed<double>(c, rq, hmode, hs, st, cat, prec, out, flags, stats, what, dcount, dhash, ha_out)
                : run_typed<float>(c, rq, hmode, hs, st, cat, prec, out, flags, stats, what, dcount, dhash, ha_out);

@@ -51,7 +51,7 @@ struct psb_ctx {
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };
-    Slot scratch[32];
+    Slot scratch[64];
 
     // adjoint: while adj_lam is set, an FP64 interpolation call writes the
     // cotangents of its per-sample sums (from the output cotangents adj_gout,
@@ -64,6 +64,10 @@ struct psb_ctx {
     struct psb_ctx* sctx = nullptr;  // LBVH over the samples of the last adjoint call
 
     cudaEvent_t ev[8] = {};
+    // copy streams (in, out) and a second compute stream of the chunked
+    // host-memory path (created on first use)
+    cudaStream_t cstream[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t pev[8] = {};
 };
 
 namespace psb {
@@ -86,7 +90,10 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, psb
 cudaError_t inclusive_max_scan_i64(int64_t* data, int64_t n, psb_ctx* c, int slot_base);
 // Stable LSD radix sort of (key, value) pairs on the low `bits` bits of key.
 // Results end in keys/vals (the alternates are scratch).
-cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches);
+// skip_constant_digits: read back which 8-bit digits vary (one host sync) and
+// sort only those; otherwise all eight passes run without a host round trip.
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches,
+                             bool skip_constant_digits = true);
 // The same sort on caller-provided scratch of at least
 // radix_sort_pairs_scratch_bytes(n) bytes (256-byte aligned); allocates nothing.
 size_t radix_sort_pairs_scratch_bytes(int64_t n);

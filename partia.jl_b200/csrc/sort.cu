@@ -240,19 +240,25 @@ __global__ void k_rs_scatter(const uint64_t* kin, const uint32_t* vin, uint64_t*
     }
 }
 
-cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches) {
+cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches,
+                             bool skip_constant_digits) {
     if (n <= 1) return cudaSuccess;
-    unsigned long long* d_or = (unsigned long long*)scratch(c, slot_base, sizeof(unsigned long long));
-    if (!d_or) return cudaErrorMemoryAllocation;
-    cudaError_t e = cudaMemsetAsync(d_or, 0, sizeof(unsigned long long), c->stream);
-    if (e != cudaSuccess) return e;
-    int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    k_key_xor_or<<<grid, 256, 0, c->stream>>>(keys, n, d_or);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    unsigned long long vary = 0;
-    if ((e = cudaMemcpyAsync(&vary, d_or, sizeof(vary), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess) return e;
-    if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
-    if (launches) *launches += 1;
+    cudaError_t e;
+    unsigned long long vary = ~0ull;  // every digit sorted: no host round trip
+    if (skip_constant_digits) {
+        // the digits on which all keys agree, read back once (one host sync)
+        unsigned long long* d_or = (unsigned long long*)scratch(c, slot_base, sizeof(unsigned long long));
+        if (!d_or) return cudaErrorMemoryAllocation;
+        e = cudaMemsetAsync(d_or, 0, sizeof(unsigned long long), c->stream);
+        if (e != cudaSuccess) return e;
+        int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+        k_key_xor_or<<<grid, 256, 0, c->stream>>>(keys, n, d_or);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        vary = 0;
+        if ((e = cudaMemcpyAsync(&vary, d_or, sizeof(vary), cudaMemcpyDeviceToHost, c->stream)) != cudaSuccess) return e;
+        if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return e;
+        if (launches) *launches += 1;
+    }
 
     const int nblocks = (int)((n + RS_TILE - 1) / RS_TILE);
     uint64_t* kalt = (uint64_t*)scratch(c, slot_base + 1, sizeof(uint64_t) * n);

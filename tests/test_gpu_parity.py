@@ -231,6 +231,31 @@ def test_two_kernel_path_overflow_tiles(prec):
     assert ctx.last_stats.pairs == int(co.sum())
 
 
+@pytest.mark.parametrize("prec,hmode", [(L.PSB_PREC_FP32C, L.PSB_H_NEAREST), (L.PSB_PREC_FP64, L.PSB_H_PER_SAMPLE)])
+def test_chunked_host_path_matches_device_path(prec, hmode):
+    """A host-memory call of more than two chunks is copied in and out in
+    chunks on copy streams that overlap the kernels; results equal the
+    device-pointer call on the same samples."""
+    import torch
+    arrs, cols = make_particles(20_000, 75)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build(want_perm=False)
+    ns = 1_200_000  # 3 chunks of 2^19
+    s = _samples(ns, 76)
+    hs = np.random.default_rng(77).uniform(0.02, 0.04, ns) if hmode == L.PSB_H_PER_SAMPLE else None
+    cat = CatalogC(**CATALOGS["all"])
+    host = ctx.interp_points(*s, cat, strategy=L.PSB_SYMMETRIC, hmode=hmode, hs=hs, prec=prec)
+    assert ctx.last_stats.launches > 9
+    pairs_host = ctx.last_stats.pairs
+    ts = tuple(torch.from_numpy(a).cuda() for a in s)
+    th = torch.from_numpy(hs).cuda() if hs is not None else None
+    dev = ctx.interp_points(*ts, cat, strategy=L.PSB_SYMMETRIC, hmode=hmode, hs=th, prec=prec)
+    assert ctx.last_stats.pairs == pairs_host
+    for k in range(cat.L):
+        assert np.array_equal(host[k], dev[k].cpu().numpy(), equal_nan=True), k
+
+
 def test_empty_neighbourhood_gives_nan_and_zero_density():
     arrs, cols = make_particles(2000, 61)
     orc, ctx, _, _ = pair(arrs, cols)

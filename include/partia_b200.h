@@ -93,7 +93,7 @@ typedef enum { PSB_H_NEAREST = 0, PSB_H_PER_SAMPLE = 1, PSB_H_CONSTANT = 2 } psb
  * PSB_PREC_FP32C path (float tests with double fallback) instead of the
  * double ones.  Both must give identical digests. */
 #define PSB_FLAG_FP32C_DECISIONS 0x100u
-/* Point interpolation of double inputs normally runs as two kernels (pair
+/* Point interpolation normally runs as two kernels (pair
  * lists, then pair sums).  This flag runs the single-kernel form instead, for
  * comparisons; results agree to rounding. */
 #define PSB_FLAG_SINGLE_KERNEL 0x200u

@@ -106,7 +106,8 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
 // list memory at SPLIT_BATCH * RCAP * 32 * 20 bytes (640 MiB).
 constexpr int64_t SPLIT_BATCH = 32768;
 
-static int run_split(psb_ctx* c, Args<double>& A, int prec, int st, int* launches, int slot_off = 0) {
+template <class T>
+static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, int slot_off = 0) {
     cudaStream_t s = c->stream;
     const int64_t nt = A.src.ntiles;
     const int64_t B = std::min<int64_t>(nt, SPLIT_BATCH);
@@ -126,11 +127,11 @@ static int run_split(psb_ctx* c, Args<double>& A, int prec, int st, int* launche
         A.sp.tile0 = t0; A.sp.ntiles = nb;
         PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, false, s), "pair-list kernel launch");
         PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, true, s), "pair-sum kernel launch");
-        Args<double> F = A;
+        Args<T> F = A;
         F.tile_list = ovf_tiles;
         F.tile_count = ovf_count;
         F.src.ntiles = nb;  // grid of the list pass: at most nb tiles
-        PSB_CUDA_TRY(c, launch_points<double>(F, prec, st, A.rec.kc, WHAT_INTERP, s), "overflow pass launch");
+        PSB_CUDA_TRY(c, launch_points<T>(F, prec, st, A.rec.kc, WHAT_INTERP, s), "overflow pass launch");
         *launches += 3;
     }
     return PSB_OK;
@@ -275,14 +276,10 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
 
     // ---- launch ----
     if (ns > 0) {
-        bool split = false;
-        if constexpr (sizeof(T) == 8)
-            split = what == WHAT_INTERP && !rq.line && !(flags & PSB_FLAG_SINGLE_KERNEL);
+        const bool split = what == WHAT_INTERP && !rq.line && !(flags & PSB_FLAG_SINGLE_KERNEL);
         if (split) {
-            if constexpr (sizeof(T) == 8) {
-                int rc = run_split(c, A, prec, st, &launches);
-                if (rc) return rc;
-            }
+            int rc = run_split(c, A, prec, st, &launches);
+            if (rc) return rc;
         } else {
             cudaError_t e = rq.line ? launch_lines<T>(A, prec, st, A.rec.kc, what, s)
                                     : launch_points<T>(A, prec, st, A.rec.kc, what, s);
@@ -449,13 +446,10 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
             PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, 6 + 32 * b, &launches, false), "sample sort");
             S.order = idx[b];
         }
-        bool split = false;
-        if constexpr (sizeof(T) == 8) split = !(flags & PSB_FLAG_SINGLE_KERNEL);
+        const bool split = !(flags & PSB_FLAG_SINGLE_KERNEL);
         if (split) {
-            if constexpr (sizeof(T) == 8) {
-                rc = run_split(c, A, prec, st, &launches, 32 * b);
-                if (rc) return rc;
-            }
+            rc = run_split(c, A, prec, st, &launches, 32 * b);
+            if (rc) return rc;
         } else {
             PSB_CUDA_TRY(c, launch_points<T>(A, prec, st, A.rec.kc, WHAT_INTERP, sc_), "interpolation kernel launch");
             ++launches;

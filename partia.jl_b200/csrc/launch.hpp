@@ -92,8 +92,13 @@ static cudaError_t dispatch_split_p(const Args<T>& a, int st, int kc, bool bodie
 template <class T> cudaError_t launch_points(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
 cudaError_t launch_split_d0(const Args<double>& a, int st, int kc, bool bodies, cudaStream_t s);
 cudaError_t launch_split_d1(const Args<double>& a, int st, int kc, bool bodies, cudaStream_t s);
+cudaError_t launch_split_f0(const Args<float>& a, int st, int kc, bool bodies, cudaStream_t s);
+cudaError_t launch_split_f1(const Args<float>& a, int st, int kc, bool bodies, cudaStream_t s);
 inline cudaError_t launch_split(const Args<double>& a, int prec, int st, int kc, bool bodies, cudaStream_t s) {
     return prec == PREC_FP64 ? launch_split_d0(a, st, kc, bodies, s) : launch_split_d1(a, st, kc, bodies, s);
+}
+inline cudaError_t launch_split(const Args<float>& a, int prec, int st, int kc, bool bodies, cudaStream_t s) {
+    return prec == PREC_FP64 ? launch_split_f0(a, st, kc, bodies, s) : launch_split_f1(a, st, kc, bodies, s);
 }
 template <class T> cudaError_t launch_lines(const Args<T>& a, int prec, int st, int kc, int what, cudaStream_t s);
 

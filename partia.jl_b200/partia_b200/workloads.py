@@ -80,6 +80,31 @@ def clumps(n, seed, nclump=64, frac_clump=0.9):
                 z=np.ascontiguousarray(p[:, 2]), m=np.full(n, 1.0 / n))
 
 
+def disc_halo_c5(n=64_000_000, seed=4, frac_disc=0.7, rd=0.2, zd=0.02, a_halo=0.3, dtype=np.float32):
+    """C5 positions (float32 by default): frac_disc of the particles in an
+    exponential disc (surface density ~ exp(-R/rd), so R ~ Gamma(2, rd);
+    sech^2(z/zd) vertical profile, z = zd atanh(2u - 1); uniform azimuth), the
+    rest in a Plummer halo (scale a_halo, truncated at 10 a_halo); equal masses
+    summing to 1.  Fields: the disc rotation velocity
+    v = (-y, x, 0) (x^2 + y^2 + 0.01)^(-3/4) and the scalar z^2.  h and rho
+    come from density_h."""
+    rng = np.random.default_rng(seed)
+    nd = int(round(frac_disc * n))
+    R = rng.gamma(2.0, rd, nd)
+    u = rng.random(nd)
+    u = np.clip(u, 1e-12, 1.0 - 1e-12)
+    zdisc = zd * np.arctanh(2.0 * u - 1.0)
+    phi = rng.uniform(0.0, 2.0 * math.pi, nd)
+    r = _plummer_radii(rng, n - nd, a_halo, 10 * a_halo)
+    ux, uy, uz = _isotropic(rng, n - nd)
+    x = np.concatenate([R * np.cos(phi), r * ux])
+    y = np.concatenate([R * np.sin(phi), r * uy])
+    z = np.concatenate([zdisc, r * uz])
+    fac = (x * x + y * y + 0.01) ** -0.75
+    out = dict(x=x, y=y, z=z, m=np.full(n, 1.0 / n), vx=-y * fac, vy=x * fac, vz=np.zeros(n), z2=z * z)
+    return {k: np.ascontiguousarray(v, dtype=dtype) for k, v in out.items()}
+
+
 def density_h(d, iters=3, eta=1.2, device=0):
     """Smoothing lengths and densities from the density sum (the clump
     configurations' recipe): h0 = eta (m / rho0)^(1/3) with rho0 the mean

@@ -1,0 +1,185 @@
+"""The benchmark configurations at their own sizes.
+
+Where the oracle would take minutes, parity is checked on a random subset of
+samples and, at full size, through properties that do not depend on the size:
+the FP32C path against the FP64 path field by field, and FP32C accept/reject
+decisions against FP64 ones (identical neighbour sets).
+
+ * C1: 100k uniform particles, rho from the density sum, gather with the mean
+   h and with the nearest particle's h, 64^3 cell-centre grid: all samples
+   against the oracle.
+ * C2: 2M-particle Plummer sphere, symmetric, 8 fields on the 128^3 grid:
+   FP32C within 1e-6 of FP64 on every field, identical neighbour sets on 200k
+   grid points, oracle on 20k of them.
+ * C3: 8M clump particles (h from the density sum), column density on the
+   1024^2 beam: FP32C against FP64, oracle on 2000 lines.
+ * C4: 1M clump particles, adjoint of the column density on a 128^2 beam
+   against the oracle's adjoint.
+ * C5-shaped: 4M float32 disc + halo particles, rho, grad rho, curl v,
+   Shepard z^2 on a grid and an oriented box: FP32C against FP64, oracle
+   subset at float accuracy.
+"""
+import numpy as np
+import pytest
+
+from conftest import has_gpu
+
+pytestmark = pytest.mark.gpu
+
+if not has_gpu():
+    pytest.skip("needs a CUDA GPU", allow_module_level=True)
+
+import oracle as O  # noqa: E402
+from partia_b200 import _lib as L  # noqa: E402
+from partia_b200 import linrange  # noqa: E402
+from partia_b200 import workloads as W  # noqa: E402
+from partia_b200.engine import CatalogC, Context  # noqa: E402
+
+
+def rel_err(a, b):
+    a, b = np.asarray(a, dtype=np.float64), np.asarray(b, dtype=np.float64)
+    na, nb = np.isnan(a), np.isnan(b)
+    assert np.array_equal(na, nb), "NaN masks differ"
+    fin = ~na
+    if not fin.any():
+        return 0.0
+    scale = np.max(np.abs(b[fin]))
+    return float(np.max(np.abs(a[fin] - b[fin])) / scale) if scale > 0 else float(np.max(np.abs(a[fin])))
+
+
+def grid_points(ax, ay, az):
+    X, Y, Z = np.meshgrid(ax, ay, az, indexing="ij")
+    return X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")
+
+
+def make_ctx(d, h, rho, cols, dtype=np.float64):
+    ctx = Context(0)
+    ctx.set_particles(d["x"], d["y"], d["z"], d["m"], h, rho, cols, dtype=dtype)
+    ctx.build(want_perm=False)
+    return ctx
+
+
+def test_c1_uniform_gather_full_size():
+    d = W.uniform_c1()
+    x, y, z, m, h = d["x"], d["y"], d["z"], d["m"], d["h"]
+    # rho_b from the method's own density sum at the particles (gather, ha = h_b)
+    rho = O.Oracle(x, y, z, m, h, np.ones_like(m)).density(x, y, z, strategy=O.GATHER, hmode=O.H_PER_SAMPLE, hs=h)
+    cols = [rho, d["A"]]
+    orc = O.Oracle(x, y, z, m, h, rho, cols)
+    ctx = make_ctx(d, h, rho, cols)
+    ax = linrange(*W.cell_centre_axis(64))
+    s = grid_points(ax, ax, ax)
+    spec = dict(scalars=[0, 1], shepard=[0, 1])
+    for hmode, hs in ((O.H_CONSTANT, np.array([np.mean(h)])), (O.H_NEAREST, None)):
+        ref = orc.interp_points(*s, O.Catalog(**spec), strategy=O.GATHER, hmode=hmode, hs=hs)
+        for prec, tol in ((L.PSB_PREC_FP64, 1e-12), (L.PSB_PREC_FP32C, 1e-6)):
+            g = ctx.interp_grid(ax, ax, ax, CatalogC(**spec), strategy=L.PSB_GATHER, hmode=hmode, hs=hs, prec=prec)
+            for k in range(2):
+                assert rel_err(g[k], ref[k]) <= tol, (hmode, prec, k, rel_err(g[k], ref[k]))
+        co, ho, _ = orc.digest(s, strategy=O.GATHER, hmode=hmode, hs=hs)
+        for fp32c in (False, True):
+            cg, hg, _ = ctx.digest(s, strategy=L.PSB_GATHER, hmode=hmode, hs=hs, fp32c=fp32c)
+            assert np.array_equal(cg, co) and np.array_equal(hg, ho)
+
+
+def test_c2_plummer_full_size():
+    d = W.plummer_c2()
+    cols = [d["rho"], d["Ax"], d["Ay"], d["Az"]]
+    ctx = make_ctx(d, d["h"], d["rho"], cols)
+    spec = dict(scalars=[0], shepard=[0], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])
+    ax = linrange(-0.5, 0.5, 128)
+    g64 = ctx.interp_grid(ax, ax, ax, CatalogC(**spec), strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP64)
+    g32 = ctx.interp_grid(ax, ax, ax, CatalogC(**spec), strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
+    for k in range(8):  # the precision target: every field within 1e-6 of FP64
+        assert rel_err(g32[k], g64[k]) <= 1e-6, (k, rel_err(g32[k], g64[k]))
+    rng = np.random.default_rng(21)
+    s_all = grid_points(ax, ax, ax)
+    idx = rng.choice(len(s_all[0]), 200_000, replace=False)
+    s = tuple(a[idx] for a in s_all)
+    c64, h64, a64 = ctx.digest(s, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST)
+    c32, h32, a32 = ctx.digest(s, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, fp32c=True)
+    assert np.array_equal(c64, c32) and np.array_equal(h64, h32) and np.array_equal(a64, a32)
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], d["h"], d["rho"], cols)
+    sub = idx[:20_000]
+    ss = tuple(a[sub] for a in s_all)
+    ref = orc.interp_points(*ss, O.Catalog(**spec), strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    for k in range(8):
+        assert rel_err(g64[k][sub], ref[k]) <= 1e-12, k
+    co, ho, _ = orc.digest(ss, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    assert np.array_equal(co, c64[:20_000]) and np.array_equal(ho, h64[:20_000])
+
+
+def test_c3_lines_full_size():
+    d = W.clumps(8_000_000, 2)
+    h, rho = W.density_h(d)
+    ctx = make_ctx(d, h, rho, [rho])
+    fr = W.c3_frame().as_array()
+    prm = np.array([0.0, 1.0, 0.0, 1.0])
+    npix = 1024
+    cat = CatalogC(scalars=[0], shepard=[0])
+    g32 = ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP32C)
+    g64 = ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP64)
+    assert rel_err(g32[0], g64[0]) <= 1e-6
+    rng = np.random.default_rng(31)
+    k = rng.choice(npix * npix, 2000, replace=False)
+    ox = tuple(a[k] for a in W.plane_coordinates(fr, (0.0, 1.0, npix), (0.0, 1.0, npix)))
+    fw = tuple(np.full(len(k), fr[9 + c]) for c in range(3))
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], h, rho, [rho])
+    ref = orc.interp_lines(ox, fw, [0], shepard=[0], strategy=O.SCATTER)
+    assert rel_err(g64[0][k], ref[0]) <= 1e-12
+    co, ho, _ = orc.digest(ox, fw, strategy=O.SCATTER, hmode=O.H_PER_SAMPLE, hs=np.zeros(len(k)))
+    cg, hg, _ = ctx.digest(ox, fw, strategy=L.PSB_SCATTER, hmode=L.PSB_H_PER_SAMPLE, hs=np.zeros(len(k)))
+    assert np.array_equal(cg, co) and np.array_equal(hg, ho)
+
+
+def test_c4_adjoint_1m_particles():
+    d = W.clumps(1_000_000, 3)
+    h, rho = W.density_h(d)
+    ctx = make_ctx(d, h, rho, [rho])
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], h, rho, [rho])
+    fr = W.c3_frame().as_array()
+    prm = np.array([0.0, 1.0, 0.0, 1.0])
+    npix = 128
+    rng = np.random.default_rng(41)
+    gout = [rng.standard_normal(npix * npix)]
+    g = ctx.adjoint_beam(fr, prm, npix, npix, CatalogC(scalars=[0], shepard=[0]), gout, strategy=L.PSB_SCATTER)
+    ox = W.plane_coordinates(fr, (0.0, 1.0, npix), (0.0, 1.0, npix))
+    fw = tuple(np.full(npix * npix, fr[9 + c]) for c in range(3))
+    threads = O.set_threads(0)
+    O.set_threads(min(threads, 4))  # per-thread gradient buffers of 1M particles
+    try:
+        r = orc.adjoint_lines(ox, fw, [0], gout, shepard=[0], strategy=O.SCATTER)
+    finally:
+        O.set_threads(threads)
+    for key in ("m", "x", "y", "z"):
+        assert rel_err(g[key], r[key]) <= 1e-10, key
+    assert rel_err(g["cols"][0], r["cols"][0]) <= 1e-10
+
+
+def test_c5_shaped_float_inputs():
+    d = W.disc_halo_c5(4_000_000, 4)
+    h, rho = W.density_h(d)
+    cols = [rho, d["vx"], d["vy"], d["vz"], d["z2"]]
+    ctx = make_ctx(d, h, rho, cols, dtype=np.float32)
+    spec = dict(scalars=[0, 4], shepard=[0, 1], grads=[0], curls=[1, 2, 3])
+    cat = CatalogC(**spec)
+    ax = linrange(-1.0, 1.0, 64).astype(np.float32)
+    g64 = ctx.interp_grid(ax, ax, ax, cat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP64)
+    g32 = ctx.interp_grid(ax, ax, ax, cat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
+    for k in range(len(g64)):
+        assert rel_err(g32[k], g64[k]) <= 1e-5, (k, rel_err(g32[k], g64[k]))
+    fr = W.Frame((0.1, -0.2, 0.0), (0.3, 0.2, 1.0), (1.0, 0.0, -0.3))
+    fr.rotate(0.4, -0.3, 0.2)
+    farr = fr.as_array().astype(np.float32)
+    bprm = np.array([-0.5, 0.5, -0.5, 0.5, -0.5, 0.5], dtype=np.float32)
+    gb = ctx.interp_box(farr, bprm, 32, 32, 32, cat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
+    assert np.isfinite(gb[0]).mean() > 0.5
+    # oracle (float arithmetic, as the reference with Float32 inputs) on grid samples
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], h, rho, cols, dtype=np.float32)
+    rng = np.random.default_rng(51)
+    s_all = grid_points(ax, ax, ax)
+    idx = rng.choice(len(s_all[0]), 5000, replace=False)
+    ss = tuple(a[idx] for a in s_all)
+    ref = orc.interp_points(*ss, O.Catalog(**spec), strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    for k in range(len(ref)):
+        assert rel_err(g64[k][idx], ref[k]) <= 2e-4, (k, rel_err(g64[k][idx], ref[k]))

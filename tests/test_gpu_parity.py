@@ -188,16 +188,17 @@ def test_point_fields_float32_inputs():
             assert rel_err(g[k], ref[k]) <= 2e-4, (prec, k)
 
 
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
 @pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
 @pytest.mark.parametrize("strategy", [L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC])
-def test_two_kernel_path_matches_single_kernel(prec, strategy):
+def test_two_kernel_path_matches_single_kernel(prec, strategy, dtype):
     """The pair-list + pair-sum kernels visit the same pairs in the same order
-    with the same arithmetic as the single kernel."""
-    arrs, cols = make_particles(30_000, 71)
+    with the same arithmetic as the single kernel (double and float inputs)."""
+    arrs, cols = make_particles(30_000, 71, dtype)
     ctx = Context(0)
-    ctx.set_particles(*arrs, cols=cols)
+    ctx.set_particles(*arrs, cols=cols, dtype=dtype)
     ctx.build(want_perm=False)
-    s = _samples(6000, 72)
+    s = tuple(a.astype(dtype) for a in _samples(6000, 72))
     cat = CatalogC(**CATALOGS["all"])
     two = ctx.interp_points(*s, cat, strategy=strategy, hmode=L.PSB_H_NEAREST, prec=prec)
     st2 = ctx.last_stats.as_dict()

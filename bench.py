@@ -238,6 +238,84 @@ def lines_and_adjoint(steps, warmup):
     return res
 
 
+def large_leg(steps, warmup):
+    """The large mixed configuration: 64M float32 particles (70% exponential
+    disc, 30% Plummer halo; h and rho from the density sum), rho, Shepard z^2,
+    grad rho and curl v on a 256^3 grid over [-1,1]^3 plus four randomly
+    oriented 128^3 boxes over [-0.5,0.5]^3 (25.2M samples), symmetric,
+    nearest-particle h.  FP32C against the all-FP64 path on the same particle
+    values (the float32 data converted to double on the device), and the
+    float32-storage path (the reference's Float32 semantics) beside them."""
+    import math
+    import torch
+    from partia_b200 import _lib as L, workloads as W, linrange
+    from partia_b200.engine import CatalogC, Context
+    stream = torch.cuda.Stream()
+    d = W.disc_halo_c5()
+    h, rho = W.density_h(d)
+    cols = [rho, d["vx"], d["vy"], d["vz"], d["z2"]]
+    cat = CatalogC(scalars=[0, 4], shepard=[0, 1], grads=[0], curls=[1, 2, 3])
+    rng = np.random.default_rng(4)
+    frames = []
+    for _ in range(4):
+        fr = W.Frame((0.0, 0.0, 0.0), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0))
+        fr.rotate(*rng.uniform(-math.pi, math.pi, 3))
+        frames.append(fr.as_array())
+    bprm = np.array([-0.5, 0.5, -0.5, 0.5, -0.5, 0.5])
+    ng, nb = 256, 128
+    ax = linrange(-1.0, 1.0, ng)
+    res = {}
+    outs = {}
+    ns = ng ** 3 + len(frames) * nb ** 3
+    runs = {torch.float32: [("float32_storage", L.PSB_PREC_FP32C)],
+            torch.float64: [("fp32c", L.PSB_PREC_FP32C), ("fp64", L.PSB_PREC_FP64)]}
+    for dt, legs in runs.items():
+        ctx = Context(0)
+        L.load().psb_set_stream(ctx.h, stream.cuda_stream)
+        dev = [torch.from_numpy(a).cuda().to(dt) for a in (d["x"], d["y"], d["z"], d["m"], h, rho)]
+        dcols = [torch.from_numpy(c).cuda().to(dt) for c in cols]
+        ctx.set_particles(*dev, cols=dcols)
+        ctx.build(want_perm=False)
+        del dev, dcols
+        go = [torch.empty(ng ** 3, dtype=dt, device="cuda") for _ in range(8)]
+        bo = [[torch.empty(nb ** 3, dtype=dt, device="cuda") for _ in range(8)] for _ in frames]
+        for label, prec in legs:
+            pairs = [0]
+
+            def step():
+                ctx.interp_grid(ax, ax, ax, cat, strategy=L.PSB_SYMMETRIC, prec=prec, out=go)
+                p = ctx.last_stats.pairs
+                for fa, o in zip(frames, bo):
+                    ctx.interp_box(fa, bprm, nb, nb, nb, cat, strategy=L.PSB_SYMMETRIC, prec=prec, out=o)
+                    p += ctx.last_stats.pairs
+                pairs[0] = p
+
+            t = timed_call(step, stream, steps, warmup)
+            res[label] = {"ms": t, "samples_per_s": ns / (t / 1e3), "pairs": int(pairs[0])}
+            outs[label] = [torch.cat([go[k].double()] + [o[k].double() for o in bo]) for k in range(8)]
+        ctx.close()
+        del go, bo
+        torch.cuda.empty_cache()
+    names = ["rho", "z2", "grad_rho_x", "grad_rho_y", "grad_rho_z", "curl_v_x", "curl_v_y", "curl_v_z"]
+
+    def errs(a_, b_):
+        e = {}
+        for k in range(8):
+            a, b = a_[k], b_[k]
+            fin = torch.isfinite(b) & torch.isfinite(a)
+            e[names[k]] = ((a[fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
+        return e
+    res["float32_storage"]["note"] = ("particle data kept in float32; inclusion tests and nearest-particle h in float "
+                                      "arithmetic, as the reference computes with Float32 inputs")
+    res["fp32c"]["particles"] = res["fp64"]["particles"] = "the float32 values converted to double on the device"
+    return {"workload": "disc+halo 64M, 256^3 grid + 4 oriented 128^3 boxes, symmetric, nearest h",
+            "N": 64_000_000, "samples": ns, "fp32c": res["fp32c"], "fp64": res["fp64"],
+            "float32_storage": res["float32_storage"],
+            "speedup_fp32c_vs_fp64": res["fp64"]["ms"] / res["fp32c"]["ms"],
+            "fp32c_rel_err_vs_fp64": errs(outs["fp32c"], outs["fp64"]),
+            "float32_storage_rel_err_vs_fp64": errs(outs["float32_storage"], outs["fp64"])}
+
+
 def cpu_reference(args, d, axis, steps, warmup, threads=None):
     """Oracle port on the host cores over a bounded random sample of grid points."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -303,6 +381,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-lines", action="store_true", help="skip the line-integrated and adjoint legs")
+    ap.add_argument("--no-large", action="store_true", help="skip the 64M-particle leg")
     args = ap.parse_args()
     NGRID = args.grid
     if args.impl == "reference":
@@ -444,6 +523,9 @@ def main():
     extra = None
     if world == 1 and not args.no_lines:
         extra = lines_and_adjoint(max(3, args.steps // 4), 2)
+    large = None
+    if world == 1 and not args.no_large:
+        large = large_leg(3, 1)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -473,6 +555,7 @@ def main():
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs,
             "grad_fwd_time_ratio": extra["adjoint"]["grad_fwd_time_ratio"] if extra else None,
             "lines": extra["lines"] if extra else None, "adjoint": extra["adjoint"] if extra else None,
+            "large": large,
             "build_ms": build_ms,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

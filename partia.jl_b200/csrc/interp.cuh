@@ -119,6 +119,23 @@ template <class C> __device__ __forceinline__ void m4_fdf(C q, C& f, C& df) {
     f = (q < C(1)) ? fi : ((q < C(2)) ? fo : C(0));
     df = (q < C(1)) ? dfi : ((q < C(2)) ? dfo : C(0));
 }
+// M4 f and f' for the float pair sums.  The inner piece (q < 1) comes from
+// q in float.  The outer piece, f = a^3 / 4 and f' = -3 a^2 / 4 with
+// a = 2 - q, takes a = (4 h^2 - d2) / (h (2 h + r)), with 4 h^2 - d2 formed
+// in double from the exact squared separation (num): from the float q alone,
+// a would carry an absolute error of a few float ulps, a relative error of
+// about 1e-6 at q = 1 that grows without bound towards the support edge,
+// where a sample with few neighbours still gets most of its weight.
+__device__ __forceinline__ void m4_fdf_edge(float q, float r, float num, float hf, float& f, float& df) {
+    if (q < 1.f) {
+        m4_fdf<float>(q, f, df);
+        return;
+    }
+    const float a = fmaxf(num * __frcp_rn(hf * (2.f * hf + r)), 0.f);
+    f = 0.25f * a * a * a;
+    df = -0.75f * a * a;
+}
+
 template <class C> __device__ __forceinline__ C m4_f(C q) {
     C a = C(2) - q, b = C(1) - q;
     C fo = C(0.25) * a * a * a;

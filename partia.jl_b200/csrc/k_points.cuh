@@ -380,6 +380,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         sa3 = sig * ia * ia * ia;
         sa4 = sa3 * ia;
     }
+    const double fa2 = 4.0 * (double)ha * (double)ha;  // (2 ha)^2 for the outer kernel piece
 
     // ---- accumulators ----
     Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
@@ -509,15 +510,25 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
             const float r = d2 * invr;
             float Wsum = 0.f, csum = 0.f;
+            const int64_t li = st.lo[b] + j;
+            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
+            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
+            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
+            if (qa >= 1.f || qb >= 1.f) {
+                const double ex = (double)p[0] - (double)tv.x[li], ey = (double)p[1] - (double)tv.y[li],
+                             ez = (double)p[2] - (double)tv.z[li];
+                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
+            }
             if (ST != ST_SCATTER) {
                 float f, df;
-                m4_fdf<float>(r * (float)ia, f, df);
+                m4_fdf_edge(qa, r, (float)(fa2 - d2d), (float)ha, f, df);
                 Wsum = (float)sa3 * f;
                 csum = (float)sa4 * df;
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                m4_fdf<float>(r * K.x, f, df);
+                const double hb2 = qb >= 1.f ? 2.0 * (double)tv.h[li] : 0.0;
+                m4_fdf_edge(qb, r, (float)fma(hb2, hb2, -d2d), Lj.w, f, df);
                 if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
                 else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
             }

@@ -291,6 +291,8 @@ template <class T, int KC> struct PairData<T, true, KC> {
     float col[KC];
     float mb;         // mass (density gradient only)
     float r[3];       // the sample relative to the span's first leaf
+    int64_t li;       // leaf index
+    double xd, yd, zd, hd;  // the particle in double (outer kernel piece)
     __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool need_dg,
                                          const float* Rs) {
         L = __ldg(&tv.leaf4[li]);
@@ -299,11 +301,13 @@ template <class T, int KC> struct PairData<T, true, KC> {
         for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&A.colF[c][li]) : 0.f;
         mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
         r[0] = Rs[0]; r[1] = Rs[1]; r[2] = Rs[2];
+        this->li = li;
+        xd = __ldg(&tv.x[li]); yd = __ldg(&tv.y[li]); zd = __ldg(&tv.z[li]); hd = __ldg(&tv.h[li]);
     }
 };
 
 template <class T, int PREC, int ST, int KC>
-__global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
+__global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
     constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
@@ -331,6 +335,7 @@ __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
         sa3 = sig * ia * ia * ia;
         sa4 = sa3 * ia;
     }
+    const double fa2 = 4.0 * (double)ha * (double)ha;  // (2 ha)^2 for the outer kernel piece
     Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
     CT a0[KC];
     bool have0 = false;
@@ -415,15 +420,23 @@ __global__ void __launch_bounds__(128) k_bodies(const Args<T> A) {
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
             const float r = d2 * invr;
             float Wsum = 0.f, csum = 0.f;
+            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
+            const float qb = (ST != ST_GATHER) ? r * cur.K.x : 0.f;
+            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
+            if (qa >= 1.f || qb >= 1.f) {
+                const double ex = (double)p[0] - cur.xd, ey = (double)p[1] - cur.yd, ez = (double)p[2] - cur.zd;
+                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
+            }
             if (ST != ST_SCATTER) {
                 float f, df;
-                m4_fdf<float>(r * (float)ia, f, df);
+                m4_fdf_edge(qa, r, (float)(fa2 - d2d), (float)ha, f, df);
                 Wsum = (float)sa3 * f;
                 csum = (float)sa4 * df;
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                m4_fdf<float>(r * cur.K.x, f, df);
+                const double hb2 = cur.hd + cur.hd;
+                m4_fdf_edge(qb, r, (float)fma(hb2, hb2, -d2d), cur.L.w, f, df);
                 if (ST == ST_SCATTER) { Wsum = cur.K.y * f; csum = cur.K.z * df; }
                 else { Wsum = 0.5f * (Wsum + cur.K.y * f); csum = 0.5f * (csum + cur.K.z * df); }
             }

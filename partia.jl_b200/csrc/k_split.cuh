@@ -171,42 +171,42 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
             float rmax = rahimax;
             if (ST != ST_GATHER) rmax = fmaxf(rmax, 2.f * sb.y * (1.f + 2.f * U1));
             const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
-            // this lane's leaf (far away for lanes past the span: never in, never undecided)
-            float4 Q = make_float4(1e18f, 1e18f, 1e18f, 0.f);
-            float Aj = 0.f, Bj = 0.f;
+            // the span's leaves (and their radius thresholds) in shared memory
+            __syncwarp();
             if (lane < cnt) {
                 const float4 L = __ldg(&tv.leaf4[lo + lane]);
-                Q = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
+                st.Q[lane] = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
                 if (ST != ST_GATHER) {
                     const float rbhi = 2.f * L.w * (1.f + 2.f * U1), rblo = 2.f * L.w * (1.f - 2.f * U1);
                     const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
-                    Aj = il * il;
-                    Bj = ih2 * ih2;
+                    st.AB[lane] = make_float2(il * il, ih2 * ih2);
                 }
             }
             __syncwarp();
-            {
+            // surely in: d2 < A; maybe in: d2 <= B (undecided = maybe and not surely);
+            // each lane tests its own sample against every leaf of the span
+            unsigned myacc = 0, mymaybe = 0;
+            if (part) {
                 float As = 0.f, Bs = 0.f;
                 if (ST != ST_SCATTER) {
                     const float il = fmaxf((Rme.x - E) * (1.f - 4.f * U1), 0.f), ih2 = (Rme.y + E) * (1.f + 4.f * U1);
                     As = il * il;
                     Bs = ih2 * ih2;
                 }
-                st.AB[lane] = make_float2(As, Bs);
-            }
-            __syncwarp();
-            // surely in: d2 < A; maybe in: d2 <= B (undecided = maybe and not surely)
-            unsigned myacc = 0, mymaybe = 0;
-            for (unsigned pp = parts; pp; pp &= pp - 1) {
-                const int s = __ffs(pp) - 1;
-                const float4 P = st.P[s];
-                const float2 AB = st.AB[s];
-                const float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
-                const float d2 = dx * dx + dy * dy + dz * dz;
-                const float At = (ST == ST_GATHER) ? AB.x : ((ST == ST_SCATTER) ? Aj : fmaxf(AB.x, Aj));
-                const float Bt = (ST == ST_GATHER) ? AB.y : ((ST == ST_SCATTER) ? Bj : fmaxf(AB.y, Bj));
-                const unsigned bi = __ballot_sync(PSB_FULL, d2 < At), bm = __ballot_sync(PSB_FULL, d2 <= Bt);
-                if (lane == s) { myacc = bi; mymaybe = bm; }
+#pragma unroll 4
+                for (int j = 0; j < cnt; ++j) {
+                    const float4 Q = st.Q[j];
+                    const float dx = Pme.x - Q.x, dy = Pme.y - Q.y, dz = Pme.z - Q.z;
+                    const float d2 = dx * dx + dy * dy + dz * dz;
+                    float At = As, Bt = Bs;
+                    if (ST != ST_GATHER) {
+                        const float2 ab = st.AB[j];
+                        At = (ST == ST_SCATTER) ? ab.x : fmaxf(As, ab.x);
+                        Bt = (ST == ST_SCATTER) ? ab.y : fmaxf(Bs, ab.y);
+                    }
+                    myacc |= (unsigned)(d2 < At) << j;
+                    mymaybe |= (unsigned)(d2 <= Bt) << j;
+                }
             }
             const unsigned myunc = mymaybe & ~myacc;
             // undecided pairs: the reference's double test

@@ -131,7 +131,7 @@ __device__ __forceinline__ void m4_fdf_edge(float q, float r, float num, float h
         m4_fdf<float>(q, f, df);
         return;
     }
-    const float a = fmaxf(num * __frcp_rn(hf * (2.f * hf + r)), 0.f);
+    const float a = fmaxf(__fdividef(num, hf * (2.f * hf + r)), 0.f);
     f = 0.25f * a * a * a;
     df = -0.75f * a * a;
 }

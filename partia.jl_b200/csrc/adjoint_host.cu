@@ -22,11 +22,16 @@ namespace psb {
 
 int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu);
 
+template <int KC, bool SCAL>
+static void launch_adj_points_ks(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
+    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL><<<g, 128, 0, s>>>(a);
+    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL><<<g, 128, 0, s>>>(a);
+    else k_adj_points<ST_SYMMETRIC, KC, SCAL><<<g, 128, 0, s>>>(a);
+}
 template <int KC>
-static void launch_adj_points_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
-    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC><<<g, 128, 0, s>>>(a);
-    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC><<<g, 128, 0, s>>>(a);
-    else k_adj_points<ST_SYMMETRIC, KC><<<g, 128, 0, s>>>(a);
+static void launch_adj_points_k(const AdjArgs& a, int st, bool scal, unsigned g, cudaStream_t s) {
+    if (scal) launch_adj_points_ks<KC, true>(a, st, g, s);
+    else launch_adj_points_ks<KC, false>(a, st, g, s);
 }
 template <int KC>
 static void launch_adj_beam_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
@@ -186,9 +191,11 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
 
         // ---- sum cotangents: directly from gout when the catalog allows and
         // h_a needs no nearest search, else a forward pass in FP64 ----
-        bool direct = true;
-        for (int o = 0; o < L; ++o)
+        bool direct = true, scal = true;
+        for (int o = 0; o < L; ++o) {
             if (rec.op[o] != OP_SCALAR || rec.a1[o]) direct = false;
+            if (rec.op[o] != OP_SCALAR) scal = false;
+        }
         if (!line && st != ST_SCATTER && hmode == PSB_H_NEAREST) direct = false;
         if (direct) {
             const unsigned gb = (unsigned)((ns + 255) / 256);
@@ -204,8 +211,9 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             c->adj_ha = ha;
             psb_stats fst;
             memset(&fst, 0, sizeof(fst));
-            rc = run(c, rq, hmode, need_h ? (const void*)hsd : nullptr, st, cat, PREC_FP64, nullptr,
-                     PSB_FLAG_DEVICE_PTRS, &fst, WHAT_INTERP, nullptr, nullptr, nullptr);
+            // (a grid runs as a grid: its sample index is that of the coordinate arrays)
+            rc = run(c, rq0.kind == SRC_GRID ? rq0 : rq, hmode, need_h ? (const void*)hsd : nullptr, st, cat,
+                     PREC_FP64, nullptr, PSB_FLAG_DEVICE_PTRS, &fst, WHAT_INTERP, nullptr, nullptr, nullptr);
             if (rc) return rc;
             launches += fst.launches;
         }
@@ -246,10 +254,10 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             J.sv = tree_view<double>(c->sctx);
             J.lam = lams;
             const unsigned g = (unsigned)((n + 127) / 128);
-            if (kcl == 1) launch_adj_points_k<1>(J, st, g, s);
-            else if (kcl == 2) launch_adj_points_k<2>(J, st, g, s);
-            else if (kcl == 4) launch_adj_points_k<4>(J, st, g, s);
-            else launch_adj_points_k<8>(J, st, g, s);
+            if (kcl == 1) launch_adj_points_k<1>(J, st, scal, g, s);
+            else if (kcl == 2) launch_adj_points_k<2>(J, st, scal, g, s);
+            else if (kcl == 4) launch_adj_points_k<4>(J, st, scal, g, s);
+            else launch_adj_points_k<8>(J, st, scal, g, s);
             PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
             launches += 2;
         } else {
@@ -292,6 +300,9 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             stats->interp_ms = ms;
             stats->pairs = (int64_t)hst[0];
             stats->warp_steps = (int64_t)hst[2];
+            stats->spans = (int64_t)hst[3];       // spans visited (point samples)
+            stats->span_tests = (int64_t)hst[4];  // particle-span tests
+            stats->body_iters = (int64_t)hst[5];  // samples in the visited spans
         }
     }
     // ---- gradients to the caller ----

@@ -349,7 +349,7 @@ static int build_typed(psb_ctx* c) {
     cudaStream_t s = c->stream;
     const size_t es = sizeof(T);
     int launches = 0;
-    free_tree(c);
+    reset_tree(c);
 
     // 1. bounding box
     const int nparts = (int)std::min<int64_t>(grid_for(n), 148 * 4);
@@ -361,10 +361,9 @@ static int build_typed(psb_ctx* c) {
     PSB_CUDA_TRY(c, cudaGetLastError(), "bbox kernels");
 
     // 2. codes
-    uint64_t* codes = nullptr;
     uint32_t* idx = (uint32_t*)scratch(c, 2, sizeof(uint32_t) * n);
-    PSB_CUDA_TRY(c, cudaMalloc(&codes, sizeof(uint64_t) * n), "cudaMalloc codes");
-    c->codes = codes;
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->codes, sizeof(uint64_t) * n), "cudaMalloc codes");
+    uint64_t* codes = c->codes;
     if (!idx) return fail(c, PSB_ENOMEM, "scratch allocation failed (index)");
     k_encode<T><<<grid_for(n), BT, 0, s>>>((const T*)c->x, (const T*)c->y, (const T*)c->z, n, bb, bb + 6, codes, idx, c->d_err);
     PSB_CUDA_TRY(c, cudaGetLastError(), "encode kernel");
@@ -381,7 +380,7 @@ static int build_typed(psb_ctx* c) {
     PSB_CUDA_TRY(c, cudaGetLastError(), "dedup kernels");
 
     // 5. permute particle arrays into Morton order
-    PSB_CUDA_TRY(c, cudaMalloc(&c->order, sizeof(int64_t) * n), "cudaMalloc order");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->order, sizeof(int64_t) * n), "cudaMalloc order");
     k_order64<<<grid_for(n), BT, 0, s>>>(idx, n, c->order);
     T* tmp = (T*)scratch(c, 3, es * n);  // dedup values are consumed
     if (!tmp) return fail(c, PSB_ENOMEM, "scratch allocation failed (permute)");
@@ -395,22 +394,22 @@ static int build_typed(psb_ctx* c) {
 
     // 6-7. tree topology
     const int64_t tot = 2 * n - 1, nint = n - 1;
-    PSB_CUDA_TRY(c, cudaMalloc(&c->left, sizeof(int32_t) * tot), "cudaMalloc left");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->right, sizeof(int32_t) * tot), "cudaMalloc right");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->escape, sizeof(int32_t) * tot), "cudaMalloc escape");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->parent, sizeof(int32_t) * tot), "cudaMalloc parent");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->left, sizeof(int32_t) * tot), "cudaMalloc left");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->right, sizeof(int32_t) * tot), "cudaMalloc right");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->escape, sizeof(int32_t) * tot), "cudaMalloc escape");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->parent, sizeof(int32_t) * tot), "cudaMalloc parent");
     PSB_CUDA_TRY(c, cudaMemsetAsync(c->left, 0, sizeof(int32_t) * tot, s), "memset");
     PSB_CUDA_TRY(c, cudaMemsetAsync(c->right, 0, sizeof(int32_t) * tot, s), "memset");
     PSB_CUDA_TRY(c, cudaMemsetAsync(c->escape, 0, sizeof(int32_t) * tot, s), "memset");
     PSB_CUDA_TRY(c, cudaMemsetAsync(c->parent, 0, sizeof(int32_t) * tot, s), "memset");
     const int64_t nalloc = nint > 0 ? nint : 1;
-    PSB_CUDA_TRY(c, cudaMalloc(&c->range_lo, sizeof(int32_t) * nalloc), "cudaMalloc range");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->range_hi, sizeof(int32_t) * nalloc), "cudaMalloc range");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->range_lo, sizeof(int32_t) * nalloc), "cudaMalloc range");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->range_hi, sizeof(int32_t) * nalloc), "cudaMalloc range");
     for (int d = 0; d < 3; ++d) {
-        PSB_CUDA_TRY(c, cudaMalloc(&c->nmin[d], es * nalloc), "cudaMalloc node_min");
-        PSB_CUDA_TRY(c, cudaMalloc(&c->nmax[d], es * nalloc), "cudaMalloc node_max");
+        PSB_CUDA_TRY(c, dgrow_t(c, &c->nmin[d], es * nalloc), "cudaMalloc node_min");
+        PSB_CUDA_TRY(c, dgrow_t(c, &c->nmax[d], es * nalloc), "cudaMalloc node_max");
     }
-    PSB_CUDA_TRY(c, cudaMalloc(&c->nscale, es * nalloc), "cudaMalloc node_scale");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->nscale, es * nalloc), "cudaMalloc node_scale");
     c->root = (n >= 2) ? 1 : 0;
     if (nint > 0) {
         k_karras<<<grid_for(nint), BT, 0, s>>>(codes, n, c->left, c->right, c->parent, c->range_lo, c->range_hi);
@@ -430,15 +429,15 @@ static int build_typed(psb_ctx* c) {
     }
 
     // float traversal records
-    PSB_CUDA_TRY(c, cudaMalloc(&c->links, sizeof(int4) * nalloc), "cudaMalloc links");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->links, sizeof(int4) * nalloc), "cudaMalloc links");
     if (nint > 0) k_pack_links<<<grid_for(nint), BT, 0, s>>>(nint, c->left, c->escape, c->range_lo, c->range_hi, c->links);
-    PSB_CUDA_TRY(c, cudaMalloc(&c->node_lo, sizeof(float4) * nalloc), "cudaMalloc node_lo");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->node_hi, sizeof(float4) * nalloc), "cudaMalloc node_hi");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->leaf4, sizeof(float4) * n), "cudaMalloc leaf4");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->mrho, sizeof(float) * n), "cudaMalloc mrho");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->mf, sizeof(float) * n), "cudaMalloc mf");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->leafK, sizeof(float4) * n), "cudaMalloc leafK");
-    PSB_CUDA_TRY(c, cudaMalloc(&c->spanb, sizeof(float2) * n), "cudaMalloc span bounds");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->node_lo, sizeof(float4) * nalloc), "cudaMalloc node_lo");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->node_hi, sizeof(float4) * nalloc), "cudaMalloc node_hi");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->leaf4, sizeof(float4) * n), "cudaMalloc leaf4");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->mrho, sizeof(float) * n), "cudaMalloc mrho");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->mf, sizeof(float) * n), "cudaMalloc mf");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->leafK, sizeof(float4) * n), "cudaMalloc leafK");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->spanb, sizeof(float2) * n), "cudaMalloc span bounds");
     PSB_CUDA_TRY(c, cudaMemsetAsync(c->spanb, 0, sizeof(float2) * n, s), "memset span bounds");
     if (nint > 0)
         k_pack_nodes<T><<<grid_for(nint), BT, 0, s>>>(nint, (const T*)c->nmin[0], (const T*)c->nmin[1],
@@ -451,7 +450,7 @@ static int build_typed(psb_ctx* c) {
                                                 (const T*)c->m, (const T*)c->rho, sfirst, c->leaf4, c->mrho, c->mf,
                                                 c->leafK, c->spanb);
     if (sizeof(T) == 8 && c->ncol > 0) {
-        PSB_CUDA_TRY(c, cudaMalloc(&c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
+        PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
         for (int k = 0; k < c->ncol; ++k)
             k_to_float<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], n, c->colsf + (size_t)k * n);
     }
@@ -466,7 +465,7 @@ static int build_typed(psb_ctx* c) {
     if (herr) {
         cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
-        free_tree(c);
+        reset_tree(c);
         if (herr & PSB_DERR_INPUT)
             return fail(c, PSB_EINVAL, "particle coordinates must be finite (NaN or Inf found)");
         return fail(c, PSB_ETRAVERSAL, "LBVH refit did not combine every internal node exactly twice");

@@ -38,36 +38,47 @@ void* scratch(psb_ctx* c, int k, size_t bytes) {
     return sl.p;
 }
 
-static void dfree(void*& p) {
-    if (p) cudaFree(p);
-    p = nullptr;
-}
-template <class P> static void dfree_t(P*& p) {
-    if (p) cudaFree((void*)p);
-    p = nullptr;
+static cudaError_t grow_buf(psb_ctx* c, void*& p, size_t& cap, size_t bytes) {
+    if (bytes < 256) bytes = 256;
+    if (p && cap >= bytes) return cudaSuccess;
+    if (p) {
+        cudaStreamSynchronize(c->stream);  // the old buffer may still be in use
+        cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    const cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return e;
+    }
+    cap = bytes;
+    return cudaSuccess;
 }
 
-void free_tree(psb_ctx* c) {
-    dfree_t(c->codes); dfree_t(c->order);
-    dfree_t(c->left); dfree_t(c->right); dfree_t(c->escape); dfree_t(c->parent);
-    dfree_t(c->range_lo); dfree_t(c->range_hi); dfree_t(c->links);
-    for (int d = 0; d < 3; ++d) { dfree(c->nmin[d]); dfree(c->nmax[d]); }
-    dfree(c->nscale);
-    dfree_t(c->node_lo); dfree_t(c->node_hi); dfree_t(c->leaf4);
-    dfree_t(c->mrho); dfree_t(c->mf); dfree_t(c->leafK); dfree_t(c->spanb); dfree_t(c->colsf);
+cudaError_t dgrow(psb_ctx* c, void** p, size_t bytes) { return grow_buf(c, *p, c->caps[(const void*)p], bytes); }
+
+void reset_tree(psb_ctx* c) {
     c->built = false;
     c->root = 0;
 }
 
-void free_particles(psb_ctx* c) {
-    free_tree(c);
-    dfree(c->x); dfree(c->y); dfree(c->z); dfree(c->m); dfree(c->h); dfree(c->rho);
-    for (auto& p : c->cols) dfree(p);
+void release_buffers(psb_ctx* c) {
+    reset_tree(c);
+    for (auto& kv : c->caps) {
+        void** p = (void**)kv.first;
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+    }
+    c->caps.clear();
+    for (void*& p : c->colpool)
+        if (p) cudaFree(p);
+    c->colpool.clear();
+    c->colcap.clear();
     c->cols.clear();
-    dfree_t(c->d_cols);
     c->n = 0;
-    c->ncol = 0;
 }
+
 
 // M4 line-integrated kernel table: I(q) = (1/pi) * integral over s of
 // f(sqrt(q^2 + s^2)), f the M4 shape (kernel_function/kernels/M4_spline.jl:13-24),
@@ -172,7 +183,7 @@ PSB_API int psb_destroy(psb_ctx* c) {
     if (!c) return PSB_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    free_particles(c);
+    release_buffers(c);
     if (c->sctx) psb_destroy(c->sctx);
     c->sctx = nullptr;
     for (auto& sl : c->scratch) {
@@ -219,7 +230,7 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
     for (int k = 0; n > 0 && k < ncol; ++k)
         if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
     cudaSetDevice(c->device);
-    free_particles(c);
+    reset_tree(c);
     c->dt = dt;
     c->es = (dt == PSB_F64) ? 8 : 4;
     c->kern = kernel;
@@ -230,15 +241,20 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
     void** dst[6] = {&c->x, &c->y, &c->z, &c->m, &c->h, &c->rho};
     const void* src[6] = {x, y, z, m, h, rho};
     for (int k = 0; k < 6; ++k) {
-        PSB_CUDA_TRY(c, cudaMalloc(dst[k], bytes), "cudaMalloc particles");
+        PSB_CUDA_TRY(c, dgrow(c, dst[k], bytes), "cudaMalloc particles");
         if (n > 0) PSB_CUDA_TRY(c, cudaMemcpyAsync(*dst[k], src[k], c->es * n, kind, c->stream), "particle copy");
+    }
+    if ((int32_t)c->colpool.size() < ncol) {
+        c->colpool.resize(ncol, nullptr);
+        c->colcap.resize(ncol, 0);
     }
     c->cols.assign(ncol, nullptr);
     for (int k = 0; k < ncol; ++k) {
-        PSB_CUDA_TRY(c, cudaMalloc(&c->cols[k], bytes), "cudaMalloc columns");
+        PSB_CUDA_TRY(c, grow_buf(c, c->colpool[k], c->colcap[k], bytes), "cudaMalloc columns");
+        c->cols[k] = c->colpool[k];
         if (n > 0) PSB_CUDA_TRY(c, cudaMemcpyAsync(c->cols[k], cols[k], c->es * n, kind, c->stream), "column copy");
     }
-    PSB_CUDA_TRY(c, cudaMalloc(&c->d_cols, sizeof(void*) * (ncol > 0 ? ncol : 1)), "cudaMalloc column table");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->d_cols, sizeof(void*) * (ncol > 0 ? ncol : 1)), "cudaMalloc column table");
     if (ncol > 0)
         PSB_CUDA_TRY(c, cudaMemcpyAsync(c->d_cols, c->cols.data(), sizeof(void*) * ncol, cudaMemcpyHostToDevice, c->stream),
                      "column table copy");

@@ -51,10 +51,11 @@ struct AdjArgs {
 
 // M4 at delta = x_s - x_b: W, gradW = sigma/h^5 g1(q) delta and the Hessian
 // (xx, yy, zz, xy, xz, yz) = sigma/h^5 (g1 I + g2 q delta delta^T / r^2), with
-// g1 = f'(q)/q and g2 = d g1/dq (kernels/M4_spline.jl:13-36).
-__device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r, double h, double& W, double g[3],
-                                         double H[6]) {
-    const double invh = 1.0 / h;
+// g1 = f'(q)/q and g2 = d g1/dq (kernels/M4_spline.jl:13-36); invh = 1/h.
+// HESS = false leaves H untouched (scalar catalogs need W and gradW only).
+template <bool HESS = true>
+__device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r, double invh, double& W,
+                                         double g[3], double H[6]) {
     const double q = r * invh;
     const double sig = inv_pi<double>();
     const double ih3 = invh * invh * invh, ih5 = ih3 * invh * invh;
@@ -73,8 +74,9 @@ __device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r
     }
     W = sig * ih3 * f;
     const double c = sig * ih5 * g1;
-    const double e = (r2 > 0.0) ? sig * ih5 * g2 * q / r2 : 0.0;
     g[0] = c * dl[0]; g[1] = c * dl[1]; g[2] = c * dl[2];
+    if (!HESS) return;
+    const double e = (r2 > 0.0) ? sig * ih5 * g2 * q / r2 : 0.0;
     H[0] = c + e * dl[0] * dl[0]; H[1] = c + e * dl[1] * dl[1]; H[2] = c + e * dl[2] * dl[2];
     H[3] = e * dl[0] * dl[1]; H[4] = e * dl[0] * dl[2]; H[5] = e * dl[1] * dl[2];
 }
@@ -87,11 +89,19 @@ __device__ __forceinline__ void hmul(const double H[6], const double v[3], doubl
 
 struct AStage {
     double sx[SPAN], sy[SPAN], sz[SPAN], sh[SPAN];  // samples of the span, h_a
-    double px[SPAN], py[SPAN], pz[SPAN], ph[SPAN];  // the warp's particles
+    double sih[SPAN];                               // 1 / h_a
+    float4 Q[SPAN];   // the samples relative to the warp anchor, float h_a
+    float2 AB[SPAN];  // their squared radius thresholds (surely in, maybe in)
+    float4 PP[SPAN];  // the warp's particles relative to the warp anchor
+    float2 PAB[SPAN]; // their squared radius thresholds
 };
 
-template <int ST, int KC>
-__global__ void __launch_bounds__(128) k_adj_points(const AdjArgs A) {
+// SCAL: every output of the catalog is a (plain or Shepard) scalar, so only
+// lambda_S1 and lambda_Sw_c can be non-zero: the pair terms drop the Hessian
+// and the gradient cotangents (the same values as the general form, which
+// adds exact zeros).
+template <int ST, int KC, bool SCAL>
+__global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs A) {
     __shared__ AStage stage_all[4];
     const TreeView<double>& pt = A.pt;
     const TreeView<double>& sv = A.sv;
@@ -112,38 +122,76 @@ __global__ void __launch_bounds__(128) k_adj_points(const AdjArgs A) {
         for (int c = 0; c < KC; ++c)
             if (c < A.kc) Ab[c] = A.colT[c][b];
     }
-    st.px[lane] = xb[0]; st.py[lane] = xb[1]; st.pz[lane] = xb[2]; st.ph[lane] = hb;
     // this particle's own support radius^2, with the forward's operation order
     const double rb = X<double>::mul(2.0, hb);
     const double rb2 = X<double>::mul(rb, rb);
-    const double mr = mb / rhob;
-    double gm = 0.0, gx[3] = {0.0, 0.0, 0.0}, ga[KC];
+    // float pair tests against a band (as in the forward's float walk): the
+    // particle relative to the warp anchor (the first valid particle) with its
+    // rounding error, its radius bounds and the warp-wide maxima of both
+    const unsigned vmask = __ballot_sync(PSB_FULL, valid);
+    const int first = vmask ? __ffs(vmask) - 1 : 0;
+    const double cw[3] = {__shfl_sync(PSB_FULL, xb[0], first), __shfl_sync(PSB_FULL, xb[1], first),
+                          __shfl_sync(PSB_FULL, xb[2], first)};
+    const float P[3] = {(float)(xb[0] - cw[0]), (float)(xb[1] - cw[1]), (float)(xb[2] - cw[2])};
+    float esmax = U1 * (fabsf(P[0]) + fabsf(P[1]) + fabsf(P[2])) + 1e-30f;
+    float rblo = 0.f, rbmax = 0.f;
+    if (ST != ST_GATHER) {
+        rblo = __double2float_rd(rb) * (1.f - 2.f * U1);
+        rbmax = __double2float_ru(rb) * (1.f + 2.f * U1);
+    }
+    const float rbhi = rbmax;
 #pragma unroll
-    for (int c = 0; c < KC; ++c) ga[c] = 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+        esmax = fmaxf(esmax, __shfl_xor_sync(PSB_FULL, esmax, o));
+        rbmax = fmaxf(rbmax, __shfl_xor_sync(PSB_FULL, rbmax, o));
+    }
+    const double mr = mb / rhob;
+    const double ihb = 1.0 / hb;
+    // pair sums; the particle's factors 1/rho_b, m_b/rho_b and m_b are applied
+    // once after the walk: dL/dm_b = sW / rho_b + sD, dL/dA_c,b = m_b/rho_b sA_c,
+    // dL/dx_b = -(m_b/rho_b vS + m_b vD)
+    double sW = 0.0, sD = 0.0, vS[3] = {0.0, 0.0, 0.0}, vD[3] = {0.0, 0.0, 0.0}, sA[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) sA[c] = 0.0;
     const int kc = A.kc;
     const int64_t L = A.lam_stride;
-    unsigned long long n_pairs = 0;
+    unsigned long long n_pairs = 0, n_spans = 0, n_parts = 0, n_leaves = 0;  // work counters (warp-uniform)
     int64_t steps = 0;
 
-    auto pair = [&](int64_t li, double sxv, double syv, double szv, double ha) {
+    auto pair = [&](int64_t li, double sxv, double syv, double szv, double iha) {
         ++n_pairs;
         const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
         const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
         const double r = sqrt(r2);
         double W, g[3], H[6];
         if (ST == ST_GATHER) {
-            m4_whess(dl, r2, r, ha, W, g, H);
+            m4_whess<!SCAL>(dl, r2, r, iha, W, g, H);
         } else if (ST == ST_SCATTER) {
-            m4_whess(dl, r2, r, hb, W, g, H);
+            m4_whess<!SCAL>(dl, r2, r, ihb, W, g, H);
         } else {
             double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
-            m4_whess(dl, r2, r, ha, Wa, ga3, Ha);
-            m4_whess(dl, r2, r, hb, Wb, gb3, Hb);
+            m4_whess<!SCAL>(dl, r2, r, iha, Wa, ga3, Ha);
+            m4_whess<!SCAL>(dl, r2, r, ihb, Wb, gb3, Hb);
             W = 0.5 * (Wa + Wb);
             for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
-            for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
+            if (!SCAL)
+                for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
         }
         const double* lam = A.lam + li;
+        if constexpr (SCAL) {
+            double aS = __ldg(&lam[0]);
+#pragma unroll
+            for (int c = 0; c < KC; ++c) {
+                if (c < kc) {
+                    const double lsw = __ldg(&lam[(8 + c) * L]);
+                    aS += lsw * Ab[c];
+                    sA[c] += lsw * W;
+                }
+            }
+            sW += aS * W;
+            for (int d = 0; d < 3; ++d) vS[d] += aS * g[d];
+            return;
+        }
         const double lS1 = __ldg(&lam[0]);
         const double lG[3] = {__ldg(&lam[L]), __ldg(&lam[2 * L]), __ldg(&lam[3 * L])};
         const double lDm = __ldg(&lam[4 * L]);
@@ -157,56 +205,126 @@ __global__ void __launch_bounds__(128) k_adj_points(const AdjArgs A) {
                                        __ldg(&lam[(10 + kc + 3 * c) * L])};
                 aS += lsw * Ab[c];
                 aG[0] += Ab[c] * lsg[0]; aG[1] += Ab[c] * lsg[1]; aG[2] += Ab[c] * lsg[2];
-                ga[c] += mr * (lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2]);
+                sA[c] += lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2];
             }
         }
-        gm += (aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2]) / rhob + lDm * W + lDg[0] * g[0] +
-              lDg[1] * g[1] + lDg[2] * g[2];
+        sW += aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2];
+        sD += lDm * W + lDg[0] * g[0] + lDg[1] * g[1] + lDg[2] * g[2];
         double Ha[3], Hd[3];
         hmul(H, aG, Ha);
         hmul(H, lDg, Hd);
-        for (int d = 0; d < 3; ++d) gx[d] -= mr * (aS * g[d] + Ha[d]) + mb * (lDm * g[d] + Hd[d]);
+        for (int d = 0; d < 3; ++d) {
+            vS[d] += aS * g[d] + Ha[d];
+            vD[d] += lDm * g[d] + Hd[d];
+        }
     };
 
-    // node test seen from the particle: the largest sample radius in the node
-    // (node scale = max h_a) for gather, the particle's own for scatter
+    // node test seen from the particle, on the float node records (box
+    // rounded outwards, scale = max h_a rounded up): the largest sample radius
+    // in the node for gather, the particle's own for scatter, the larger for
+    // symmetric.  A lower bound of the distance against an upper bound of
+    // the radius never prunes a node holding a pair (the pair test itself
+    // stays exact).
+    const float pf[3] = {(float)xb[0], (float)xb[1], (float)xb[2]};
+    const float pem = U1 * fmaxf(fmaxf(fabsf(pf[0]), fabsf(pf[1])), fabsf(pf[2])) + 1e-30f;
+    const float rb2_hi = __double2float_ru(rb2) * (1.f + RELM);
+    constexpr int SN = (ST == ST_GATHER) ? ST_SCATTER : ((ST == ST_SCATTER) ? ST_GATHER : ST_SYMMETRIC);
     auto node_fn = [&](int ni) -> bool {
-        const double d2n = ex_d2_pbox<double>(xb, sv, ni);
-        double r2;
-        if (ST == ST_SCATTER) {
-            r2 = rb2;
-        } else {
-            const double rs = X<double>::mul(2.0, __ldg(&sv.nscale[ni]));
-            const double rs2 = X<double>::mul(rs, rs);
-            r2 = (ST == ST_GATHER) ? rs2 : jmax(rs2, rb2);
-        }
-        return !(d2n > r2);
+        const float4 lo = __ldg(&sv.node_lo[ni]), hi = __ldg(&sv.node_hi[ni]);
+        return !(lb_d2_pbox(pf, pem, lo, hi) > hi_r2_node<SN>(rb2_hi, lo.w));
     };
     auto span_fn = [&](int64_t lo, int cnt, bool part) {
+        const unsigned parts = __ballot_sync(PSB_FULL, part);
+        if (!parts) return;
+        ++n_spans;
+        n_parts += __popc(parts);
+        n_leaves += cnt;
+        // one error bound E for every float distance of the span (the
+        // samples are stored relative to the span's first sample)
+        const float o0 = (float)(__ldg(&sv.x[lo]) - cw[0]);
+        const float o1 = (float)(__ldg(&sv.y[lo]) - cw[1]);
+        const float o2 = (float)(__ldg(&sv.z[lo]) - cw[2]);
+        const float2 sb = __ldg(&sv.spanb[lo]);
+        const float eqm = U1 * (2.f * sb.x + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
+        float rmax = rbmax;
+        if (ST != ST_SCATTER) rmax = fmaxf(rmax, 2.f * sb.y * (1.f + 2.f * U1));
+        const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
+        // squared radius thresholds of this lane's particle and of sample
+        // `lane` (surely in: d2 < A; maybe in: d2 <= B)
+        float As = 0.f, Bs = 0.f, Aj = 0.f, Bj = 0.f;
+        if (ST != ST_GATHER) {  // the particle's own radius 2 h_b
+            const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih = (rbhi + E) * (1.f + 4.f * U1);
+            As = il * il;
+            Bs = ih * ih;
+        }
+        float4 Qme = make_float4(0.f, 0.f, 0.f, 0.f);
         __syncwarp();
         if (lane < cnt) {
             st.sx[lane] = __ldg(&sv.x[lo + lane]); st.sy[lane] = __ldg(&sv.y[lo + lane]);
             st.sz[lane] = __ldg(&sv.z[lo + lane]); st.sh[lane] = __ldg(&sv.h[lo + lane]);
+            st.sih[lane] = 1.0 / st.sh[lane];
+            const float4 Lq = __ldg(&sv.leaf4[lo + lane]);
+            Qme = make_float4(Lq.x + o0, Lq.y + o1, Lq.z + o2, Lq.w);
+            st.Q[lane] = Qme;
+            if (ST != ST_SCATTER) {  // the sample's radius 2 h_a
+                const float rahi = 2.f * Lq.w * (1.f + 2.f * U1), ralo = 2.f * Lq.w * (1.f - 2.f * U1);
+                const float il = fmaxf((ralo - E) * (1.f - 4.f * U1), 0.f), ih = (rahi + E) * (1.f + 4.f * U1);
+                Aj = il * il;
+                Bj = ih * ih;
+                st.AB[lane] = make_float2(Aj, Bj);
+            }
+        }
+        const int np = __popc(parts);
+        const bool by_particle = 3 * np >= 2 * cnt;  // warp-uniform
+        if (!by_particle) {
+            st.PP[lane] = make_float4(P[0], P[1], P[2], 0.f);
+            st.PAB[lane] = make_float2(As, Bs);
         }
         __syncwarp();
-        const unsigned parts = __ballot_sync(PSB_FULL, part);
-        if (!parts) return;
-        // lane j holds sample j; the forward's pair test for every participating particle
-        const int j = lane < cnt ? lane : 0;
-        const double ps[3] = {st.sx[j], st.sy[j], st.sz[j]};
-        const double ra = X<double>::mul(2.0, st.sh[j]);
-        const double ra2 = X<double>::mul(ra, ra);
-        unsigned acc = 0;
-        for (unsigned pp = parts; pp; pp &= pp - 1) {
-            const int s = __ffs(pp) - 1;
-            const double e2 = ex_d2_pp<double>(ps, st.px[s], st.py[s], st.pz[s]);
-            const bool in = (lane < cnt) && (e2 <= ex_r2<ST, double>(ra2, st.ph[s]));
-            const unsigned bi = __ballot_sync(PSB_FULL, in);
-            if (lane == s) acc = bi;
+        unsigned acc = 0, maybe = 0;
+        if (!by_particle) {
+            // few particles take part: sample `lane` against each of them
+            for (unsigned pp = parts; pp; pp &= pp - 1) {
+                const int s = __ffs(pp) - 1;
+                const float4 Pp = st.PP[s];
+                const float2 ab = st.PAB[s];
+                const float dx = Pp.x - Qme.x, dy = Pp.y - Qme.y, dz = Pp.z - Qme.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                const float At = (ST == ST_GATHER) ? Aj : ((ST == ST_SCATTER) ? ab.x : fmaxf(ab.x, Aj));
+                const float Bt = (ST == ST_GATHER) ? Bj : ((ST == ST_SCATTER) ? ab.y : fmaxf(ab.y, Bj));
+                const unsigned bi = __ballot_sync(PSB_FULL, lane < cnt && d2 < At);
+                const unsigned bm = __ballot_sync(PSB_FULL, lane < cnt && d2 <= Bt);
+                if (lane == s) { acc = bi; maybe = bm; }
+            }
+        } else if (part) {
+            // this lane's particle against every sample of the span
+#pragma unroll 4
+            for (int j = 0; j < cnt; ++j) {
+                const float4 Q = st.Q[j];
+                const float dx = P[0] - Q.x, dy = P[1] - Q.y, dz = P[2] - Q.z;
+                const float d2 = dx * dx + dy * dy + dz * dz;
+                float At = As, Bt = Bs;
+                if (ST != ST_SCATTER) {
+                    const float2 ab = st.AB[j];
+                    At = (ST == ST_GATHER) ? ab.x : fmaxf(As, ab.x);
+                    Bt = (ST == ST_GATHER) ? ab.y : fmaxf(Bs, ab.y);
+                }
+                acc |= (unsigned)(d2 < At) << j;
+                maybe |= (unsigned)(d2 <= Bt) << j;
+            }
+        }
+        // undecided pairs: the forward's exact test
+        for (unsigned u = maybe & ~acc; u; u &= u - 1) {
+            const int jj = __ffs(u) - 1;
+            const double ps[3] = {st.sx[jj], st.sy[jj], st.sz[jj]};
+            const double ra = X<double>::mul(2.0, st.sh[jj]);
+            const double ra2 = X<double>::mul(ra, ra);
+            const double e2 = ex_d2_pp<double>(ps, xb[0], xb[1], xb[2]);
+            if (e2 <= ex_r2<ST, double>(ra2, hb)) acc |= 1u << jj;
         }
         for (; acc; acc &= acc - 1) {
             const int jj = __ffs(acc) - 1;
-            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj]);
+            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sih[jj]);
         }
     };
     const int32_t start = (sv.root == 0) ? (int32_t)sv.n : sv.root;
@@ -214,18 +332,24 @@ __global__ void __launch_bounds__(128) k_adj_points(const AdjArgs A) {
 
     if (valid) {
         const int64_t o = A.porder[b];
-        A.gm[o] = gm;
-        A.gx[o] = gx[0]; A.gy[o] = gx[1]; A.gz[o] = gx[2];
+        A.gm[o] = sW / rhob + sD;
+        A.gx[o] = -(mr * vS[0] + mb * vD[0]);
+        A.gy[o] = -(mr * vS[1] + mb * vD[1]);
+        A.gz[o] = -(mr * vS[2] + mb * vD[2]);
 #pragma unroll
         for (int c = 0; c < KC; ++c)
-            if (c < kc && A.gcol[c]) A.gcol[c][o] = ga[c];
+            if (c < kc && A.gcol[c]) A.gcol[c][o] = mr * sA[c];
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
     if (lane == 0 && A.stats) {
         atomicAdd(&A.stats[0], n_pairs);
         atomicAdd(&A.stats[2], (unsigned long long)steps);
+        atomicAdd(&A.stats[3], n_spans);
+        atomicAdd(&A.stats[4], n_parts);
+        atomicAdd(&A.stats[5], n_leaves);
     }
+
     if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
 }
 

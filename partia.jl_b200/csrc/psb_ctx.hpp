@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "psb_common.cuh"
@@ -22,7 +23,9 @@ struct psb_ctx {
     int32_t ncol = 0;
     void* x = nullptr; void* y = nullptr; void* z = nullptr;
     void* m = nullptr; void* h = nullptr; void* rho = nullptr;
-    std::vector<void*> cols;
+    std::vector<void*> cols;        // ncol column buffers (taken from colpool)
+    std::vector<void*> colpool;     // column buffers kept across set_particles calls
+    std::vector<size_t> colcap;     // their sizes in bytes
     void** d_cols = nullptr;
 
     // LBVH
@@ -52,6 +55,11 @@ struct psb_ctx {
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };
     Slot scratch[64];
+    // sizes of the particle and tree buffers above, keyed by the address of
+    // the pointer member: they are kept across set_particles and builds and
+    // reallocated only to grow, so repeated builds of the same size (the
+    // sample LBVH of every adjoint call) allocate nothing
+    std::unordered_map<const void*, size_t> caps;
 
     // adjoint: while adj_lam is set, an FP64 interpolation call writes the
     // cotangents of its per-sample sums (from the output cotangents adj_gout,
@@ -79,8 +87,14 @@ int cuda_fail(psb_ctx* c, cudaError_t e, const char* what);
 // Grow-on-demand scratch slot k to at least `bytes`; returns nullptr on failure.
 void* scratch(psb_ctx* c, int k, size_t bytes);
 // Free every particle and tree buffer (not the scratch).
-void free_particles(psb_ctx* c);
-void free_tree(psb_ctx* c);
+// Device buffer *p with room for at least `bytes`, reallocated only when it
+// must grow (after the context's stream has finished with the old one).
+cudaError_t dgrow(psb_ctx* c, void** p, size_t bytes);
+template <class P> cudaError_t dgrow_t(psb_ctx* c, P** p, size_t bytes) { return dgrow(c, (void**)p, bytes); }
+// Mark the LBVH as absent (its buffers are kept for the next build).
+void reset_tree(psb_ctx* c);
+// Free every particle and tree buffer (context destruction).
+void release_buffers(psb_ctx* c);
 
 // build.cu
 int build_lbvh(psb_ctx* c);

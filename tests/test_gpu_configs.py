@@ -17,7 +17,8 @@ decisions against FP64 ones (identical neighbour sets).
    against the oracle's adjoint.
  * C5-shaped: 4M float32 disc + halo particles, rho, grad rho, curl v,
    Shepard z^2 on a grid and an oriented box: FP32C against FP64, oracle
-   subset at float accuracy.
+   subset at float accuracy.  The adjoint of the grid scalar's L2 norm for
+   2M of them: identities at full grid size, oracle on a sample subset.
 """
 import numpy as np
 import pytest
@@ -183,3 +184,46 @@ def test_c5_shaped_float_inputs():
     ref = orc.interp_points(*ss, O.Catalog(**spec), strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
     for k in range(len(ref)):
         assert rel_err(g64[k][idx], ref[k]) <= 2e-4, (k, rel_err(g64[k][idx], ref[k]))
+
+
+def test_c5_shaped_adjoint_of_grid_scalar():
+    """Gradient of the grid scalar's L2 norm (Shepard z^2) for 2M disc + halo
+    particles (the float32 values in double).  At full grid size: S is linear
+    in A and invariant under a common mass scaling, so <dL/dA, A> = <gout, S>
+    and <dL/dm, m> = 0.  Against the oracle's adjoint with the cotangent on
+    1500 random grid samples."""
+    d = W.disc_halo_c5(2_000_000, 4)
+    h, rho = W.density_h(d)
+    dd = {k: np.asarray(d[k], dtype=np.float64) for k in ("x", "y", "z", "m", "z2")}
+    h, rho = np.asarray(h, dtype=np.float64), np.asarray(rho, dtype=np.float64)
+    cols = [rho, dd["z2"]]
+    ctx = make_ctx(dd, h, rho, cols)
+    spec = dict(scalars=[1], shepard=[1])
+    ax = linrange(-1.0, 1.0, 48)
+    S = ctx.interp_grid(ax, ax, ax, CatalogC(**spec), strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP64)[0]
+    S0 = np.nan_to_num(S, nan=0.0)
+    gout = S0 / np.linalg.norm(S0)
+    g = ctx.adjoint_grid(ax, ax, ax, CatalogC(**spec), [gout], strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST)
+    lhs, rhs = float(np.dot(g["cols"][1], dd["z2"])), float(np.dot(gout, S0))
+    assert abs(lhs - rhs) <= 1e-10 * abs(rhs), (lhs, rhs)
+    gm = g["m"] * dd["m"]
+    assert abs(gm.sum()) <= 1e-10 * np.abs(gm).sum()
+    assert np.abs(g["cols"][0]).max() == 0  # column 0 enters only as rho_b
+    # oracle on a subset of samples
+    rng = np.random.default_rng(52)
+    s_all = grid_points(ax, ax, ax)
+    idx = rng.choice(len(S0), 1500, replace=False)
+    gsub = np.zeros_like(gout)
+    gsub[idx] = rng.standard_normal(len(idx))
+    g2 = ctx.adjoint_grid(ax, ax, ax, CatalogC(**spec), [gsub], strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST)
+    orc = O.Oracle(dd["x"], dd["y"], dd["z"], dd["m"], h, rho, cols)
+    threads = O.set_threads(0)
+    O.set_threads(min(threads, 4))  # per-thread gradient buffers of 2M particles
+    try:
+        r = orc.adjoint_points(*(a[idx] for a in s_all), O.Catalog(**spec), [gsub[idx]], strategy=O.SYMMETRIC,
+                               hmode=O.H_NEAREST)
+    finally:
+        O.set_threads(threads)
+    for key in ("m", "x", "y", "z"):
+        assert rel_err(g2[key], r[key]) <= 1e-10, key
+    assert rel_err(g2["cols"][1], r["cols"][1]) <= 1e-10

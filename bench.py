@@ -200,10 +200,16 @@ def lines_and_adjoint(steps, warmup):
     a, b = out32[0], out64[0]
     fin = torch.isfinite(b)
     err = ((a[fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
+    # the 1000-entry float table of the line integral, against the 4096-entry FP64 result
+    ctx.extra_flags = L.PSB_FLAG_LUT1000_F32
+    t1000 = timed_call(f32, stream, steps, warmup)
+    ctx.extra_flags = 0
+    err1000 = ((out32[0][fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
     res["lines"] = {"workload": "clumps-8M column density, 1024^2 parallel beam, scatter", "N": 8_000_000,
                     "lines": npix * npix, "pairs": int(pairs), "fp32c_ms": t32, "fp64_ms": t64,
                     "lines_per_s": npix * npix / (t32 / 1e3), "fp64_lines_per_s": npix * npix / (t64 / 1e3),
-                    "speedup_fp32c_vs_fp64": t64 / t32, "fp32c_rel_err_vs_fp64": err}
+                    "speedup_fp32c_vs_fp64": t64 / t32, "fp32c_rel_err_vs_fp64": err,
+                    "lut1000_f32": {"fp32c_ms": t1000, "rel_err_vs_fp64_lut4096": err1000}}
     ctx.close()
     del out32, out64
 
@@ -238,7 +244,7 @@ def lines_and_adjoint(steps, warmup):
     return res
 
 
-def large_leg(steps, warmup):
+def large_leg(steps, warmup, oracle_check=True):
     """The large mixed configuration: 64M float32 particles (70% exponential
     disc, 30% Plummer halo; h and rho from the density sum), rho, Shepard z^2,
     grad rho and curl v on a 256^3 grid over [-1,1]^3 plus four randomly
@@ -308,6 +314,7 @@ def large_leg(steps, warmup):
             fin = torch.isfinite(b) & torch.isfinite(a)
             e[names[k]] = ((a[fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
         return e
+    ora = oracle_subset(d, h, rho, cols, ax, frames, bprm, nb, outs, names) if oracle_check else None
     res["float32_storage"]["note"] = ("particle data kept in float32; inclusion tests and nearest-particle h in float "
                                       "arithmetic, as the reference computes with Float32 inputs")
     res["fp32c"]["particles"] = res["fp64"]["particles"] = "the float32 values converted to double on the device"
@@ -317,7 +324,55 @@ def large_leg(steps, warmup):
             "speedup_fp32c_vs_fp64": res["fp64"]["ms"] / res["fp32c"]["ms"],
             "fp32c_rel_err_vs_fp64": errs(outs["fp32c"], outs["fp64"]),
             "float32_storage_rel_err_vs_fp64": errs(outs["float32_storage"], outs["fp64"]),
-            "adjoint": res["adjoint"]}
+            "oracle_subset": ora, "adjoint": res["adjoint"]}
+
+
+def oracle_subset(d, h, rho, cols, ax, frames, bprm, nb, outs, names, nsub=100_000):
+    """The FP64 CPU oracle over all particles (the float32 values in double) on
+    a random subset of the grid and box samples; relative error of each GPU
+    field (FP64 and FP32C) against it, over the subset's finite values."""
+    import torch
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    nthr = O.set_threads(os.cpu_count() or 1)
+    f64 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    t0 = time.time()
+    orc = O.Oracle(f64(d["x"]), f64(d["y"]), f64(d["z"]), f64(d["m"]), f64(h), f64(rho), [f64(c) for c in cols])
+    build_s = time.time() - t0
+    ng = len(ax)
+    ng3, nb3 = ng ** 3, nb ** 3
+    rng = np.random.default_rng(41)
+    idx = np.sort(rng.choice(ng3 + len(frames) * nb3, nsub, replace=False))
+    sx, sy, sz = np.empty(nsub), np.empty(nsub), np.empty(nsub)
+    g = idx < ng3
+    i, r = idx[g] % ng, idx[g] // ng
+    sx[g], sy[g], sz[g] = ax[i], ax[r % ng], ax[r // ng]
+    lo, hi = bprm[0], bprm[1]
+    dq = (hi - lo) / float(nb - 1)
+    for bi, fa in enumerate(frames):  # box_coordinates' arithmetic at the chosen indices
+        sel = (idx >= ng3 + bi * nb3) & (idx < ng3 + (bi + 1) * nb3)
+        k = idx[sel] - ng3 - bi * nb3
+        xi, eta, ze = (lo + (k % nb) * dq, lo + ((k // nb) % nb) * dq, lo + (k // (nb * nb)) * dq)
+        x0, rr, u, f = fa[0:3], fa[3:6], fa[6:9], fa[9:12]
+        sx[sel], sy[sel], sz[sel] = (x0[c] + xi * rr[c] + eta * u[c] + ze * f[c] for c in range(3))
+    t0 = time.time()
+    ref = orc.interp_points(sx, sy, sz, O.Catalog(scalars=[0, 4], shepard=[0, 1], grads=[0], curls=[1, 2, 3]),
+                            strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    interp_s = time.time() - t0
+    ti = torch.from_numpy(idx).cuda()
+    out = {"samples": nsub, "threads": nthr, "oracle_build_s": build_s, "oracle_interp_s": interp_s}
+    for label in ("fp64", "fp32c"):
+        e, nan_diff = {}, 0
+        for k in range(8):
+            a = outs[label][k][ti].cpu().numpy()
+            b = np.asarray(ref[k])
+            nan_diff += int(np.count_nonzero(np.isnan(a) != np.isnan(b)))
+            fin = np.isfinite(b) & np.isfinite(a)
+            e[names[k]] = float(np.max(np.abs(a[fin] - b[fin])) / np.max(np.abs(b[fin])))
+        out[label + "_rel_err_vs_oracle"] = e
+        out[label + "_nan_mask_differences"] = nan_diff
+    del orc
+    return out
 
 
 def large_adjoint(ctx, ax, stream, steps, warmup, a_col, m):
@@ -570,7 +625,7 @@ def main():
         extra = lines_and_adjoint(max(3, args.steps // 4), 2)
     large = None
     if world == 1 and not args.no_large:
-        large = large_leg(3, 1)
+        large = large_leg(3, 1, oracle_check=not args.no_cpu)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

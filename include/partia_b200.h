@@ -97,6 +97,13 @@ typedef enum { PSB_H_NEAREST = 0, PSB_H_PER_SAMPLE = 1, PSB_H_CONSTANT = 2 } psb
  * lists, then pair sums).  This flag runs the single-kernel form instead, for
  * comparisons; results agree to rounding. */
 #define PSB_FLAG_SINGLE_KERNEL 0x200u
+/* Line-integrated samples: use a 1000-entry float table of the M4 line
+ * integral (the tabulation the benchmark configuration names) instead of the
+ * 4096-entry table of the reference (table/line_integrated_kernel_tables.jl:1,
+ * looked up as in kernel_function/line_integrated_kernel.jl:13-19).  Both
+ * come from the same quadrature; the short table adds its interpolation and
+ * float rounding error.  No effect on point samples or the adjoint. */
+#define PSB_FLAG_LUT1000_F32 0x400u
 
 /* InterpolationCatalogConcise
  * (src/julia/KernelInterpolation/interpolation_setup/InterpolationCatalog.jl:26-32),

@@ -90,7 +90,7 @@ static long double m4_shape_ld(long double q) {
     return 0;
 }
 
-void m4_line_table(double* I) {
+void m4_line_table(double* I, int n) {
     const int G = 64;
     long double gx[G], gw[G];
     const long double pi = 3.141592653589793238462643383279502884L;
@@ -111,8 +111,8 @@ void m4_line_table(double* I) {
         gx[i] = z;
         gw[i] = 2 / ((1 - z * z) * pp * pp);
     }
-    for (int k = 0; k < LUT_N; ++k) {
-        long double b = 2.0L / (LUT_N - 1) * k, tot = 0;
+    for (int k = 0; k < n; ++k) {
+        long double b = 2.0L / (n - 1) * k, tot = 0;
         if (b < 2) {
             long double s2 = std::sqrt(4 - b * b);
             long double edges[3] = {0, b < 1 ? std::sqrt(1 - b * b) : s2, s2};
@@ -134,7 +134,7 @@ static const double* host_line_table() {
     static double table[LUT_N];
     static bool ready = false;
     if (!ready) {
-        m4_line_table(table);
+        m4_line_table(table, LUT_N);
         ready = true;
     }
     return table;
@@ -161,12 +161,20 @@ PSB_API int psb_create(psb_ctx** out, int device) {
     if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMalloc(&c->lut_d, sizeof(double) * LUT_N);
     if (e == cudaSuccess) e = cudaMalloc(&c->lut_f, sizeof(float) * LUT_N);
+    if (e == cudaSuccess) e = cudaMalloc(&c->lut_fs, sizeof(float) * LUT_SHORT_N);
     if (e == cudaSuccess) {
         const double* t = host_line_table();
         float tf[LUT_N];
         for (int k = 0; k < LUT_N; ++k) tf[k] = (float)t[k];
         e = cudaMemcpy(c->lut_d, t, sizeof(double) * LUT_N, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(c->lut_f, tf, sizeof(float) * LUT_N, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) {
+        static double ts[LUT_SHORT_N];
+        m4_line_table(ts, LUT_SHORT_N);
+        float tsf[LUT_SHORT_N];
+        for (int k = 0; k < LUT_SHORT_N; ++k) tsf[k] = (float)ts[k];
+        e = cudaMemcpy(c->lut_fs, tsf, sizeof(float) * LUT_SHORT_N, cudaMemcpyHostToDevice);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -193,6 +201,7 @@ PSB_API int psb_destroy(psb_ctx* c) {
     if (c->d_err) cudaFree(c->d_err);
     if (c->lut_d) cudaFree(c->lut_d);
     if (c->lut_f) cudaFree(c->lut_f);
+    if (c->lut_fs) cudaFree(c->lut_fs);
     for (auto& ev : c->ev)
         if (ev) cudaEventDestroy(ev);
     for (auto& ev : c->pev)

@@ -15,6 +15,7 @@ enum { WHAT_INTERP = 0, WHAT_DENSITY = 1, WHAT_DIGEST = 2 };
 constexpr int MAX_OUT = 64;
 constexpr int MAX_KC = 8;   // distinct catalog columns per call
 constexpr int LUT_N = 4096;
+constexpr int LUT_SHORT_N = 1000;  // the optional short float table of line kernels
 
 // Output recipes: each output field is a function of the per-sample sums
 // S1 = sum w, G = sum g, Sw[c] = sum A_c w, Sg[c] = sum A_c g,

@@ -171,6 +171,8 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     A.err = c->d_err;
     A.lut_d = c->lut_d;
     A.lut_f = c->lut_f;
+    A.lut_fs = c->lut_fs;
+    A.lut_n = (flags & PSB_FLAG_LUT1000_F32) ? LUT_SHORT_N : LUT_N;
     if (adj) {
         A.gout = c->adj_gout;
         A.lam = c->adj_lam;
@@ -382,6 +384,8 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     A.err = c->d_err;
     A.lut_d = c->lut_d;
     A.lut_f = c->lut_f;
+    A.lut_fs = c->lut_fs;
+    A.lut_n = (flags & PSB_FLAG_LUT1000_F32) ? LUT_SHORT_N : LUT_N;
     for (size_t q = 0; q < colu.size(); ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];

@@ -58,6 +58,8 @@ template <class T> struct Args {
     T* ha_out;
     const double* lut_d;
     const float* lut_f;
+    const float* lut_fs;  // short float table (LUT_SHORT_N entries), used when lut_n == LUT_SHORT_N
+    int lut_n;            // entries of the line table in use
     unsigned* err;
     unsigned long long* stats;  // [0] accepted pairs, [1] exact re-tests, [2] traversal steps
     SplitBufs sp;
@@ -218,12 +220,13 @@ __device__ __forceinline__ float lb_d2_line_box(const float o[3], const float m[
 // ---------------------------------------------------------------------------
 // _lin_lut, kernel_function/line_integrated_kernel.jl:13-19, with the
 // q >= q_max cut (:90-94) and the 1/h factor (:132-137).
-template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq) {
+// n = entries of the table, dq its spacing.
+template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq, int n) {
     C q = r * invh;
     if (q >= C(2)) return C(0);
     C idxf = q / dq + C(1);
     int i = (int)idxf;  // q >= 0
-    i = i < 1 ? 1 : (i > LUT_N - 1 ? LUT_N - 1 : i);
+    i = i < 1 ? 1 : (i > n - 1 ? n - 1 : i);
     C t = idxf - C(i);
     C v = lut[i - 1] * (C(1) - t) + lut[i] * t;
     return invh * v;
@@ -248,11 +251,13 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     CT* lut = (CT*)smem_raw;
     __shared__ LStage<KC> lstage_all[4];
-    for (int i = threadIdx.x; i < LUT_N; i += blockDim.x)
-        lut[i] = (PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i];
+    const int nlut = A.lut_n;
+    const bool short_lut = nlut == LUT_SHORT_N;
+    for (int i = threadIdx.x; i < nlut; i += blockDim.x)
+        lut[i] = short_lut ? (CT)A.lut_fs[i] : ((PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i]);
     __syncthreads();
-    // dq = Q[2] - Q[1] of the 4096-point table = 2/4095 rounded to CT
-    const CT dq = (CT)(2.0 / 4095.0);
+    // dq = Q[2] - Q[1] of the n-point table over [0, 2] = 2/(n-1) rounded to CT
+    const CT dq = (CT)(2.0 / (double)(nlut - 1));
 
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
@@ -304,10 +309,10 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         }
         const CT dr = sqrt(s < CT(0) ? CT(0) : s);
         CT W;
-        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq);
+        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut);
         else {
-            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq);
-            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq) + Wb);
+            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq, nlut);
+            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut) + Wb);
         }
         const CT w = mr * W;
         S1.add(w);

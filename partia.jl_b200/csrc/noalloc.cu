@@ -154,6 +154,8 @@ int noalloc_typed(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const 
     A.err = c->d_err;
     A.lut_d = c->lut_d;
     A.lut_f = c->lut_f;
+    A.lut_fs = c->lut_fs;
+    A.lut_n = LUT_N;
     for (int q = 0; q < A.rec.kc; ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];

@@ -51,6 +51,7 @@ struct psb_ctx {
     unsigned* d_err = nullptr;  // device error word
     double* lut_d = nullptr;    // M4 line-integrated table (4096, double)
     float* lut_f = nullptr;     // the same table rounded to float
+    float* lut_fs = nullptr;    // a 1000-entry float table of the same integral (PSB_FLAG_LUT1000_F32)
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };

@@ -30,6 +30,7 @@ PSB_H_NEAREST, PSB_H_PER_SAMPLE, PSB_H_CONSTANT = 0, 1, 2
 PSB_FLAG_DEVICE_PTRS = 1
 PSB_FLAG_FP32C_DECISIONS = 0x100
 PSB_FLAG_SINGLE_KERNEL = 0x200
+PSB_FLAG_LUT1000_F32 = 0x400
 PSB_NOALLOC_MAX_SAMPLES = 262144
 
 

@@ -51,3 +51,14 @@ def test_struct_layouts_match_python_binding():
     assert r.returncode == 0, r.stderr
     a, b = map(int, subprocess.run([exe], capture_output=True, text=True).stdout.split())
     assert a == C.sizeof(L.Stats) and b == C.sizeof(L.Catalog)
+
+
+def test_flag_constants_match_header():
+    import re
+    with open(L.HEADER_PATH) as f:
+        hdr = f.read()
+    names = re.findall(r"#define\s+(PSB_FLAG_\w+)\s", hdr)
+    assert len(names) >= 4
+    for name in names:
+        m = re.search(r"#define\s+%s\s+(0x[0-9a-fA-F]+|\d+)u" % name, hdr)
+        assert m and int(m.group(1), 0) == getattr(L, name), name

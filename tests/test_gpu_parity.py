@@ -349,3 +349,34 @@ def test_error_paths():
     with pytest.raises(L.PsbError) as e:
         ctx.interp_points(x, x, x, CatalogC(scalars=[99]))
     assert e.value.code == L.PSB_EINVAL
+
+
+def test_short_float_line_table():
+    """PSB_FLAG_LUT1000_F32: line integrals from the 1000-entry float table
+    stay within its interpolation error of the 4096-entry table (spacing
+    2/999: |error| <= dq^2/8 max|I''|, about 1e-6 of I(0)) for the plain
+    column sum.  A Shepard ratio divides by the weight sum: on lines that only
+    graze supports (q near 2, where I -> 0 and the linear interpolation's
+    relative error is largest) its error grows to some 1e-5 of the field's
+    max, so it gets a looser bound.  Point samples are unaffected."""
+    arrs, cols = make_particles(30_000, 91)
+    _, ctx, _, _ = pair(arrs, cols)
+    rng = np.random.default_rng(92)
+    nl = 3000
+    o = tuple(rng.uniform(-0.2, 1.2, nl) for _ in range(3))
+    d = rng.standard_normal((3, nl))
+    d = tuple(d / np.linalg.norm(d, axis=0))
+    cat = CatalogC(scalars=[0, 1], shepard=[0, 1])
+    ref = ctx.interp_lines(o, d, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP64)
+    s = tuple(rng.random(2000) for _ in range(3))
+    pcat = CatalogC(**CATALOGS["all"])
+    p0 = ctx.interp_points(*s, pcat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
+    ctx.extra_flags = L.PSB_FLAG_LUT1000_F32
+    for prec in (L.PSB_PREC_FP64, L.PSB_PREC_FP32C):
+        g = ctx.interp_lines(o, d, cat, strategy=L.PSB_SCATTER, prec=prec)
+        for k, tol in ((0, 1e-5), (1, 2e-4)):
+            e = rel_err(g[k], ref[k])
+            assert 0 < e <= tol, (prec, k, e)
+    p1 = ctx.interp_points(*s, pcat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
+    for a, b in zip(p0, p1):
+        assert np.array_equal(a, b, equal_nan=True)

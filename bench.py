@@ -244,7 +244,7 @@ def lines_and_adjoint(steps, warmup):
     return res
 
 
-def large_leg(steps, warmup, oracle_check=True):
+def large_leg(steps, warmup, oracle_check=True, n=64_000_000, ng=256):
     """The large mixed configuration: 64M float32 particles (70% exponential
     disc, 30% Plummer halo; h and rho from the density sum), rho, Shepard z^2,
     grad rho and curl v on a 256^3 grid over [-1,1]^3 plus four randomly
@@ -257,7 +257,7 @@ def large_leg(steps, warmup, oracle_check=True):
     from partia_b200 import _lib as L, workloads as W, linrange
     from partia_b200.engine import CatalogC, Context
     stream = torch.cuda.Stream()
-    d = W.disc_halo_c5()
+    d = W.disc_halo_c5(n)
     h, rho = W.density_h(d)
     cols = [rho, d["vx"], d["vy"], d["vz"], d["z2"]]
     cat = CatalogC(scalars=[0, 4], shepard=[0, 1], grads=[0], curls=[1, 2, 3])
@@ -268,7 +268,7 @@ def large_leg(steps, warmup, oracle_check=True):
         fr.rotate(*rng.uniform(-math.pi, math.pi, 3))
         frames.append(fr.as_array())
     bprm = np.array([-0.5, 0.5, -0.5, 0.5, -0.5, 0.5])
-    ng, nb = 256, 128
+    nb = ng // 2
     ax = linrange(-1.0, 1.0, ng)
     res = {}
     outs = {}
@@ -318,8 +318,8 @@ def large_leg(steps, warmup, oracle_check=True):
     res["float32_storage"]["note"] = ("particle data kept in float32; inclusion tests and nearest-particle h in float "
                                       "arithmetic, as the reference computes with Float32 inputs")
     res["fp32c"]["particles"] = res["fp64"]["particles"] = "the float32 values converted to double on the device"
-    return {"workload": "disc+halo 64M, 256^3 grid + 4 oriented 128^3 boxes, symmetric, nearest h",
-            "N": 64_000_000, "samples": ns, "fp32c": res["fp32c"], "fp64": res["fp64"],
+    return {"workload": f"disc+halo {n / 1e6:g}M, {ng}^3 grid + 4 oriented {nb}^3 boxes, symmetric, nearest h",
+            "N": n, "samples": ns, "fp32c": res["fp32c"], "fp64": res["fp64"],
             "float32_storage": res["float32_storage"],
             "speedup_fp32c_vs_fp64": res["fp64"]["ms"] / res["fp32c"]["ms"],
             "fp32c_rel_err_vs_fp64": errs(outs["fp32c"], outs["fp64"]),
@@ -409,7 +409,7 @@ def large_adjoint(ctx, ax, stream, steps, warmup, a_col, m):
     pairs = int(ctx.last_stats.pairs)
     gA, gm = g["cols"][4], g["m"]
     lhs, rhs = float((gA * a_col).sum()), float((gout[0] * S).sum())
-    return {"output": "Shepard z^2 on the 256^3 grid, L = ||S||_2", "gradients": "dL/dA_b, dL/dm_b, dL/dr_b (FP64)",
+    return {"output": f"Shepard z^2 on the {len(ax)}^3 grid, L = ||S||_2", "gradients": "dL/dA_b, dL/dm_b, dL/dr_b (FP64)",
             "forward_fp32c_ms": t_fwd, "forward_fp64_ms": t_fwd64, "backward_ms": t_bwd,
             "grad_fwd_time_ratio": t_bwd / t_fwd, "grad_fwd_time_ratio_vs_fp64": t_bwd / t_fwd64, "pairs": pairs,
             "linearity_in_A_rel_residual": abs(lhs - rhs) / abs(rhs),
@@ -482,6 +482,10 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-lines", action="store_true", help="skip the line-integrated and adjoint legs")
     ap.add_argument("--no-large", action="store_true", help="skip the 64M-particle leg")
+    ap.add_argument("--large-n", type=int, default=64_000_000,
+                    help="particles of the large leg (64M = the workload; fewer only for profiling captures)")
+    ap.add_argument("--large-grid", type=int, default=256,
+                    help="grid points per axis of the large leg (256 = the workload; boxes take half)")
     args = ap.parse_args()
     NGRID = args.grid
     if args.impl == "reference":
@@ -625,7 +629,7 @@ def main():
         extra = lines_and_adjoint(max(3, args.steps // 4), 2)
     large = None
     if world == 1 and not args.no_large:
-        large = large_leg(3, 1, oracle_check=not args.no_cpu)
+        large = large_leg(3, 1, oracle_check=not args.no_cpu, n=args.large_n, ng=args.large_grid)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

@@ -119,13 +119,18 @@ static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, in
     if (!ent4 || !emask || !cnt || !hab || !ovf) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
     unsigned* ovf_count = (unsigned*)ovf;
     int32_t* ovf_tiles = (int32_t*)(ovf + 256);
+    // The adjoint's cotangent pass (double particles) collects its pair lists
+    // with the FP32C walk: float tests with the exact double test for every
+    // undecided pair give the same pairs in the same order as the double
+    // walk, at about half its cost; the sums stay in double.
+    const int cprec = (sizeof(T) == 8 && A.lam) ? PREC_FP32C : prec;
     for (int64_t t0 = 0; t0 < nt; t0 += B) {
         const int64_t nb = std::min<int64_t>(B, nt - t0);
         PSB_CUDA_TRY(c, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned), s), "memset overflow count");
         A.sp.ent4 = ent4; A.sp.emask = emask; A.sp.cnt = cnt; A.sp.ha = hab;
         A.sp.ovf_tiles = ovf_tiles; A.sp.ovf_count = ovf_count;
         A.sp.tile0 = t0; A.sp.ntiles = nb;
-        PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, false, s), "pair-list kernel launch");
+        PSB_CUDA_TRY(c, launch_split(A, cprec, st, A.rec.kc, false, s), "pair-list kernel launch");
         PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, true, s), "pair-sum kernel launch");
         Args<T> F = A;
         F.tile_list = ovf_tiles;

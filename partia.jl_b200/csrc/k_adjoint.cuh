@@ -51,12 +51,15 @@ struct AdjArgs {
 
 // M4 at delta = x_s - x_b: W, gradW = sigma/h^5 g1(q) delta and the Hessian
 // (xx, yy, zz, xy, xz, yz) = sigma/h^5 (g1 I + g2 q delta delta^T / r^2), with
-// g1 = f'(q)/q and g2 = d g1/dq (kernels/M4_spline.jl:13-36); invh = 1/h.
-// HESS = false leaves H untouched (scalar catalogs need W and gradW only).
+// g1 = f'(q)/q and g2 = d g1/dq (kernels/M4_spline.jl:13-36).  r = |delta|,
+// ir = 1/r (0 at r = 0), h and invh = 1/h: 1/q = h ir, so no pair needs a
+// division.  HESS = false leaves H untouched (scalar catalogs need W and
+// gradW only).
 template <bool HESS = true>
-__device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r, double invh, double& W,
+__device__ __forceinline__ void m4_whess(const double dl[3], double r, double ir, double h, double invh, double& W,
                                          double g[3], double H[6]) {
     const double q = r * invh;
+    const double iq = h * ir;
     const double sig = inv_pi<double>();
     const double ih3 = invh * invh * invh, ih5 = ih3 * invh * invh;
     double f, g1, g2;
@@ -67,8 +70,8 @@ __device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r
     } else if (q < 2.0) {
         const double a = 2.0 - q;
         f = 0.25 * a * a * a;
-        g1 = -0.75 * a * a / q;
-        g2 = 0.75 * a * (q + 2.0) / (q * q);
+        g1 = -0.75 * a * a * iq;
+        g2 = 0.75 * a * (q + 2.0) * (iq * iq);
     } else {
         f = 0.0; g1 = 0.0; g2 = 0.0;
     }
@@ -76,7 +79,7 @@ __device__ __forceinline__ void m4_whess(const double dl[3], double r2, double r
     const double c = sig * ih5 * g1;
     g[0] = c * dl[0]; g[1] = c * dl[1]; g[2] = c * dl[2];
     if (!HESS) return;
-    const double e = (r2 > 0.0) ? sig * ih5 * g2 * q / r2 : 0.0;
+    const double e = sig * ih5 * g2 * q * (ir * ir);  // 0 at r = 0 (ir = 0)
     H[0] = c + e * dl[0] * dl[0]; H[1] = c + e * dl[1] * dl[1]; H[2] = c + e * dl[2] * dl[2];
     H[3] = e * dl[0] * dl[1]; H[4] = e * dl[0] * dl[2]; H[5] = e * dl[1] * dl[2];
 }
@@ -158,20 +161,21 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     unsigned long long n_pairs = 0, n_spans = 0, n_parts = 0, n_leaves = 0;  // work counters (warp-uniform)
     int64_t steps = 0;
 
-    auto pair = [&](int64_t li, double sxv, double syv, double szv, double iha) {
+    auto pair = [&](int64_t li, double sxv, double syv, double szv, double ha, double iha) {
         ++n_pairs;
         const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
         const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
-        const double r = sqrt(r2);
+        const double ir = (r2 > 0.0) ? rsqrt(r2) : 0.0;
+        const double r = r2 * ir;
         double W, g[3], H[6];
         if (ST == ST_GATHER) {
-            m4_whess<!SCAL>(dl, r2, r, iha, W, g, H);
+            m4_whess<!SCAL>(dl, r, ir, ha, iha, W, g, H);
         } else if (ST == ST_SCATTER) {
-            m4_whess<!SCAL>(dl, r2, r, ihb, W, g, H);
+            m4_whess<!SCAL>(dl, r, ir, hb, ihb, W, g, H);
         } else {
             double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
-            m4_whess<!SCAL>(dl, r2, r, iha, Wa, ga3, Ha);
-            m4_whess<!SCAL>(dl, r2, r, ihb, Wb, gb3, Hb);
+            m4_whess<!SCAL>(dl, r, ir, ha, iha, Wa, ga3, Ha);
+            m4_whess<!SCAL>(dl, r, ir, hb, ihb, Wb, gb3, Hb);
             W = 0.5 * (Wa + Wb);
             for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
             if (!SCAL)
@@ -324,7 +328,7 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         }
         for (; acc; acc &= acc - 1) {
             const int jj = __ffs(acc) - 1;
-            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sih[jj]);
+            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj], st.sih[jj]);
         }
     };
     const int32_t start = (sv.root == 0) ? (int32_t)sv.n : sv.root;

@@ -66,14 +66,109 @@ template <class T> static inline T m4_df(T q) {
 }
 
 template <class T> static inline T m4_norm3() { return T(1) / T(3.141592653589793238462643383279502884L); }
-template <class T> static inline T m4_support() { return T(2); }
+
+// ---------------------------------------------------------------------------
+// The other kernel families, as the reference writes them:
+// kernels/M5_spline.jl (support 2.5, 3D norm 0.05/pi), kernels/M6_spline.jl
+// (support 3, 1/(120 pi)), kernels/C2_Wendland.jl (2, 21/(16 pi)),
+// kernels/C4_Wendland.jl (2, 495/(256 pi)), kernels/C6_Wendland.jl
+// (2, 1365/(512 pi)), each with f and f' per piece.  g_kern is the kernel of
+// the current call (orc_set_kernel; calls are made one at a time).
+// ---------------------------------------------------------------------------
+enum { KERN_M4 = 0, KERN_M5 = 1, KERN_M6 = 2, KERN_C2 = 3, KERN_C4 = 4, KERN_C6 = 5, KERN_COUNT = 6 };
+static int g_kern = KERN_M4;
+
+template <class T> static inline T pw2(T x) { return x * x; }
+template <class T> static inline T pw3(T x) { return x * x * x; }
+template <class T> static inline T pw4(T x) { T y = x * x; return y * y; }
+template <class T> static inline T pw5(T x) { T y = x * x; return y * y * x; }
+
+template <class T> static inline T kern_support() {
+    switch (g_kern) {
+    case KERN_M5: return T(2.5);
+    case KERN_M6: return T(3.0);
+    default: return T(2.0);
+    }
+}
+
+template <class T> static inline T kern_norm3() {
+    const T pi = T(3.141592653589793238462643383279502884L);
+    switch (g_kern) {
+    case KERN_M5: return T(0.05) / pi;
+    case KERN_M6: return T(1) / (T(120) * pi);
+    case KERN_C2: return T(21) / (T(16) * pi);
+    case KERN_C4: return T(495) / (T(256) * pi);
+    case KERN_C6: return T(1365) / (T(512) * pi);
+    default: return m4_norm3<T>();
+    }
+}
+
+template <class T> static inline T kern_f(T q) {
+    if (q < T(0)) return std::numeric_limits<T>::quiet_NaN();
+    switch (g_kern) {
+    case KERN_M5:
+        if (q < T(0.5)) return pw4(T(2.5) - q) - T(5) * pw4(T(1.5) - q) + T(10) * pw4(T(0.5) - q);
+        if (q < T(1.5)) return pw4(T(2.5) - q) - T(5) * pw4(T(1.5) - q);
+        if (q < T(2.5)) return pw4(T(2.5) - q);
+        return T(0);
+    case KERN_M6:
+        if (q < T(1)) return pw5(T(3) - q) - T(6) * pw5(T(2) - q) + T(15) * pw5(T(1) - q);
+        if (q < T(2)) return pw5(T(3) - q) - T(6) * pw5(T(2) - q);
+        if (q < T(3)) return pw5(T(3) - q);
+        return T(0);
+    case KERN_C2:
+        if (q < T(2)) return pw4(T(1) - T(0.5) * q) * (T(2) * q + T(1));
+        return T(0);
+    case KERN_C4:
+        if (q < T(2)) { T a = T(1) - T(0.5) * q; return pw3(a) * pw3(a) * ((T(35) / T(12)) * pw2(q) + T(3) * q + T(1)); }
+        return T(0);
+    case KERN_C6:
+        if (q < T(2)) { T a = T(1) - T(0.5) * q; return pw4(a) * pw4(a) * (T(4) * pw3(q) + T(6.25) * pw2(q) + T(4) * q + T(1)); }
+        return T(0);
+    default: return m4_f(q);
+    }
+}
+
+template <class T> static inline T kern_df(T q) {
+    if (q < T(0)) return std::numeric_limits<T>::quiet_NaN();
+    switch (g_kern) {
+    case KERN_M5:
+        if (q < T(0.5)) return T(-4) * pw3(T(2.5) - q) + T(20) * pw3(T(1.5) - q) - T(40) * pw3(T(0.5) - q);
+        if (q < T(1.5)) return T(-4) * pw3(T(2.5) - q) + T(20) * pw3(T(1.5) - q);
+        if (q < T(2.5)) return T(-4) * pw3(T(2.5) - q);
+        return T(0);
+    case KERN_M6:
+        if (q < T(1)) return T(-5) * pw4(T(3) - q) + T(30) * pw4(T(2) - q) - T(75) * pw4(T(1) - q);
+        if (q < T(2)) return T(-5) * pw4(T(3) - q) + T(30) * pw4(T(2) - q);
+        if (q < T(3)) return T(-5) * pw4(T(3) - q);
+        return T(0);
+    case KERN_C2:
+        if (q < T(2)) { T a = T(1) - T(0.5) * q; return pw4(a) * T(2) - pw3(a) * (T(4) * q + T(2)); }
+        return T(0);
+    case KERN_C4:
+        if (q < T(2)) {
+            T a = T(1) - T(0.5) * q;
+            return pw3(a) * pw3(a) * ((T(35) / T(6)) * q + T(3)) -
+                   pw5(a) * ((T(35) / T(4)) * pw2(q) + T(9) * q + T(3));
+        }
+        return T(0);
+    case KERN_C6:
+        if (q < T(2)) {
+            T a = T(1) - T(0.5) * q;
+            return pw4(a) * pw4(a) * (T(12) * pw2(q) + T(12.5) * q + T(4)) -
+                   pw4(a) * pw3(a) * (T(16) * pw3(q) + T(25) * pw2(q) + T(16) * q + T(4));
+        }
+        return T(0);
+    default: return m4_df(q);
+    }
+}
 
 // Smoothed_kernel_function(K, r, h, Val(3)), kernel.jl:141-146
 template <class T> static inline T kernel_W(T r, T h) {
     T invh = T(1) / h;
     T inv_hD = invh * invh * invh;
     T q = r * invh;
-    return inv_hD * (m4_norm3<T>() * m4_f(q));
+    return inv_hD * (kern_norm3<T>() * kern_f(q));
 }
 
 // Smoothed_gradient_kernel_function(K, dx, dy, dz, h), kernel.jl:273-286,360-365
@@ -88,7 +183,7 @@ template <class T> static inline void kernel_gradW(T dx, T dy, T dz, T h, T& gx,
         T r = std::sqrt(r2);
         T invr = T(1) / r;
         T q = r / h;
-        T coeff = m4_df(q) * m4_norm3<T>() * invr;
+        T coeff = kern_df(q) * kern_norm3<T>() * invr;
         wx = dx * coeff; wy = dy * coeff; wz = dz * coeff;
     }
     gx = inv_hDp1 * wx; gy = inv_hDp1 * wy; gz = inv_hDp1 * wz;
@@ -126,36 +221,89 @@ static void gauss_legendre(int n, std::vector<long double>& x, std::vector<long 
     }
 }
 
-static long double m4_f_ld(long double q) {
-    if (q < 1) { long double a = 2 - q, b = 1 - q; return 0.25L * a * a * a - b * b * b; }
-    if (q < 2) { long double a = 2 - q; return 0.25L * a * a * a; }
-    return 0;
+// kernel shape f(q) of kernel kid in long double, and its break points (the
+// last one is the support)
+static long double shape_ld(int kid, long double q) {
+    switch (kid) {
+    case KERN_M5: {
+        long double a = 2.5L - q, b = 1.5L - q, c = 0.5L - q;
+        if (q < 0.5L) return a * a * a * a - 5 * b * b * b * b + 10 * c * c * c * c;
+        if (q < 1.5L) return a * a * a * a - 5 * b * b * b * b;
+        if (q < 2.5L) return a * a * a * a;
+        return 0;
+    }
+    case KERN_M6: {
+        long double a = 3 - q, b = 2 - q, c = 1 - q;
+        if (q < 1) return a * a * a * a * a - 6 * b * b * b * b * b + 15 * c * c * c * c * c;
+        if (q < 2) return a * a * a * a * a - 6 * b * b * b * b * b;
+        if (q < 3) return a * a * a * a * a;
+        return 0;
+    }
+    case KERN_C2: { if (q >= 2) return 0; long double a = 1 - 0.5L * q; return a * a * a * a * (2 * q + 1); }
+    case KERN_C4: {
+        if (q >= 2) return 0;
+        long double a = 1 - 0.5L * q, a2 = a * a;
+        return a2 * a2 * a2 * (35.0L / 12 * q * q + 3 * q + 1);
+    }
+    case KERN_C6: {
+        if (q >= 2) return 0;
+        long double a = 1 - 0.5L * q, a4 = a * a * a * a;
+        return a4 * a4 * (4 * q * q * q + 6.25L * q * q + 4 * q + 1);
+    }
+    default:
+        if (q < 1) { long double a = 2 - q, b = 1 - q; return 0.25L * a * a * a - b * b * b; }
+        if (q < 2) { long double a = 2 - q; return 0.25L * a * a * a; }
+        return 0;
+    }
+}
+static int breaks_ld(int kid, long double* t) {
+    switch (kid) {
+    case KERN_M5: t[0] = 0.5L; t[1] = 1.5L; t[2] = 2.5L; return 3;
+    case KERN_M6: t[0] = 1; t[1] = 2; t[2] = 3; return 3;
+    case KERN_C2: case KERN_C4: case KERN_C6: t[0] = 2; return 1;
+    default: t[0] = 1; t[1] = 2; return 2;
+    }
 }
 
-static void build_m4_line_table(double* Q, double* Inorm) {
+// I(b) = norm3 * 2 * int_0^sqrt(K^2-b^2) f(sqrt(b^2+s^2)) ds on the reference's
+// grid Q_k = (k-1) K/4095, k = 1..4096, by 64-point Gauss-Legendre on each
+// smooth segment (split where sqrt(b^2+s^2) crosses a break point).
+static void build_line_table(int kid, double* Q, double* Inorm) {
     std::vector<long double> gx, gw;
     gauss_legendre(64, gx, gw);
     const long double pi = 3.141592653589793238462643383279502884L;
-    const long double dq = 2.0L / (LUT_N - 1);
+    long double t[3];
+    const int nb = breaks_ld(kid, t);
+    const long double K = t[nb - 1];
+    long double norm;
+    switch (kid) {
+    case KERN_M5: norm = 0.05L / pi; break;
+    case KERN_M6: norm = 1 / (120 * pi); break;
+    case KERN_C2: norm = 21 / (16 * pi); break;
+    case KERN_C4: norm = 495 / (256 * pi); break;
+    case KERN_C6: norm = 1365 / (512 * pi); break;
+    default: norm = 1 / pi;
+    }
+    const double Kd = (double)K;
     for (int k = 0; k < LUT_N; ++k) {
-        long double b = dq * k;
-        Q[k] = (double)(2.0 / 4095.0 * (double)k);
+        long double b = K / (LUT_N - 1) * k;
+        Q[k] = Kd / 4095.0 * (double)k;
         long double tot = 0;
-        if (b < 2) {
-            long double s2 = std::sqrt(4 - b * b);
-            long double segs[3] = {0, 0, s2};
-            int nseg = 1;
-            if (b < 1) { segs[1] = std::sqrt(1 - b * b); nseg = 2; } else { segs[1] = s2; }
-            for (int sgi = 0; sgi < nseg; ++sgi) {
+        if (b < K) {
+            long double segs[4] = {0, 0, 0, 0};
+            int ns = 0;
+            for (int i = 0; i < nb; ++i)
+                if (t[i] > b) segs[++ns] = std::sqrt(t[i] * t[i] - b * b);
+            for (int sgi = 0; sgi < ns; ++sgi) {
                 long double a = segs[sgi], c = segs[sgi + 1];
                 for (int i = 0; i < 64; ++i) {
                     long double s = 0.5L * (c - a) * gx[i] + 0.5L * (c + a);
-                    tot += 0.5L * (c - a) * gw[i] * m4_f_ld(std::sqrt(b * b + s * s));
+                    tot += 0.5L * (c - a) * gw[i] * shape_ld(kid, std::sqrt(b * b + s * s));
                 }
             }
             tot *= 2;
         }
-        Inorm[k] = (double)(tot / pi);
+        Inorm[k] = (double)(tot * norm);
     }
     Q[0] = 0.0;
 }
@@ -163,12 +311,22 @@ static void build_m4_line_table(double* Q, double* Inorm) {
 struct LineTable {
     double Q[LUT_N], I[LUT_N];
     float Qf[LUT_N], If[LUT_N];
-    LineTable() {
-        build_m4_line_table(Q, I);
+    explicit LineTable(int kid) {
+        build_line_table(kid, Q, I);
         for (int k = 0; k < LUT_N; ++k) { Qf[k] = (float)Q[k]; If[k] = (float)I[k]; }
     }
 };
-static const LineTable& line_table() { static LineTable t; return t; }
+template <int KID> static const LineTable& line_table_k() { static LineTable t(KID); return t; }
+static const LineTable& line_table() {
+    switch (g_kern) {
+    case KERN_M5: return line_table_k<KERN_M5>();
+    case KERN_M6: return line_table_k<KERN_M6>();
+    case KERN_C2: return line_table_k<KERN_C2>();
+    case KERN_C4: return line_table_k<KERN_C4>();
+    case KERN_C6: return line_table_k<KERN_C6>();
+    default: return line_table_k<KERN_M4>();
+    }
+}
 
 template <class T> static inline const T* lut_Q();
 template <class T> static inline const T* lut_I();
@@ -197,7 +355,7 @@ template <class T> static inline T lin_lut(T q) {
 template <class T> static inline T line_kernel(T r, T h) {
     T invh = T(1) / h;
     T q = r * invh;
-    T Idl = (q >= m4_support<T>()) ? T(0) : lin_lut(q);
+    T Idl = (q >= kern_support<T>()) ? T(0) : lin_lut(q);
     return invh * Idl;
 }
 
@@ -579,7 +737,7 @@ struct Mix { static inline uint64_t mix64(uint64_t v) {
 
 template <class T>
 static bool interp_point(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T pa[3], T ha, int mode, T* out) {
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
     const int NS = cat.ns, NG = cat.ng, ND = cat.nd, NC = cat.nc;
@@ -678,7 +836,7 @@ static bool interp_point(const Particles<T>& P, const Tree<T>& tr, const Catalog
 // point-line d2 (rounding) is clamped to 0 before sqrt.
 template <class T>
 static bool interp_line(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T o[3], const T dir[3], T ha, int mode, T* out) {
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
     T S1 = 0;
@@ -707,7 +865,7 @@ static bool interp_line(const Particles<T>& P, const Tree<T>& tr, const Catalog&
 // _density_kernel, single_point_interpolation/kernels/scalar_interpolation.jl:1-75
 template <class T>
 static bool density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3], T ha, int mode, T& out) {
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
     T rho = 0;
@@ -781,7 +939,7 @@ template <class T> static inline void hess_mul(const T H[6], const T v[3], T out
 template <class T>
 static bool adjoint_point(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T pa[3], T ha, int mode,
                           const T* gout, T* acc) {
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
     const int nc = (int)P.cols.size();
@@ -892,7 +1050,7 @@ static bool adjoint_point(const Particles<T>& P, const Tree<T>& tr, const Catalo
 template <class T> static inline void line_kernel_d(T r, T h, T& W, T& dW) {
     const T invh = T(1) / h;
     const T q = r * invh;
-    if (q >= m4_support<T>()) { W = T(0); dW = T(0); return; }
+    if (q >= kern_support<T>()) { W = T(0); dW = T(0); return; }
     const T* Q = lut_Q<T>();
     const T* I = lut_I<T>();
     const T dq = Q[1] - Q[0];
@@ -908,7 +1066,7 @@ template <class T> static inline void line_kernel_d(T r, T h, T& W, T& dW) {
 template <class T>
 static bool adjoint_line(const Particles<T>& P, const Tree<T>& tr, const Catalog& cat, const T o[3], const T dir[3],
                          T ha, int mode, const T* gout, T* acc) {
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
     const int nc = (int)P.cols.size();
@@ -999,8 +1157,16 @@ ORC_API int orc_set_threads(int n) {
 
 ORC_API double orc_W(double r, double h) { return kernel_W<double>(r, h); }
 ORC_API float orc_Wf(float r, float h) { return kernel_W<float>(r, h); }
-ORC_API double orc_f(double q) { return m4_f<double>(q); }
-ORC_API double orc_df(double q) { return m4_df<double>(q); }
+ORC_API double orc_f(double q) { return kern_f<double>(q); }
+ORC_API double orc_df(double q) { return kern_df<double>(q); }
+ORC_API double orc_support(void) { return kern_support<double>(); }
+ORC_API double orc_norm3(void) { return kern_norm3<double>(); }
+// The kernel family of the following calls (0 M4, 1 M5, 2 M6, 3 C2, 4 C4, 5 C6).
+ORC_API int orc_set_kernel(int k) {
+    if (k < 0 || k >= KERN_COUNT) return -1;
+    g_kern = k;
+    return 0;
+}
 ORC_API void orc_gradW(double dx, double dy, double dz, double h, double* g) { kernel_gradW<double>(dx, dy, dz, h, g[0], g[1], g[2]); }
 ORC_API double orc_line_kernel(double r, double h) { return line_kernel<double>(r, h); }
 ORC_API float orc_line_kernelf(float r, float h) { return line_kernel<float>(r, h); }
@@ -1195,7 +1361,7 @@ template <class T> static int digest_impl(orc_ctx* c, int kind, int64_t ns, cons
                                           int mode, int64_t* cnt, uint64_t* hsh, T* ha_out) {
     Tree<T>& tr = tree<T>(c);
     std::atomic<int> bad(0);
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t i = 0; i < ns; ++i) {
         T p[3] = {a[0][i], a[1][i], a[2][i]};
@@ -1234,7 +1400,7 @@ ORC_API int orc_neighbor_digest(orc_ctx* c, int kind, int64_t ns, const void* co
 template <class T> static void brute_impl(orc_ctx* c, int kind, int64_t ns, const T* const* a, const T* ha_in,
                                           int mode, int64_t* cnt, uint64_t* hsh) {
     Tree<T>& tr = tree<T>(c);
-    const T K = m4_support<T>();
+    const T K = kern_support<T>();
     #pragma omp parallel for schedule(dynamic, 16)
     for (int64_t i = 0; i < ns; ++i) {
         T p[3] = {a[0][i], a[1][i], a[2][i]};
@@ -1329,6 +1495,7 @@ ORC_API int orc_adjoint_points(orc_ctx* c, int64_t ns, const void* sx, const voi
                                void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
     if (!c->built) return -7;
     if (c->dtype != 0) return -6;
+    if (g_kern != KERN_M4) return -5;  // the adjoint is restated for M4
     Catalog cat = make_cat(nsc, ss, sh, ng, gs, nd, ds, nc, cs);
     const int L = cat.L();
     const double* X = (const double*)sx; const double* Y = (const double*)sy; const double* Z = (const double*)sz;
@@ -1346,6 +1513,7 @@ ORC_API int orc_adjoint_points(orc_ctx* c, int64_t ns, const void* sx, const voi
 ORC_API int orc_adjoint_lines(orc_ctx* c, int64_t nl, const void* const* od, int hmode, const void* hs, int mode,
                               int nsc, const int32_t* ss, const uint8_t* sh, const void* const* gout,
                               void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
+    if (g_kern != KERN_M4) return -5;  // the adjoint is restated for M4
     if (!c->built) return -7;
     if (c->dtype != 0) return -6;
     if (mode != SCATTER && hmode == 0) return -1;

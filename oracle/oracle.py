@@ -17,6 +17,8 @@ _LIB_PATH = os.path.join(_HERE, "_build", "liboracle_partia.so")
 _lib = None
 
 GATHER, SCATTER, SYMMETRIC = 0, 1, 2
+# kernel families (kernel_function/kernels/*.jl), numbered as psb_kernel
+M4, M5, M6, C2, C4, C6 = 0, 1, 2, 3, 4, 5
 H_NEAREST, H_PER_SAMPLE, H_CONSTANT = 0, 1, 2
 
 _vp = C.c_void_p
@@ -48,6 +50,11 @@ def lib():
         for name in ("orc_f", "orc_df"):
             getattr(L, name).argtypes = [C.c_double]
             getattr(L, name).restype = C.c_double
+        for name in ("orc_support", "orc_norm3"):
+            getattr(L, name).argtypes = []
+            getattr(L, name).restype = C.c_double
+        L.orc_set_kernel.argtypes = [C.c_int]
+        L.orc_set_kernel.restype = C.c_int
         L.orc_gradW.argtypes = [C.c_double] * 4 + [_vp]
         L.orc_gradW.restype = None
         L.orc_line_table.argtypes = [_vp, _vp]
@@ -101,29 +108,51 @@ def _ptr_array(arrs):
     return t
 
 
-def W(r, h):
+def set_kernel(kernel: int):
+    """Kernel family of the following oracle calls (M4 ... C6)."""
+    if lib().orc_set_kernel(int(kernel)) != 0:
+        raise ValueError(f"unknown kernel {kernel}")
+
+
+def W(r, h, kernel=M4):
+    set_kernel(kernel)
     return lib().orc_W(float(r), float(h))
 
 
-def f(q):
+def f(q, kernel=M4):
+    set_kernel(kernel)
     return lib().orc_f(float(q))
 
 
-def df(q):
+def df(q, kernel=M4):
+    set_kernel(kernel)
     return lib().orc_df(float(q))
 
 
-def gradW(dx, dy, dz, h):
+def support(kernel=M4):
+    set_kernel(kernel)
+    return lib().orc_support()
+
+
+def norm3(kernel=M4):
+    set_kernel(kernel)
+    return lib().orc_norm3()
+
+
+def gradW(dx, dy, dz, h, kernel=M4):
+    set_kernel(kernel)
     g = np.zeros(3)
     lib().orc_gradW(float(dx), float(dy), float(dz), float(h), g.ctypes.data)
     return g
 
 
-def line_kernel(r, h):
+def line_kernel(r, h, kernel=M4):
+    set_kernel(kernel)
     return lib().orc_line_kernel(float(r), float(h))
 
 
-def line_table():
+def line_table(kernel=M4):
+    set_kernel(kernel)
     Q = np.zeros(4096)
     I = np.zeros(4096)
     lib().orc_line_table(Q.ctypes.data, I.ctypes.data)
@@ -160,7 +189,9 @@ class Catalog:
 class Oracle:
     """One particle set + its LBVH, restated on the CPU."""
 
-    def __init__(self, x, y, z, m, h, rho, cols=(), dtype=np.float64):
+    def __init__(self, x, y, z, m, h, rho, cols=(), dtype=np.float64, kernel=M4):
+        self.kernel = int(kernel)
+        set_kernel(self.kernel)
         self.dtype = np.dtype(dtype)
         cv = lambda a: np.ascontiguousarray(np.asarray(a, dtype=self.dtype))
         self._keep = [cv(a) for a in (x, y, z, m, h, rho)]
@@ -202,6 +233,7 @@ class Oracle:
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         outs = [np.zeros(ns, dtype=self.dtype) for _ in range(cat.L)]
         optr = _ptr_array(outs)
+        set_kernel(self.kernel)
         rc = lib().orc_interp_points(self.ctx, ns, _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy,
                                      len(cat.scalars), _p(cat.scalars), _p(cat.shepard),
                                      len(cat.grads), _p(cat.grads), len(cat.divs) // 3, _p(cat.divs),
@@ -216,6 +248,7 @@ class Oracle:
         cat = Catalog(scalars=scalars, shepard=shepard)
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         outs = [np.zeros(nl, dtype=self.dtype) for _ in range(len(cat.scalars))]
+        set_kernel(self.kernel)
         rc = lib().orc_interp_lines(self.ctx, nl, _ptr_array(arrs), hmode, _p(hsa), strategy,
                                     len(cat.scalars), _p(cat.scalars), _p(cat.shepard), _ptr_array(outs))
         if rc != 0:
@@ -234,6 +267,7 @@ class Oracle:
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         go = [np.ascontiguousarray(g, dtype=np.float64) for g in gout]
         g, cptr = self._grad_bufs()
+        set_kernel(self.kernel)
         rc = lib().orc_adjoint_points(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy,
                                       len(cat.scalars), _p(cat.scalars), _p(cat.shepard),
                                       len(cat.grads), _p(cat.grads), len(cat.divs) // 3, _p(cat.divs),
@@ -249,6 +283,7 @@ class Oracle:
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         go = [np.ascontiguousarray(g, dtype=np.float64) for g in gout]
         g, cptr = self._grad_bufs()
+        set_kernel(self.kernel)
         rc = lib().orc_adjoint_lines(self.ctx, len(arrs[0]), _ptr_array(arrs), hmode, _p(hsa), strategy,
                                      len(cat.scalars), _p(cat.scalars), _p(cat.shepard), _ptr_array(go),
                                      _p(g["m"]), cptr, _p(g["x"]), _p(g["y"]), _p(g["z"]))
@@ -260,6 +295,7 @@ class Oracle:
         sx, sy, sz = self._s(sx), self._s(sy), self._s(sz)
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         out = np.zeros(len(sx), dtype=self.dtype)
+        set_kernel(self.kernel)
         rc = lib().orc_density(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy, _p(out))
         if rc != 0:
             raise RuntimeError(f"oracle density failed ({rc})")
@@ -273,6 +309,7 @@ class Oracle:
         cnt = np.zeros(ns, dtype=np.int64)
         hsh = np.zeros(ns, dtype=np.uint64)
         ha = np.zeros(ns, dtype=self.dtype)
+        set_kernel(self.kernel)
         rc = lib().orc_neighbor_digest(self.ctx, kind, ns, _ptr_array(arrs), hmode, _p(hsa), strategy,
                                        _p(cnt), _p(hsh), _p(ha))
         if rc != 0:
@@ -286,6 +323,7 @@ class Oracle:
         haa = self._s(np.broadcast_to(np.asarray(ha), (ns,)))
         cnt = np.zeros(ns, dtype=np.int64)
         hsh = np.zeros(ns, dtype=np.uint64)
+        set_kernel(self.kernel)
         lib().orc_brute_digest(self.ctx, kind, ns, _ptr_array(arrs), _p(haa), strategy, _p(cnt), _p(hsh))
         return cnt, hsh
 

@@ -11,16 +11,57 @@ import math
 import numpy as np
 
 SIG = 1.0 / math.pi
+K = 2.0
+KERNEL = 0  # 0 M4, 1 M5, 2 M6, 3 C2, 4 C4, 5 C6 (kernel_function/kernels/*.jl)
+_SUPPORT = [2.0, 2.5, 3.0, 2.0, 2.0, 2.0]
+_NORM3 = [1 / math.pi, 0.05 / math.pi, 1 / (120 * math.pi), 21 / (16 * math.pi), 495 / (256 * math.pi),
+          1365 / (512 * math.pi)]
+
+
+def set_kernel(kid):
+    """Kernel family of the evaluators below."""
+    global SIG, K, KERNEL
+    KERNEL, SIG, K = kid, _NORM3[kid], _SUPPORT[kid]
 
 
 def f(q):
     q = np.asarray(q, dtype=float)
+    if KERNEL == 1:
+        a, b, c = 2.5 - q, 1.5 - q, 0.5 - q
+        return np.where(q < 0.5, a ** 4 - 5 * b ** 4 + 10 * c ** 4,
+                        np.where(q < 1.5, a ** 4 - 5 * b ** 4, np.where(q < 2.5, a ** 4, 0.0)))
+    if KERNEL == 2:
+        a, b, c = 3 - q, 2 - q, 1 - q
+        return np.where(q < 1, a ** 5 - 6 * b ** 5 + 15 * c ** 5,
+                        np.where(q < 2, a ** 5 - 6 * b ** 5, np.where(q < 3, a ** 5, 0.0)))
+    if KERNEL >= 3:
+        a = 1 - 0.5 * q
+        poly = {3: 2 * q + 1, 4: 35 / 12 * q ** 2 + 3 * q + 1, 5: 4 * q ** 3 + 6.25 * q ** 2 + 4 * q + 1}[KERNEL]
+        return np.where(q < 2, a ** {3: 4, 4: 6, 5: 8}[KERNEL] * poly, 0.0)
     a, b = 2 - q, 1 - q
     return np.where(q < 1, 0.25 * a ** 3 - b ** 3, np.where(q < 2, 0.25 * a ** 3, 0.0))
 
 
 def df(q):
     q = np.asarray(q, dtype=float)
+    if KERNEL == 1:
+        a, b, c = 2.5 - q, 1.5 - q, 0.5 - q
+        return np.where(q < 0.5, -4 * a ** 3 + 20 * b ** 3 - 40 * c ** 3,
+                        np.where(q < 1.5, -4 * a ** 3 + 20 * b ** 3, np.where(q < 2.5, -4 * a ** 3, 0.0)))
+    if KERNEL == 2:
+        a, b, c = 3 - q, 2 - q, 1 - q
+        return np.where(q < 1, -5 * a ** 4 + 30 * b ** 4 - 75 * c ** 4,
+                        np.where(q < 2, -5 * a ** 4 + 30 * b ** 4, np.where(q < 3, -5 * a ** 4, 0.0)))
+    if KERNEL == 3:
+        a = 1 - 0.5 * q
+        return np.where(q < 2, 2 * a ** 4 - a ** 3 * (4 * q + 2), 0.0)
+    if KERNEL == 4:
+        a = 1 - 0.5 * q
+        return np.where(q < 2, a ** 6 * (35 / 6 * q + 3) - a ** 5 * (35 / 4 * q ** 2 + 9 * q + 3), 0.0)
+    if KERNEL == 5:
+        a = 1 - 0.5 * q
+        return np.where(q < 2, a ** 8 * (12 * q ** 2 + 12.5 * q + 4) -
+                        a ** 7 * (16 * q ** 3 + 25 * q ** 2 + 16 * q + 4), 0.0)
     a, b = 2 - q, 1 - q
     return np.where(q < 1, -0.75 * a ** 2 + 3 * b ** 2, np.where(q < 2, -0.75 * a ** 2, 0.0))
 
@@ -42,11 +83,11 @@ def _neighbours(P, p, ha, strategy):
     d2 = np.sum(d * d, axis=0)
     hb = P["h"]
     if strategy == "gather":
-        rad = 2 * ha * np.ones_like(hb)
+        rad = K * ha * np.ones_like(hb)
     elif strategy == "scatter":
-        rad = 2 * hb
+        rad = K * hb
     else:
-        rad = 2 * np.maximum(ha, hb)
+        rad = K * np.maximum(ha, hb)
     sel = d2 <= rad * rad
     return sel, d[:, sel], np.sqrt(d2[sel]), hb[sel]
 
@@ -113,7 +154,7 @@ def line_quantities(P, cols, o, m_dir, ha, strategy, scalars, shepard, table):
     Dm = np.sum(D * np.asarray(m_dir, float)[:, None], axis=0)
     d2 = np.sum(D * D, axis=0) - Dm * Dm
     hb = P["h"]
-    rad = {"gather": 2 * ha * np.ones_like(hb), "scatter": 2 * hb, "symmetric": 2 * np.maximum(ha, hb)}[strategy]
+    rad = {"gather": K * ha * np.ones_like(hb), "scatter": K * hb, "symmetric": K * np.maximum(ha, hb)}[strategy]
     sel = d2 <= rad * rad
     if not sel.any():
         return [math.nan] * len(scalars)
@@ -126,7 +167,7 @@ def line_quantities(P, cols, o, m_dir, ha, strategy, scalars, shepard, table):
         i = np.clip(np.trunc(idxf).astype(int), 1, len(Q) - 1)
         t = idxf - i
         v = I[i - 1] * (1 - t) + I[i] * t
-        return np.where(q >= 2, 0.0, v) / h
+        return np.where(q >= K, 0.0, v) / h
 
     hbs = hb[sel]
     Wv = {"gather": lambda: lk(dr, ha), "scatter": lambda: lk(dr, hbs),

@@ -1,15 +1,18 @@
-"""Sample the reference's M4 line-integrated table into a small golden fixture.
+"""Sample the reference's line-integrated kernel tables into a small golden fixture.
 
 Reads src/julia/KernelInterpolation/table/line_integrated_kernel_tables.jl of a
-Partia.jl checkout (first argument, default /root/reference) and writes every
-64th entry of _M4_spline_Q and _M4_spline_Inorm (64 + the last entry) to
-m4_line_table_samples.json next to this script.  The full table is not copied.
+Partia.jl checkout (first argument, default /root/reference) and writes, for
+each kernel family, every 64th entry of _<K>_Q and _<K>_Inorm (64 + the last
+entry) and the grid spacing Q[2] - Q[1] to line_table_samples.json next to
+this script.  The full tables are not copied.
 """
 import json
 import os
 import sys
 
 import numpy as np
+
+KERNELS = ["M4_spline", "M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"]
 
 
 def parse_table(root, name):
@@ -23,13 +26,14 @@ def parse_table(root, name):
 
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    Q = parse_table(root, "_M4_spline_Q")
-    I = parse_table(root, "_M4_spline_Inorm")
     idx = list(range(0, 4096, 64)) + [4095]
-    out = {"source": "table/line_integrated_kernel_tables.jl (_M4_spline_Q, _M4_spline_Inorm)",
-           "index0": idx, "Q": [repr(float(Q[k])) for k in idx], "Inorm": [repr(float(I[k])) for k in idx],
-           "dq": repr(float(Q[1] - Q[0]))}
-    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "m4_line_table_samples.json"), "w") as f:
+    out = {"source": "table/line_integrated_kernel_tables.jl (_<K>_Q, _<K>_Inorm)", "index0": idx, "kernels": {}}
+    for k in KERNELS:
+        Q = parse_table(root, f"_{k}_Q")
+        I = parse_table(root, f"_{k}_Inorm")
+        out["kernels"][k] = {"Q": [repr(float(Q[i])) for i in idx], "Inorm": [repr(float(I[i])) for i in idx],
+                             "dq": repr(float(Q[1] - Q[0]))}
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "line_table_samples.json"), "w") as f:
         json.dump(out, f, indent=1)
 
 

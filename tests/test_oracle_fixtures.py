@@ -156,3 +156,43 @@ def test_density_kernel_matches_brute_force():
         p = np.array([s[0][i], s[1][i], s[2][i]])
         sel, d, r, hb = B._neighbours(P, p, ha[i], "gather")
         assert got[i] == pytest.approx(np.sum(P["m"][sel] * B.W(r, ha[i])), rel=1e-12)
+
+
+@pytest.mark.parametrize("kid", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("strategy,name", [(O.GATHER, "gather"), (O.SCATTER, "scatter"), (O.SYMMETRIC, "symmetric")])
+def test_other_kernels_points_vs_brute_force(kid, strategy, name):
+    """M5, M6 and the Wendland kernels (kernels/*.jl): support K h, weights and
+    gradients of each family, every output kind, against brute force."""
+    rng = np.random.default_rng(40 + kid)
+    n = 400
+    P = dict(x=rng.random(n), y=rng.random(n), z=rng.random(n), m=rng.uniform(0.5, 1.5, n) / n,
+             h=0.09 * rng.uniform(0.7, 1.4, n), rho=rng.uniform(0.8, 1.2, n))
+    cols = [rng.uniform(1, 2, n), np.sin(3 * P["x"]) + P["y"], P["y"] - P["z"], P["x"] * P["z"]]
+    orc = O.Oracle(P["x"], P["y"], P["z"], P["m"], P["h"], P["rho"], cols, kernel=kid)
+    s = tuple(rng.uniform(0.1, 0.9, 25) for _ in range(3))
+    spec = dict(scalars=[0, 1], shepard=[1, 0], grads=[0, -1], divs=[(1, 2, 3)], curls=[(1, 2, 3)])
+    cat = O.Catalog(scalars=spec["scalars"], shepard=spec["shepard"], grads=spec["grads"],
+                    divs=[c for t in spec["divs"] for c in t], curls=[c for t in spec["curls"] for c in t])
+    out = orc.interp_points(*s, cat, strategy=strategy, hmode=O.H_NEAREST)
+    B.set_kernel(kid)
+    try:
+        for i in range(25):
+            p = np.array([s[0][i], s[1][i], s[2][i]])
+            ref = B.general(P, cols, p, B.nearest_h(P, p), name, **spec)
+            for a, b in zip([o[i] for o in out], ref):
+                if math.isnan(b):
+                    assert math.isnan(a)
+                else:
+                    assert a == pytest.approx(b, rel=1e-10, abs=1e-10 * max(1.0, abs(b)))
+        # line-integrated scalars with the family's own table
+        o = (rng.uniform(0.1, 0.9, 6), rng.uniform(0.1, 0.9, 6), np.zeros(6))
+        d = (np.zeros(6), np.zeros(6), np.ones(6))
+        lo = orc.interp_lines(o, d, scalars=[0, 1], shepard=[1, 0], strategy=O.SCATTER)
+        table = O.line_table(kid)
+        for i in range(6):
+            ref = B.line_quantities(P, cols, [o[k][i] for k in range(3)], [d[k][i] for k in range(3)], 0.0,
+                                    "scatter", [0, 1], [1, 0], table)
+            assert lo[0][i] == pytest.approx(ref[0], rel=1e-10, abs=1e-12)
+            assert lo[1][i] == pytest.approx(ref[1], rel=1e-10, abs=1e-12)
+    finally:
+        B.set_kernel(0)

@@ -1,9 +1,10 @@
-"""Oracle pins: M4 kernel functions and the line-integrated table.
+"""Oracle pins: the six kernel families and their line-integrated tables.
 
-Restates test/kernel_function_tests.jl:88-205 of the reference (support,
+Restates test/kernel_function_tests.jl:28-205 of the reference (support,
 normalisation, analytic values, compact support, gradient vs finite
-difference, W scaling) and pins the regenerated 4096-entry M4 line-integral
-table against the reference's own table (table/line_integrated_kernel_tables.jl).
+difference, W scaling) for every kernel family, and pins each regenerated
+4096-entry line-integral table against the reference's own table
+(table/line_integrated_kernel_tables.jl).
 """
 import json
 import math
@@ -16,97 +17,142 @@ import oracle as O
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF = "/root/reference"
+NAMES = ["M4_spline", "M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"]
+KIDS = list(range(6))
+SUPPORT = [2.0, 2.5, 3.0, 2.0, 2.0, 2.0]  # test/kernel_function_tests.jl:88-94
+NORM3 = [1 / math.pi, 0.05 / math.pi, 1 / (120 * math.pi), 21 / (16 * math.pi), 495 / (256 * math.pi),
+         1365 / (512 * math.pi)]  # kernels/*.jl KernelFunctionnorm(.., Val(3), ..)
+
+
+def analytic(kid, q):
+    """f(q) of each family (test/kernel_function_tests.jl:36-86)."""
+    if q < 0:
+        return math.nan
+    if q >= SUPPORT[kid]:
+        return 0.0
+    if kid == 0:
+        return 0.25 * (2 - q) ** 3 - (1 - q) ** 3 if q < 1 else 0.25 * (2 - q) ** 3
+    if kid == 1:
+        if q < 0.5:
+            return (2.5 - q) ** 4 - 5 * (1.5 - q) ** 4 + 10 * (0.5 - q) ** 4
+        return (2.5 - q) ** 4 - 5 * (1.5 - q) ** 4 if q < 1.5 else (2.5 - q) ** 4
+    if kid == 2:
+        if q < 1:
+            return (3 - q) ** 5 - 6 * (2 - q) ** 5 + 15 * (1 - q) ** 5
+        return (3 - q) ** 5 - 6 * (2 - q) ** 5 if q < 2 else (3 - q) ** 5
+    if kid == 3:
+        return (1 - 0.5 * q) ** 4 * (2 * q + 1)
+    if kid == 4:
+        return (1 - 0.5 * q) ** 6 * (35 / 12 * q ** 2 + 3 * q + 1)
+    return (1 - 0.5 * q) ** 8 * (4 * q ** 3 + 6.25 * q ** 2 + 4 * q + 1)
 
 
 def analytic_m4(q):
-    # test/kernel_function_tests.jl:36-40
-    if q < 0:
-        return math.nan
-    if q >= 2:
-        return 0.0
-    return 0.25 * (2 - q) ** 3 - (1 - q) ** 3 if q < 1 else 0.25 * (2 - q) ** 3
+    return analytic(0, q)
 
 
+@pytest.mark.parametrize("kid", KIDS)
+def test_support_and_norm(kid):
+    assert O.support(kid) == SUPPORT[kid]
+    assert O.norm3(kid) == pytest.approx(NORM3[kid], rel=1e-15)
+
+
+@pytest.mark.parametrize("kid", KIDS)
 @pytest.mark.parametrize("q", [0.0, 0.3, 0.7, 1.0, 1.3, 1.8])
-def test_analytic_values(q):
-    sigma = 1 / math.pi
+def test_analytic_values(kid, q):
     # W(r=q, h=1) = sigma f(q)
-    assert abs(O.W(q, 1.0) - sigma * analytic_m4(q)) <= 1e-14
-    assert abs(O.f(q) - analytic_m4(q)) <= 1e-14
+    assert abs(O.W(q, 1.0, kid) - NORM3[kid] * analytic(kid, q)) <= 1e-14 * max(1.0, analytic(kid, 0.0))
+    assert abs(O.f(q, kid) - analytic(kid, q)) <= 1e-13 * max(1.0, analytic(kid, 0.0))
 
 
-def test_compact_support_and_nan():
-    assert O.f(2.1) == 0.0 and O.f(12.0) == 0.0
-    assert math.isnan(O.f(-0.1))
-    assert O.W(0.5, 0.2) == 0.0  # q = 2.5
+@pytest.mark.parametrize("kid", KIDS)
+def test_compact_support_and_nan(kid):
+    K = SUPPORT[kid]
+    assert O.f(K + 0.1, kid) == 0.0 and O.f(K + 10.0, kid) == 0.0
+    assert math.isnan(O.f(-0.1, kid))
+    assert O.W(0.3 * (K + 0.5), 0.3, kid) == 0.0
 
 
-def test_gradient_finite_difference():
+@pytest.mark.parametrize("kid", KIDS)
+def test_gradient_finite_difference(kid):
     h, d = 0.1, 1e-6
     ra = np.array([0.5, 0.5, 0.5])
     rb = np.array([0.55, 0.52, 0.48])
-    W0 = O.W(float(np.linalg.norm(ra - rb)), h)
+    W0 = O.W(float(np.linalg.norm(ra - rb)), h, kid)
     rbx = rb + np.array([d, 0, 0])
-    Wdx = O.W(float(np.linalg.norm(ra - rbx)), h)
-    g = O.gradW(*(rb - ra), h)
+    Wdx = O.W(float(np.linalg.norm(ra - rbx)), h, kid)
+    g = O.gradW(*(rb - ra), h, kernel=kid)
     assert g[0] == pytest.approx((Wdx - W0) / d, rel=1e-4)
+    # f' against a central difference of f at points inside each piece
+    for q in np.linspace(0.05, SUPPORT[kid] - 0.05, 23):
+        e = 1e-6
+        assert O.df(q, kid) == pytest.approx((O.f(q + e, kid) - O.f(q - e, kid)) / (2 * e), rel=1e-6, abs=1e-7)
 
 
 def test_gradient_zero_separation():
-    assert np.array_equal(O.gradW(0.0, 0.0, 0.0, 0.1), np.zeros(3))
+    for kid in KIDS:
+        assert np.array_equal(O.gradW(0.0, 0.0, 0.0, 0.1, kernel=kid), np.zeros(3))
 
 
-def test_W_scaling():
+@pytest.mark.parametrize("kid", KIDS)
+def test_W_scaling(kid):
     h, r = 0.15, 0.2
     q = r / h
-    assert abs(O.W(r, h) - (1 / math.pi) * analytic_m4(q) / h ** 3) <= 1e-14
+    assert abs(O.W(r, h, kid) - NORM3[kid] * analytic(kid, q) / h ** 3) <= 1e-13 * NORM3[kid] * analytic(kid, 0.0) / h ** 3
 
 
-def test_kernel_normalisation_integral():
+@pytest.mark.parametrize("kid", KIDS)
+def test_kernel_normalisation_integral(kid):
     # integral of W over space = 1 (radial quadrature)
-    r = np.linspace(0, 2, 200001)
-    w = np.array([O.W(float(x), 1.0) for x in r[::100]])
-    integ = np.trapezoid(4 * np.pi * r[::100] ** 2 * w, r[::100])
-    assert integ == pytest.approx(1.0, abs=1e-6)
+    r = np.linspace(0, SUPPORT[kid], 2001)
+    w = np.array([O.W(float(x), 1.0, kid) for x in r])
+    assert np.trapezoid(4 * np.pi * r ** 2 * w, r) == pytest.approx(1.0, abs=1e-5)
 
 
 def _fixture():
-    with open(os.path.join(HERE, "golden", "m4_line_table_samples.json")) as f:
+    with open(os.path.join(HERE, "golden", "line_table_samples.json")) as f:
         return json.load(f)
 
 
-def test_line_table_against_reference_samples():
+@pytest.mark.parametrize("kid", KIDS)
+def test_line_table_against_reference_samples(kid):
     """Regenerated table vs every 64th entry of the reference table."""
     fx = _fixture()
-    Q, I = O.line_table()
+    ref = fx["kernels"][NAMES[kid]]
+    Q, I = O.line_table(kid)
     idx = np.array(fx["index0"])
-    qref = np.array([float(v) for v in fx["Q"]])
-    iref = np.array([float(v) for v in fx["Inorm"]])
+    qref = np.array([float(v) for v in ref["Q"]])
+    iref = np.array([float(v) for v in ref["Inorm"]])
     # grid spacing used by _lin_lut (dq = Q[2] - Q[1]) is bit-identical
-    assert Q[1] - Q[0] == float(fx["dq"])
+    assert Q[1] - Q[0] == float(ref["dq"])
     assert np.max(np.abs(Q[idx] - qref)) <= 4.5e-16
-    # the reference table carries ~2e-10 quadrature error; ours is exact to ~1e-16
-    assert np.max(np.abs(I[idx] - iref)) <= 2.5e-10 / math.pi
+    # the reference tables carry up to ~1e-10 quadrature error; ours is exact to ~1e-16
+    assert np.max(np.abs(I[idx] - iref)) <= 8e-11
 
 
 @pytest.mark.skipif(not os.path.isdir(REF), reason="reference checkout not present")
-def test_line_table_against_full_reference_table():
+@pytest.mark.parametrize("kid", KIDS)
+def test_line_table_against_full_reference_table(kid):
     import importlib.util
     spec = importlib.util.spec_from_file_location("mk", os.path.join(HERE, "golden", "make_lut_fixture.py"))
     mk = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mk)
-    Qr = mk.parse_table(REF, "_M4_spline_Q")
-    Ir = mk.parse_table(REF, "_M4_spline_Inorm")
-    Q, I = O.line_table()
+    Qr = mk.parse_table(REF, f"_{NAMES[kid]}_Q")
+    Ir = mk.parse_table(REF, f"_{NAMES[kid]}_Inorm")
+    Q, I = O.line_table(kid)
     assert np.max(np.abs(Q - Qr)) <= 4.5e-16
-    assert np.max(np.abs(I - Ir)) <= 2.5e-10 / math.pi
+    assert np.max(np.abs(I - Ir)) <= 8e-11
     assert np.max(np.abs(I - Ir) / np.maximum(np.abs(Ir), 1e-300)) <= 4e-9
 
 
-def test_line_kernel_semantics():
-    # q >= 2 -> 0; value at q = 0 equals the table's first entry / h
-    Q, I = O.line_table()
-    assert O.line_kernel(0.21, 0.1) == 0.0
-    assert O.line_kernel(0.0, 0.5) == pytest.approx(I[0] / 0.5, rel=1e-15)
-    # column integral of M4 through the centre: 2 * int_0^2 f(s) ds / pi = 1.5 / pi
-    assert I[0] == pytest.approx(1.5 / math.pi, rel=1e-14)
+@pytest.mark.parametrize("kid", KIDS)
+def test_line_kernel_semantics(kid):
+    # q >= K -> 0; value at q = 0 equals the table's first entry / h
+    K = SUPPORT[kid]
+    Q, I = O.line_table(kid)
+    assert O.line_kernel(0.1 * K + 1e-3, 0.1, kid) == 0.0
+    assert O.line_kernel(0.0, 0.5, kid) == pytest.approx(I[0] / 0.5, rel=1e-15)
+    # column integral through the centre: sigma * 2 * int_0^K f(s) ds
+    s = np.linspace(0.0, K, 200001)
+    f = np.array([analytic(kid, float(x)) for x in s[::10]])
+    assert I[0] == pytest.approx(NORM3[kid] * 2 * np.trapezoid(f, s[::10]), rel=1e-8)

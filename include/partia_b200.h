@@ -57,9 +57,11 @@ typedef enum {
 
 typedef enum { PSB_F64 = 0, PSB_F32 = 1 } psb_dtype;
 
-/* SPH kernel families of src/julia/KernelInterpolation/kernel_function/kernels/ (one file each).
- * This build evaluates PSB_KERNEL_M4 (M4_spline.jl); the others return
- * PSB_EUNSUPPORTED. */
+/* SPH kernel families of src/julia/KernelInterpolation/kernel_function/kernels/ (one file each):
+ * support K h (KernelFunctionValid: 2, 2.5, 3, 2, 2, 2), the 3D norm and f, f'
+ * of each file, and each family's line-integrated table
+ * (table/line_integrated_kernel_tables.jl).  The adjoint calls evaluate
+ * PSB_KERNEL_M4 only and return PSB_EUNSUPPORTED for the others. */
 typedef enum {
     PSB_KERNEL_M4 = 0,
     PSB_KERNEL_M5 = 1,
@@ -159,7 +161,9 @@ int psb_set_stream(psb_ctx* ctx, void* stream);
  * n particles, coordinates, mass, smoothing length, density and ncol extra
  * columns, all of element type dt.  Pointers are host pointers unless
  * PSB_FLAG_DEVICE_PTRS is set.  The data are copied; the caller's arrays are
- * not modified.  Invalidates any previous LBVH. */
+ * not modified.  Invalidates any previous LBVH.  kernel is the input's
+ * smoothed_kernel (InterpolationInput.jl:49); it sets the support radius of
+ * every later query and the kernel evaluated in the sums. */
 int psb_set_particles(psb_ctx* ctx, int64_t n, psb_dtype dt,
                       const void* x, const void* y, const void* z,
                       const void* m, const void* h, const void* rho,

@@ -74,6 +74,7 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
                 uint32_t flags, psb_stats* stats) {
     if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before the adjoint");
     if (c->dt != PSB_F64) return fail(c, PSB_EUNSUPPORTED, "the adjoint needs double particle data");
+    if (c->kern != PSB_KERNEL_M4) return fail(c, PSB_EUNSUPPORTED, "the adjoint evaluates the M4_spline kernel only");
     if (st < 0 || st > 2) return fail(c, PSB_EINVAL, "unknown interpolation strategy");
     if (hmode < 0 || hmode > 2) return fail(c, PSB_EINVAL, "unknown smoothing-length mode");
     const bool line = rq0.line;

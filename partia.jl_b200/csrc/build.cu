@@ -306,7 +306,7 @@ __global__ void k_span_roots(int64_t n, const int32_t* parent, const int32_t* rl
 template <class T>
 __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, const T* h, const T* m, const T* rho,
                               const int32_t* sfirst, float4* leaf4, float* mrho, float* mf, float4* leafK,
-                              float2* spanb) {
+                              float2* spanb, float sig) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     double ax = 0, ay = 0, az = 0;
@@ -327,7 +327,7 @@ __global__ void k_pack_leaves(int64_t n, const T* x, const T* y, const T* z, con
     mf[i] = (float)m[i];
     // kernel-weight factors of the float pair bodies
     const float ih = 1.f / r.w;
-    const float s3 = 0.318309886183790671538f * ih * ih * ih;
+    const float s3 = sig * ih * ih * ih;  // sig = the kernel's 3D norm
     leafK[i] = make_float4(ih, s3, s3 * ih, mr);
     // span bounds: max |offset|_1 and max h, rounded up (non-negative floats
     // order like their bit patterns); spanb starts at zero
@@ -448,7 +448,7 @@ static int build_typed(psb_ctx* c) {
     k_span_roots<<<grid_for(n), BT, 0, s>>>(n, c->parent, c->range_lo, c->range_hi, sfirst);
     k_pack_leaves<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->x, (const T*)c->y, (const T*)c->z, (const T*)c->h,
                                                 (const T*)c->m, (const T*)c->rho, sfirst, c->leaf4, c->mrho, c->mf,
-                                                c->leafK, c->spanb);
+                                                c->leafK, c->spanb, (float)kern_norm3(c->kern));
     if (sizeof(T) == 8 && c->ncol > 0) {
         PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
         for (int k = 0; k < c->ncol; ++k)

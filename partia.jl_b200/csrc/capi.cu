@@ -1,7 +1,9 @@
 // capi.cu -- the extern "C" entry points of libpartia_b200 (include/partia_b200.h).
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
+#include <vector>
 
 #include "psb_host.hpp"
 
@@ -80,17 +82,54 @@ void release_buffers(psb_ctx* c) {
 }
 
 
-// M4 line-integrated kernel table: I(q) = (1/pi) * integral over s of
-// f(sqrt(q^2 + s^2)), f the M4 shape (kernel_function/kernels/M4_spline.jl:13-24),
-// by 64-point Gauss-Legendre quadrature on each smooth piece (split where
-// sqrt(q^2+s^2) crosses 1 and 2), in long double.
-static long double m4_shape_ld(long double q) {
-    if (q < 1) { long double a = 2 - q, b = 1 - q; return 0.25L * a * a * a - b * b * b; }
-    if (q < 2) { long double a = 2 - q; return 0.25L * a * a * a; }
-    return 0;
+// Line-integrated kernel tables: I(q) = sigma * 2 * integral over s in
+// [0, sqrt(K^2 - q^2)] of f(sqrt(q^2 + s^2)), for the kernel family's shape
+// f (kernel_function/kernels/*.jl) and 3D norm sigma, on q_k = K k/(n-1), by
+// 64-point Gauss-Legendre quadrature on each smooth piece (split where
+// sqrt(q^2+s^2) crosses a break point of f), in long double.  The reference
+// tabulates the same integrals at 4096 points over [0, K]
+// (table/line_integrated_kernel_tables.jl).
+static long double shape_ld(int kid, long double q) {
+    switch (kid) {
+    case KERN_M5: {
+        long double a = 2.5L - q, b = 1.5L - q, c = 0.5L - q;
+        if (q < 0.5L) return a * a * a * a - 5 * b * b * b * b + 10 * c * c * c * c;
+        if (q < 1.5L) return a * a * a * a - 5 * b * b * b * b;
+        return q < 2.5L ? a * a * a * a : 0;
+    }
+    case KERN_M6: {
+        long double a = 3 - q, b = 2 - q, c = 1 - q;
+        if (q < 1) return a * a * a * a * a - 6 * b * b * b * b * b + 15 * c * c * c * c * c;
+        if (q < 2) return a * a * a * a * a - 6 * b * b * b * b * b;
+        return q < 3 ? a * a * a * a * a : 0;
+    }
+    case KERN_C2: case KERN_C4: case KERN_C6: {
+        if (q >= 2) return 0;
+        long double a = 1 - 0.5L * q, a2 = a * a;
+        if (kid == KERN_C2) return a2 * a2 * (2 * q + 1);
+        if (kid == KERN_C4) return a2 * a2 * a2 * (35.0L / 12 * q * q + 3 * q + 1);
+        return a2 * a2 * a2 * a2 * (4 * q * q * q + 6.25L * q * q + 4 * q + 1);
+    }
+    default:
+        if (q < 1) { long double a = 2 - q, b = 1 - q; return 0.25L * a * a * a - b * b * b; }
+        if (q < 2) { long double a = 2 - q; return 0.25L * a * a * a; }
+        return 0;
+    }
 }
 
-void m4_line_table(double* I, int n) {
+static long double norm3_ld(int kid) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    switch (kid) {
+    case KERN_M5: return 0.05L / pi;
+    case KERN_M6: return 1 / (120 * pi);
+    case KERN_C2: return 21 / (16 * pi);
+    case KERN_C4: return 495 / (256 * pi);
+    case KERN_C6: return 1365 / (512 * pi);
+    default: return 1 / pi;
+    }
+}
+
+void line_table(int kid, double* I, int n) {
     const int G = 64;
     long double gx[G], gw[G];
     const long double pi = 3.141592653589793238462643383279502884L;
@@ -111,33 +150,67 @@ void m4_line_table(double* I, int n) {
         gx[i] = z;
         gw[i] = 2 / ((1 - z * z) * pp * pp);
     }
+    long double brk[3];
+    int nb = 0;
+    switch (kid) {
+    case KERN_M5: brk[0] = 0.5L; brk[1] = 1.5L; brk[2] = 2.5L; nb = 3; break;
+    case KERN_M6: brk[0] = 1; brk[1] = 2; brk[2] = 3; nb = 3; break;
+    case KERN_C2: case KERN_C4: case KERN_C6: brk[0] = 2; nb = 1; break;
+    default: brk[0] = 1; brk[1] = 2; nb = 2; break;
+    }
+    const long double K = brk[nb - 1], sig = norm3_ld(kid);
     for (int k = 0; k < n; ++k) {
-        long double b = 2.0L / (n - 1) * k, tot = 0;
-        if (b < 2) {
-            long double s2 = std::sqrt(4 - b * b);
-            long double edges[3] = {0, b < 1 ? std::sqrt(1 - b * b) : s2, s2};
-            int nseg = b < 1 ? 2 : 1;
-            for (int g = 0; g < nseg; ++g) {
+        long double b = K / (n - 1) * k, tot = 0;
+        if (b < K) {
+            long double edges[4] = {0, 0, 0, 0};
+            int ne = 0;
+            for (int t = 0; t < nb; ++t)
+                if (brk[t] > b) edges[++ne] = std::sqrt(brk[t] * brk[t] - b * b);
+            for (int g = 0; g < ne; ++g) {
                 long double a = edges[g], e = edges[g + 1];
                 for (int i = 0; i < G; ++i) {
                     long double s = 0.5L * (e - a) * gx[i] + 0.5L * (e + a);
-                    tot += 0.5L * (e - a) * gw[i] * m4_shape_ld(std::sqrt(b * b + s * s));
+                    tot += 0.5L * (e - a) * gw[i] * shape_ld(kid, std::sqrt(b * b + s * s));
                 }
             }
             tot *= 2;
         }
-        I[k] = (double)(tot / pi);
+        I[k] = (double)(tot * sig);
     }
 }
 
-static const double* host_line_table() {
-    static double table[LUT_N];
-    static bool ready = false;
-    if (!ready) {
-        m4_line_table(table, LUT_N);
-        ready = true;
+// the kernel family's tables (4096 double, 1000 double), built once per family
+struct HostTables {
+    double full[LUT_N];
+    double shrt[LUT_SHORT_N];
+};
+static const HostTables& host_line_tables(int kid) {
+    static HostTables t[KERN_COUNT];
+    static bool ready[KERN_COUNT] = {};
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ready[kid]) {
+        line_table(kid, t[kid].full, LUT_N);
+        line_table(kid, t[kid].shrt, LUT_SHORT_N);
+        ready[kid] = true;
     }
-    return table;
+    return t[kid];
+}
+
+// Upload kernel family kid's line tables (double, float and the short float
+// table) to the context, unless they are the ones it holds.
+static cudaError_t load_line_tables(psb_ctx* c, int kid) {
+    if (c->lut_kern == kid) return cudaSuccess;
+    const HostTables& t = host_line_tables(kid);
+    std::vector<float> tf(LUT_N), ts(LUT_SHORT_N);
+    for (int k = 0; k < LUT_N; ++k) tf[k] = (float)t.full[k];
+    for (int k = 0; k < LUT_SHORT_N; ++k) ts[k] = (float)t.shrt[k];
+    cudaStreamSynchronize(c->stream);  // a running line kernel may still read the old tables
+    cudaError_t e = cudaMemcpy(c->lut_d, t.full, sizeof(double) * LUT_N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->lut_f, tf.data(), sizeof(float) * LUT_N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(c->lut_fs, ts.data(), sizeof(float) * LUT_SHORT_N, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) c->lut_kern = kid;
+    return e;
 }
 
 }  // namespace psb
@@ -162,20 +235,7 @@ PSB_API int psb_create(psb_ctx** out, int device) {
     if (e == cudaSuccess) e = cudaMalloc(&c->lut_d, sizeof(double) * LUT_N);
     if (e == cudaSuccess) e = cudaMalloc(&c->lut_f, sizeof(float) * LUT_N);
     if (e == cudaSuccess) e = cudaMalloc(&c->lut_fs, sizeof(float) * LUT_SHORT_N);
-    if (e == cudaSuccess) {
-        const double* t = host_line_table();
-        float tf[LUT_N];
-        for (int k = 0; k < LUT_N; ++k) tf[k] = (float)t[k];
-        e = cudaMemcpy(c->lut_d, t, sizeof(double) * LUT_N, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(c->lut_f, tf, sizeof(float) * LUT_N, cudaMemcpyHostToDevice);
-    }
-    if (e == cudaSuccess) {
-        static double ts[LUT_SHORT_N];
-        m4_line_table(ts, LUT_SHORT_N);
-        float tsf[LUT_SHORT_N];
-        for (int k = 0; k < LUT_SHORT_N; ++k) tsf[k] = (float)ts[k];
-        e = cudaMemcpy(c->lut_fs, tsf, sizeof(float) * LUT_SHORT_N, cudaMemcpyHostToDevice);
-    }
+    if (e == cudaSuccess) e = load_line_tables(c, KERN_M4);
     if (e != cudaSuccess) {
         cudaGetLastError();
         int code = (e == cudaErrorMemoryAllocation) ? PSB_ENOMEM : PSB_ECUDA;
@@ -233,13 +293,14 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
     if (n < 0) return fail(c, PSB_EINVAL, "particle count must be non-negative");
     if (dt != PSB_F64 && dt != PSB_F32) return fail(c, PSB_EINVAL, "unknown dtype");
     if (ncol < 0) return fail(c, PSB_EINVAL, "ncol must be non-negative");
-    if (kernel != PSB_KERNEL_M4) return fail(c, PSB_EUNSUPPORTED, "only the M4_spline kernel is provided by this build");
+    if ((int)kernel < 0 || (int)kernel >= KERN_COUNT) return fail(c, PSB_EINVAL, "unknown kernel");
     if (n > 0 && (!x || !y || !z || !m || !h || !rho)) return fail(c, PSB_EINVAL, "particle arrays must not be NULL");
     if (n > 0 && ncol > 0 && !cols) return fail(c, PSB_EINVAL, "column pointer array must not be NULL");
     for (int k = 0; n > 0 && k < ncol; ++k)
         if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
     cudaSetDevice(c->device);
     reset_tree(c);
+    PSB_CUDA_TRY(c, load_line_tables(c, (int)kernel), "line table upload");
     c->dt = dt;
     c->es = (dt == PSB_F64) ? 8 : 4;
     c->kern = kernel;

@@ -137,6 +137,19 @@ __device__ __forceinline__ void m4_fdf_edge(float q, float r, float num, float h
     df = -0.75f * a * a;
 }
 
+// f, f' of the kernel family: KF = 0 is M4 (its own forms above), KF = 1 any
+// other family, selected by kern (warp-uniform).
+template <int KF, class C> __device__ __forceinline__ void kfdf(int kern, C q, C& f, C& df) {
+    if constexpr (KF == 0) m4_fdf<C>(q, f, df);
+    else kern_fdf<C>(kern, q, f, df);
+}
+// the float pair sums' form: num = K^2 h^2 - d^2 formed in double
+template <int KF> __device__ __forceinline__ void kfdf_edge(int kern, float q, float r, float num, float hf, float Kf,
+                                                            float& f, float& df) {
+    if constexpr (KF == 0) m4_fdf_edge(q, r, num, hf, f, df);
+    else kern_fdf_f32(kern, q, r, num, hf, Kf, f, df);
+}
+
 template <class C> __device__ __forceinline__ C m4_f(C q) {
     C a = C(2) - q, b = C(1) - q;
     C fo = C(0.25) * a * a * a;

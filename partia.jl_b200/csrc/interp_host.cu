@@ -31,6 +31,11 @@ template <class T> TreeView<T> tree_view(psb_ctx* c) {
     v.node_lo = c->node_lo; v.node_hi = c->node_hi; v.leaf4 = c->leaf4;
     v.mrho = c->mrho; v.mf = c->mf; v.leafK = c->leafK; v.spanb = c->spanb;
     v.coord_err = c->coord_err;
+    v.kern = (int)c->kern;
+    v.Kd = kern_support(v.kern);
+    v.Kf = (float)v.Kd;
+    v.sig = kern_norm3(v.kern);
+    v.qedge = kern_qedge(v.kern);
     return v;
 }
 template TreeView<double> tree_view<double>(psb_ctx*);

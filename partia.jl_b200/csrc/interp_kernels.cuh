@@ -153,10 +153,12 @@ template <class T> __device__ __forceinline__ T ex_d2_line_box(const T o[3], con
     return X<T>::mul(dl, dl);
 }
 
-// radius^2 of a leaf or node: gather (K ha)^2, scatter (K hb)^2, symmetric max
-template <int ST, class T> __device__ __forceinline__ T ex_r2(T ra2, T hb) {
+// radius^2 of a leaf or node: gather (K ha)^2, scatter (K hb)^2, symmetric
+// max; K = the kernel's support in units of h (Kvalid * h, then squared:
+// LinearBVHTraversalMacros.jl:189,246)
+template <int ST, class T> __device__ __forceinline__ T ex_r2(T ra2, T hb, T K) {
     if (ST == ST_GATHER) return ra2;
-    T r = X<T>::mul(T(2), hb);
+    T r = X<T>::mul(K, hb);
     T r2 = X<T>::mul(r, r);
     if (ST == ST_SCATTER) return r2;
     return jmax(ra2, r2);
@@ -179,11 +181,11 @@ __device__ __forceinline__ float lb_d2_pbox(const float pf[3], float pem, float4
     return (tx * tx + ty * ty + tz * tz) * (1.f - RELM);
 }
 
-// upper bound of the node radius^2 (node scale is rounded up)
-template <int ST> __device__ __forceinline__ float hi_r2_node(float ra2_hi, float scale_up) {
+// upper bound of the node radius^2 (node scale is rounded up; K = support)
+template <int ST> __device__ __forceinline__ float hi_r2_node(float ra2_hi, float scale_up, float Kf) {
     if (ST == ST_GATHER) return ra2_hi;
-    float r = 2.f * scale_up;
-    float r2 = r * r * (1.f + RELM);
+    float r = Kf * scale_up;
+    float r2 = r * r * (1.f + 2.f * RELM);
     if (ST == ST_SCATTER) return r2;
     return fmaxf(ra2_hi, r2);
 }
@@ -220,10 +222,10 @@ __device__ __forceinline__ float lb_d2_line_box(const float o[3], const float m[
 // ---------------------------------------------------------------------------
 // _lin_lut, kernel_function/line_integrated_kernel.jl:13-19, with the
 // q >= q_max cut (:90-94) and the 1/h factor (:132-137).
-// n = entries of the table, dq its spacing.
-template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq, int n) {
+// n = entries of the table, dq its spacing, K the kernel's support.
+template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq, int n, C K) {
     C q = r * invh;
-    if (q >= C(2)) return C(0);
+    if (q >= K) return C(0);
     C idxf = q / dq + C(1);
     int i = (int)idxf;  // q >= 0
     i = i < 1 ? 1 : (i > n - 1 ? n - 1 : i);
@@ -256,8 +258,9 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     for (int i = threadIdx.x; i < nlut; i += blockDim.x)
         lut[i] = short_lut ? (CT)A.lut_fs[i] : ((PREC == PREC_FP64) ? (CT)A.lut_d[i] : (CT)A.lut_f[i]);
     __syncthreads();
-    // dq = Q[2] - Q[1] of the n-point table over [0, 2] = 2/(n-1) rounded to CT
-    const CT dq = (CT)(2.0 / (double)(nlut - 1));
+    // dq = Q[2] - Q[1] of the n-point table over [0, K] = K/(n-1) rounded to CT
+    const CT dq = (CT)(A.tv.Kd / (double)(nlut - 1));
+    const CT Kc = (CT)A.tv.Kd;
 
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
@@ -282,7 +285,8 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
 
     T ha = T(0);
     if (ST != ST_SCATTER && valid) ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
-    const T ra = X<T>::mul(T(2), ha);
+    const T Kt = (T)tv.Kd;
+    const T ra = X<T>::mul(Kt, ha);
     const T ra2 = X<T>::mul(ra, ra);
     float ra2_hi = 0.f, ra2_lo = 0.f;
     if (BAND && ST != ST_SCATTER) {
@@ -309,10 +313,10 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         }
         const CT dr = sqrt(s < CT(0) ? CT(0) : s);
         CT W;
-        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut);
+        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut, Kc);
         else {
-            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq, nlut);
-            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut) + Wb);
+            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq, nlut, Kc);
+            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut, Kc) + Wb);
         }
         const CT w = mr * W;
         S1.add(w);
@@ -326,7 +330,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         auto node_fn = [&](int ni) -> bool {
             float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
             float lb = lb_d2_line_box(of, mf3, el, lo, hi);
-            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w, tv.Kf));
         };
         // perpendicular offset of a span's anchor (its first leaf) from the
         // line, in double
@@ -366,11 +370,15 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
                 float ev = 8.f * U1 * (vn + fabsf(L.x) + fabsf(L.y) + fabsf(L.z)) + cerr + 1e-30f;
                 float r = sqrtf(fs);
                 float up = r + ev, dn = fmaxf(r - ev, 0.f);
-                float rb2 = 4.f * L.w * L.w;
+                const float kb = tv.Kf * L.w;
+                float rb2 = kb * kb;
                 float r2lo, r2hi;
                 if (ST == ST_GATHER) { r2lo = ra2_lo; r2hi = ra2_hi; }
-                else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - RELM); r2hi = rb2 * (1.f + RELM); }
-                else { r2lo = fmaxf(ra2_lo, rb2 * (1.f - RELM)); r2hi = fmaxf(ra2_hi, rb2 * (1.f + RELM)); }
+                else if (ST == ST_SCATTER) { r2lo = rb2 * (1.f - 2.f * RELM); r2hi = rb2 * (1.f + 2.f * RELM); }
+                else {
+                    r2lo = fmaxf(ra2_lo, rb2 * (1.f - 2.f * RELM));
+                    r2hi = fmaxf(ra2_hi, rb2 * (1.f + 2.f * RELM));
+                }
                 bool acc;
                 if (up * up * (1.f + RELM) + e64 < r2lo) acc = true;
                 else if (dn * dn * (1.f - RELM) - e64 > r2hi) acc = false;
@@ -378,7 +386,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
                     ++n_retest;
                     const int64_t li = lo + j;
                     T e2 = ex_d2_line<T>(o, m, tv.x[li], tv.y[li], tv.z[li]);
-                    acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li]);
+                    acc = e2 <= ex_r2<ST, T>(ra2, tv.h[li], Kt);
                 }
                 if (!acc) continue;
                 CT cols[KC];
@@ -392,13 +400,13 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
         auto node_fn = [&](int ni) -> bool {
             ++steps;
             T d2n = ex_d2_line_box<T>(o, m, tv, ni);
-            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]), Kt);
             return !(d2n > r2);
         };
         auto leaf_fn = [&](int64_t li) {
             T e2 = ex_d2_line<T>(o, m, __ldg(&tv.x[li]), __ldg(&tv.y[li]), __ldg(&tv.z[li]));
             T hb = __ldg(&tv.h[li]);
-            if (!(e2 <= ex_r2<ST, T>(ra2, hb))) return;
+            if (!(e2 <= ex_r2<ST, T>(ra2, hb, Kt))) return;
             CT cols[KC];
 #pragma unroll
             for (int c = 0; c < KC; ++c) cols[c] = (c < kc) ? (CT)__ldg(&A.colT[c][li]) : CT(0);

@@ -1,4 +1,5 @@
-// k_adjoint.cuh -- adjoint (vector-Jacobian product) kernels.
+// k_adjoint.cuh -- adjoint (vector-Jacobian product) kernels (M4 kernel: its
+// support 2 and Hessian are written out below; the host refuses other kernels).
 //
 // For a loss L = sum_s sum_k gout_k(s) out_k(s) the forward pass in FP64 first
 // writes, per sample, the cotangents lambda of its sums (S1, G, Dm, Dg, Sw_c,
@@ -235,7 +236,7 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     constexpr int SN = (ST == ST_GATHER) ? ST_SCATTER : ((ST == ST_SCATTER) ? ST_GATHER : ST_SYMMETRIC);
     auto node_fn = [&](int ni) -> bool {
         const float4 lo = __ldg(&sv.node_lo[ni]), hi = __ldg(&sv.node_hi[ni]);
-        return !(lb_d2_pbox(pf, pem, lo, hi) > hi_r2_node<SN>(rb2_hi, lo.w));
+        return !(lb_d2_pbox(pf, pem, lo, hi) > hi_r2_node<SN>(rb2_hi, lo.w, 2.f));
     };
     auto span_fn = [&](int64_t lo, int cnt, bool part) {
         const unsigned parts = __ballot_sync(PSB_FULL, part);
@@ -324,7 +325,7 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             const double ra = X<double>::mul(2.0, st.sh[jj]);
             const double ra2 = X<double>::mul(ra, ra);
             const double e2 = ex_d2_pp<double>(ps, xb[0], xb[1], xb[2]);
-            if (e2 <= ex_r2<ST, double>(ra2, hb)) acc |= 1u << jj;
+            if (e2 <= ex_r2<ST, double>(ra2, hb, 2.0)) acc |= 1u << jj;
         }
         for (; acc; acc &= acc - 1) {
             const int jj = __ffs(acc) - 1;
@@ -420,7 +421,7 @@ __global__ void __launch_bounds__(128) k_adj_beam(const AdjArgs A) {
             const double ra = X<double>::mul(2.0, ha);
             const double ra2 = X<double>::mul(ra, ra);
             const double e2 = ex_d2_line<double>(o, m, xb[0], xb[1], xb[2]);
-            if (!(e2 <= ex_r2<ST, double>(ra2, hb))) continue;
+            if (!(e2 <= ex_r2<ST, double>(ra2, hb, 2.0))) continue;
             ++n_pairs;
             const double dr = sqrt(e2 < 0.0 ? 0.0 : e2);
             double W, dW;

@@ -266,7 +266,7 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
     return valid ? ((bidx >= 0) ? tv.h[bidx] : qnan<T>()) : T(0);
 }
 
-template <class T, int PREC, int ST, int KC, int WHAT>
+template <class T, int PREC, int ST, int KC, int WHAT, int KF>
 __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
@@ -357,7 +357,8 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         }
     }
     // radius = Kvalid * ha; radius2 = radius * radius (general_interpolation.jl:20-21)
-    const T ra = X<T>::mul(T(2), ha);
+    const T Kt = (T)tv.Kd;
+    const T ra = X<T>::mul(Kt, ha);
     const T ra2 = X<T>::mul(ra, ra);
     if constexpr (BAND) {
         float ralo = 0.f, rahi = 0.f;
@@ -373,14 +374,16 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     if (BAND && ST != ST_SCATTER) ra2_hi = __double2float_ru((double)ra2) * (1.f + RELM);
 
     // ---- per-sample constants of the kernel weights ----
-    const CT sig = inv_pi<CT>();
+    const CT sig = (KF == 0) ? inv_pi<CT>() : (CT)tv.sig;
     CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
     if (ST != ST_SCATTER) {
         ia = CT(1) / (CT)ha;
         sa3 = sig * ia * ia * ia;
         sa4 = sa3 * ia;
     }
-    const double fa2 = 4.0 * (double)ha * (double)ha;  // (2 ha)^2 for the outer kernel piece
+    const double kha = tv.Kd * (double)ha;
+    const double fa2 = kha * kha;  // (K ha)^2 for the kernel piece at the support edge
+    const float qe = (KF == 0) ? 1.f : tv.qedge;
 
     // ---- accumulators ----
     Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
@@ -413,7 +416,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         CT Wsum = CT(0), csum = CT(0);  // kernel value and gradient coefficient (grad W = c * delta)
         if (ST != ST_SCATTER) {
             CT f, df;
-            m4_fdf<CT>(r * ia, f, df);
+            kfdf<KF, CT>(tv.kern, r * ia, f, df);
             Wsum = sa3 * f;
             csum = sa4 * df * invr;
         }
@@ -421,7 +424,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             CT ib = CT(1) / hb;
             CT sb3 = sig * ib * ib * ib;
             CT f, df;
-            m4_fdf<CT>(r * ib, f, df);
+            kfdf<KF, CT>(tv.kern, r * ib, f, df);
             CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
             if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
             else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }
@@ -469,10 +472,10 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         if constexpr (BAND) {
             float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
             float lb = lb_d2_pbox(pf, pem, lo, hi);
-            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w, tv.Kf));
         } else {
             T d2n = ex_d2_pbox<T>(p, tv, ni);
-            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]), Kt);
             return !(d2n > r2);
         }
     };
@@ -514,21 +517,21 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
             const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
             double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            if (qa >= 1.f || qb >= 1.f) {
+            if (qa >= qe || qb >= qe) {
                 const double ex = (double)p[0] - (double)tv.x[li], ey = (double)p[1] - (double)tv.y[li],
                              ez = (double)p[2] - (double)tv.z[li];
                 d2d = fma(ex, ex, fma(ey, ey, ez * ez));
             }
             if (ST != ST_SCATTER) {
                 float f, df;
-                m4_fdf_edge(qa, r, (float)(fa2 - d2d), (float)ha, f, df);
+                kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
                 Wsum = (float)sa3 * f;
                 csum = (float)sa4 * df;
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                const double hb2 = qb >= 1.f ? 2.0 * (double)tv.h[li] : 0.0;
-                m4_fdf_edge(qb, r, (float)fma(hb2, hb2, -d2d), Lj.w, f, df);
+                const double hbK = qb >= qe ? tv.Kd * (double)tv.h[li] : 0.0;
+                kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), Lj.w, tv.Kf, f, df);
                 if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
                 else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
             }
@@ -574,7 +577,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
                     const int64_t li = st.lo[b] + jj;
                     ++n_retest;
                     T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) add |= 1u << jj;
+                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li], Kt)) add |= 1u << jj;
                 }
                 if (b == 0) acc0 |= add; else if (b == 1) acc1 |= add; else if (b == 2) acc2 |= add; else acc3 |= add;
             }
@@ -636,7 +639,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             float eqm = eq;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) eqm = fmaxf(eqm, __shfl_xor_sync(PSB_FULL, eqm, o));
-            const float rbhi = 2.f * hb * (1.f + 2.f * U1), rblo = 2.f * hb * (1.f - 2.f * U1);
+            const float rbhi = tv.Kf * hb * (1.f + 3.f * U1), rblo = tv.Kf * hb * (1.f - 3.f * U1);
             // the rounding of r itself enters through 4 U1 r (r <= the larger radius)
             float rmax = rahimax;
             if (ST != ST_GATHER) {
@@ -700,7 +703,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             if constexpr (BAND) {
                 const float4 Q = st.Q[j];
                 const float eq = st.eq[j];
-                const float rblo = 2.f * Q.w * (1.f - 2.f * U1), rbhi = 2.f * Q.w * (1.f + 2.f * U1);
+                const float rblo = tv.Kf * Q.w * (1.f - 3.f * U1), rbhi = tv.Kf * Q.w * (1.f + 3.f * U1);
                 for (unsigned pp = parts; pp; pp &= pp - 1) {
                     const int s = __ffs(pp) - 1;
                     const float4 P = st.P[s];
@@ -724,7 +727,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
                     const int64_t li = lo + jj;
                     ++n_retest;
                     T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) acc |= 1u << jj;
+                    if (e2 <= ex_r2<ST, T>(ra2, tv.h[li], Kt)) acc |= 1u << jj;
                 }
                 const float sr0 = st.P[lane].x, sr1 = st.P[lane].y, sr2 = st.P[lane].z;
                 n_bodyit += __reduce_max_sync(PSB_FULL, (unsigned)__popc(acc));
@@ -736,7 +739,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
                 }
             } else {
                 const T xj = st.x[j], yj = st.y[j], zj = st.z[j], hj = st.h[j];
-                const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj);  // (2 hb)^2
+                const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj, Kt);  // (K hb)^2
                 for (unsigned pp = parts; pp; pp &= pp - 1) {
                     const int s = __ffs(pp) - 1;
                     const T ps[3] = {st.px[s], st.py[s], st.pz[s]};

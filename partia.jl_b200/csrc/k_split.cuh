@@ -95,7 +95,8 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
             ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
         }
     }
-    const T ra = X<T>::mul(T(2), ha);
+    const T Kt = (T)tv.Kd;
+    const T ra = X<T>::mul(Kt, ha);
     const T ra2 = X<T>::mul(ra, ra);
     float ra2_hi = 0.f;
     if constexpr (BAND) {
@@ -140,10 +141,10 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
         if constexpr (BAND) {
             float4 lo = __ldg(&tv.node_lo[ni]), hi = __ldg(&tv.node_hi[ni]);
             float lb = lb_d2_pbox(pf, pem, lo, hi);
-            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w));
+            return !(lb > hi_r2_node<ST>(ra2_hi, lo.w, tv.Kf));
         } else {
             T d2n = ex_d2_pbox<T>(p, tv, ni);
-            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]));
+            T r2 = (ST == ST_GATHER) ? ra2 : ex_r2<ST, T>(ra2, __ldg(&tv.nscale[ni]), Kt);
             return !(d2n > r2);
         }
     };
@@ -169,7 +170,7 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
             const float eqm = U1 * (2.f * sb.x + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
             // the rounding of r itself enters through 4 U1 r (r <= the larger radius)
             float rmax = rahimax;
-            if (ST != ST_GATHER) rmax = fmaxf(rmax, 2.f * sb.y * (1.f + 2.f * U1));
+            if (ST != ST_GATHER) rmax = fmaxf(rmax, tv.Kf * sb.y * (1.f + 3.f * U1));
             const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
             // the span's leaves (and their radius thresholds) in shared memory
             __syncwarp();
@@ -177,7 +178,7 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
                 const float4 L = __ldg(&tv.leaf4[lo + lane]);
                 st.Q[lane] = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
                 if (ST != ST_GATHER) {
-                    const float rbhi = 2.f * L.w * (1.f + 2.f * U1), rblo = 2.f * L.w * (1.f - 2.f * U1);
+                    const float rbhi = tv.Kf * L.w * (1.f + 3.f * U1), rblo = tv.Kf * L.w * (1.f - 3.f * U1);
                     const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
                     st.AB[lane] = make_float2(il * il, ih2 * ih2);
                 }
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
                 const int64_t li = lo + jj;
                 ++n_retest;
                 T e2 = ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                if (e2 <= ex_r2<ST, T>(ra2, tv.h[li])) myacc |= 1u << jj;
+                if (e2 <= ex_r2<ST, T>(ra2, tv.h[li], Kt)) myacc |= 1u << jj;
             }
             emit(lo, myacc);
             ++n_spans;
@@ -232,7 +233,7 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
             unsigned acc = 0;
             const int j = lane < cnt ? lane : 0;
             const T xj = st.x[j], yj = st.y[j], zj = st.z[j], hj = st.h[j];
-            const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj);  // (2 hb)^2
+            const T r2b = ex_r2<ST_SCATTER, T>(T(0), hj, Kt);  // (K hb)^2
             for (unsigned pp = parts; pp; pp &= pp - 1) {
                 const int s = __ffs(pp) - 1;
                 const T ps[3] = {st.px[s], st.py[s], st.pz[s]};
@@ -306,7 +307,7 @@ template <class T, int KC> struct PairData<T, true, KC> {
     }
 };
 
-template <class T, int PREC, int ST, int KC>
+template <class T, int PREC, int ST, int KC, int KF>
 __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
@@ -328,14 +329,16 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
     const int kc = A.rec.kc;
     const bool need_dg = A.rec.need_dg != 0;
 
-    const CT sig = inv_pi<CT>();
+    const CT sig = (KF == 0) ? inv_pi<CT>() : (CT)tv.sig;
     CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
     if (ST != ST_SCATTER) {
         ia = CT(1) / (CT)ha;
         sa3 = sig * ia * ia * ia;
         sa4 = sa3 * ia;
     }
-    const double fa2 = 4.0 * (double)ha * (double)ha;  // (2 ha)^2 for the outer kernel piece
+    const double kha = tv.Kd * (double)ha;
+    const double fa2 = kha * kha;  // (K ha)^2 for the kernel piece at the support edge
+    const float qe = (KF == 0) ? 1.f : tv.qedge;
     Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
     CT a0[KC];
     bool have0 = false;
@@ -423,20 +426,20 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
             const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
             const float qb = (ST != ST_GATHER) ? r * cur.K.x : 0.f;
             double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            if (qa >= 1.f || qb >= 1.f) {
+            if (qa >= qe || qb >= qe) {
                 const double ex = (double)p[0] - cur.xd, ey = (double)p[1] - cur.yd, ez = (double)p[2] - cur.zd;
                 d2d = fma(ex, ex, fma(ey, ey, ez * ez));
             }
             if (ST != ST_SCATTER) {
                 float f, df;
-                m4_fdf_edge(qa, r, (float)(fa2 - d2d), (float)ha, f, df);
+                kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
                 Wsum = (float)sa3 * f;
                 csum = (float)sa4 * df;
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                const double hb2 = cur.hd + cur.hd;
-                m4_fdf_edge(qb, r, (float)fma(hb2, hb2, -d2d), cur.L.w, f, df);
+                const double hbK = tv.Kd * cur.hd;
+                kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), cur.L.w, tv.Kf, f, df);
                 if (ST == ST_SCATTER) { Wsum = cur.K.y * f; csum = cur.K.z * df; }
                 else { Wsum = 0.5f * (Wsum + cur.K.y * f); csum = 0.5f * (csum + cur.K.z * df); }
             }
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
             CT Wsum = CT(0), csum = CT(0);
             if (ST != ST_SCATTER) {
                 CT f, df;
-                m4_fdf<CT>(r * ia, f, df);
+                kfdf<KF, CT>(tv.kern, r * ia, f, df);
                 Wsum = sa3 * f;
                 csum = sa4 * df * invr;
             }
@@ -459,7 +462,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
                 CT ib = CT(1) / hb;
                 CT sb3 = sig * ib * ib * ib;
                 CT f, df;
-                m4_fdf<CT>(r * ib, f, df);
+                kfdf<KF, CT>(tv.kern, r * ib, f, df);
                 CT Wb = sb3 * f, cb = sb3 * ib * df * invr;
                 if (ST == ST_SCATTER) { Wsum = Wb; csum = cb; }
                 else { Wsum = CT(0.5) * (Wsum + Wb); csum = CT(0.5) * (csum + cb); }

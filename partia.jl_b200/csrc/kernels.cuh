@@ -1,0 +1,167 @@
+// kernels.cuh -- the SPH kernel families other than M4
+// (kernel_function/kernels/M5_spline.jl, M6_spline.jl, C2_Wendland.jl,
+// C4_Wendland.jl, C6_Wendland.jl): support K in units of h
+// (KernelFunctionValid), the 3D norm (KernelFunctionnorm(K, Val(3), T)) and
+// f, f' of the dimensionless kernel.  Ids follow psb_kernel.  M4 keeps its own
+// functions (m4_fdf, m4_fdf_edge in interp.cuh).
+#pragma once
+
+namespace psb {
+
+enum { KERN_M4 = 0, KERN_M5 = 1, KERN_M6 = 2, KERN_C2 = 3, KERN_C4 = 4, KERN_C6 = 5, KERN_COUNT = 6 };
+
+__host__ __device__ inline double kern_support(int k) {
+    return k == KERN_M5 ? 2.5 : (k == KERN_M6 ? 3.0 : 2.0);
+}
+
+__host__ __device__ inline double kern_norm3(int k) {
+    const double pi = 3.141592653589793;
+    switch (k) {
+    case KERN_M5: return 0.05 / pi;
+    case KERN_M6: return 1.0 / (120.0 * pi);
+    case KERN_C2: return 21.0 / (16.0 * pi);
+    case KERN_C4: return 495.0 / (256.0 * pi);
+    case KERN_C6: return 1365.0 / (512.0 * pi);
+    default: return 0.31830988618379067154;
+    }
+}
+
+// First q of the piece that reaches the support edge: from there on the float
+// pair sums take K - q from K^2 h^2 - d^2 formed in double (see kern_fdf_f32).
+__host__ __device__ inline float kern_qedge(int k) {
+    return k == KERN_M5 ? 1.5f : (k == KERN_M6 ? 2.f : 1.f);
+}
+
+// f and f' for k != M4 at q >= 0, in the reference's piecewise forms; the
+// Wendland derivatives are written in their factored form
+// (C2: f' = -5 q a^3, C4: -14/3 q (1 + 5q/2) a^5, C6: -11/2 q (1 + 7q/2 + 4q^2) a^7,
+// a = 1 - q/2), the same polynomials without the cancellation at small q.
+template <class C> __device__ __forceinline__ void kern_fdf(int k, C q, C& f, C& df) {
+    f = C(0);
+    df = C(0);
+    switch (k) {
+    case KERN_M5: {
+        const C a = C(2.5) - q, b = C(1.5) - q, c = C(0.5) - q;
+        const C a3 = a * a * a, b3 = b * b * b, c3 = c * c * c;
+        if (q < C(0.5)) {
+            f = a3 * a - C(5) * (b3 * b) + C(10) * (c3 * c);
+            df = C(-4) * a3 + C(20) * b3 - C(40) * c3;
+        } else if (q < C(1.5)) {
+            f = a3 * a - C(5) * (b3 * b);
+            df = C(-4) * a3 + C(20) * b3;
+        } else if (q < C(2.5)) {
+            f = a3 * a;
+            df = C(-4) * a3;
+        }
+        break;
+    }
+    case KERN_M6: {
+        const C a = C(3) - q, b = C(2) - q, c = C(1) - q;
+        const C a4 = (a * a) * (a * a), b4 = (b * b) * (b * b), c4 = (c * c) * (c * c);
+        if (q < C(1)) {
+            f = a4 * a - C(6) * (b4 * b) + C(15) * (c4 * c);
+            df = C(-5) * a4 + C(30) * b4 - C(75) * c4;
+        } else if (q < C(2)) {
+            f = a4 * a - C(6) * (b4 * b);
+            df = C(-5) * a4 + C(30) * b4;
+        } else if (q < C(3)) {
+            f = a4 * a;
+            df = C(-5) * a4;
+        }
+        break;
+    }
+    case KERN_C2:
+        if (q < C(2)) {
+            const C a = C(1) - C(0.5) * q, a3 = a * a * a;
+            f = a3 * a * (C(2) * q + C(1));
+            df = C(-5) * q * a3;
+        }
+        break;
+    case KERN_C4:
+        if (q < C(2)) {
+            const C a = C(1) - C(0.5) * q, a2 = a * a, a5 = a2 * a2 * a;
+            f = a5 * a * ((C(35) / C(12)) * (q * q) + C(3) * q + C(1));
+            df = (C(-14) / C(3)) * q * (C(1) + C(2.5) * q) * a5;
+        }
+        break;
+    case KERN_C6:
+        if (q < C(2)) {
+            const C a = C(1) - C(0.5) * q, a2 = a * a, a7 = a2 * a2 * a2 * a;
+            f = a7 * a * (C(4) * (q * q * q) + C(6.25) * (q * q) + C(4) * q + C(1));
+            df = C(-5.5) * q * (C(1) + C(3.5) * q + C(4) * (q * q)) * a7;
+        }
+        break;
+    default:
+        break;
+    }
+}
+
+// f and f' for k != M4 in the float pair sums of double inputs.  The
+// innermost spline pieces are expanded (M5 on q < 1/2: 14.375 - 15 q^2 + 6 q^4,
+// M6 on q < 1: 66 - 60 q^2 + 30 q^4 - 10 q^5), so f' carries its factor q
+// exactly instead of a difference of terms of size ~70.  On the piece that
+// reaches the support edge, K - q is taken as num / (h (K h + r)) with
+// num = K^2 h^2 - d^2 formed in double: from the float q it would carry a
+// few float ulps of absolute error, a relative error that grows without bound
+// towards the edge.  A pair beyond this h's support (accepted for the other h
+// of a symmetric pair) has num < 0 and gets f = f' = 0.
+__device__ __forceinline__ void kern_fdf_f32(int k, float q, float r, float num, float hf, float Kf, float& f,
+                                             float& df) {
+    f = 0.f;
+    df = 0.f;
+    const float u = fmaxf(__fdividef(num, hf * (Kf * hf + r)), 0.f);  // K - q
+    switch (k) {
+    case KERN_M5:
+        if (q < 0.5f) {
+            const float q2 = q * q;
+            f = 14.375f + q2 * (6.f * q2 - 15.f);
+            df = q * (24.f * q2 - 30.f);
+        } else if (q < 1.5f) {
+            const float a = 2.5f - q, b = 1.5f - q, a3 = a * a * a, b3 = b * b * b;
+            f = a3 * a - 5.f * (b3 * b);
+            df = -4.f * a3 + 20.f * b3;
+        } else {
+            const float u3 = u * u * u;
+            f = u3 * u;
+            df = -4.f * u3;
+        }
+        break;
+    case KERN_M6:
+        if (q < 1.f) {
+            const float q2 = q * q;
+            f = 66.f + q2 * (-60.f + q2 * (30.f - 10.f * q));
+            df = q * (-120.f + q2 * (120.f - 50.f * q));
+        } else if (q < 2.f) {
+            const float a = 3.f - q, b = 2.f - q, a4 = (a * a) * (a * a), b4 = (b * b) * (b * b);
+            f = a4 * a - 6.f * (b4 * b);
+            df = -5.f * a4 + 30.f * b4;
+        } else {
+            const float u4 = (u * u) * (u * u);
+            f = u4 * u;
+            df = -5.f * u4;
+        }
+        break;
+    case KERN_C2: case KERN_C4: case KERN_C6: {
+        const float a = (q < 1.f) ? 1.f - 0.5f * q : 0.5f * u;
+        const float a2 = a * a;
+        if (k == KERN_C2) {
+            const float a3 = a2 * a;
+            f = a3 * a * (2.f * q + 1.f);
+            df = -5.f * q * a3;
+        } else if (k == KERN_C4) {
+            const float a5 = a2 * a2 * a;
+            f = a5 * a * ((35.f / 12.f) * (q * q) + 3.f * q + 1.f);
+            df = (-14.f / 3.f) * q * (1.f + 2.5f * q) * a5;
+        } else {
+            const float a7 = a2 * a2 * a2 * a;
+            f = a7 * a * (4.f * (q * q * q) + 6.25f * (q * q) + 4.f * q + 1.f);
+            df = -5.5f * q * (1.f + 3.5f * q + 4.f * (q * q)) * a7;
+        }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+}  // namespace psb

@@ -6,16 +6,23 @@
 
 namespace psb {
 
+// KF: 0 = the M4 kernel's own code, 1 = the other kernel families (digests
+// evaluate no kernel)
+template <class T, int P, int S, int W, int KF>
+static void dispatch_points_kf(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
+    if constexpr (W != WHAT_INTERP) {
+        k_points<T, P, S, 1, W, KF><<<g, 128, 0, s>>>(a);
+    } else {
+        if (kc <= 1) k_points<T, P, S, 1, W, KF><<<g, 128, 0, s>>>(a);
+        else if (kc <= 2) k_points<T, P, S, 2, W, KF><<<g, 128, 0, s>>>(a);
+        else if (kc <= 4) k_points<T, P, S, 4, W, KF><<<g, 128, 0, s>>>(a);
+        else k_points<T, P, S, 8, W, KF><<<g, 128, 0, s>>>(a);
+    }
+}
 template <class T, int P, int S, int W>
 static void dispatch_points_k(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
-    if constexpr (W != WHAT_INTERP) {
-        k_points<T, P, S, 1, W><<<g, 128, 0, s>>>(a);
-    } else {
-        if (kc <= 1) k_points<T, P, S, 1, W><<<g, 128, 0, s>>>(a);
-        else if (kc <= 2) k_points<T, P, S, 2, W><<<g, 128, 0, s>>>(a);
-        else if (kc <= 4) k_points<T, P, S, 4, W><<<g, 128, 0, s>>>(a);
-        else k_points<T, P, S, 8, W><<<g, 128, 0, s>>>(a);
-    }
+    if (W == WHAT_DIGEST || a.tv.kern == KERN_M4) dispatch_points_kf<T, P, S, W, 0>(a, kc, g, s);
+    else if constexpr (W != WHAT_DIGEST) dispatch_points_kf<T, P, S, W, 1>(a, kc, g, s);
 }
 
 template <class T, int P, int W>
@@ -64,12 +71,17 @@ static cudaError_t dispatch_lines_p(const Args<T>& a, int st, int kc, int what, 
 
 // two-kernel point path: k_collect (bodies = false) or k_bodies (bodies = true)
 // over the batch a.sp
+template <class T, int P, int S, int KF>
+static void dispatch_bodies_kf(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
+    if (kc <= 1) k_bodies<T, P, S, 1, KF><<<g, 128, 0, s>>>(a);
+    else if (kc <= 2) k_bodies<T, P, S, 2, KF><<<g, 128, 0, s>>>(a);
+    else if (kc <= 4) k_bodies<T, P, S, 4, KF><<<g, 128, 0, s>>>(a);
+    else k_bodies<T, P, S, 8, KF><<<g, 128, 0, s>>>(a);
+}
 template <class T, int P, int S>
 static void dispatch_bodies_k(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
-    if (kc <= 1) k_bodies<T, P, S, 1><<<g, 128, 0, s>>>(a);
-    else if (kc <= 2) k_bodies<T, P, S, 2><<<g, 128, 0, s>>>(a);
-    else if (kc <= 4) k_bodies<T, P, S, 4><<<g, 128, 0, s>>>(a);
-    else k_bodies<T, P, S, 8><<<g, 128, 0, s>>>(a);
+    if (a.tv.kern == KERN_M4) dispatch_bodies_kf<T, P, S, 0>(a, kc, g, s);
+    else dispatch_bodies_kf<T, P, S, 1>(a, kc, g, s);
 }
 
 template <class T, int P>

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "partia_b200.h"
+#include "kernels.cuh"
 
 #define PSB_WARP 32
 #define PSB_FULL 0xffffffffu
@@ -111,6 +112,13 @@ template <class T> struct TreeView {
     // |leaf4.y| + |leaf4.z|, max h), both rounded up (float error bounds)
     const float2* spanb;
     float coord_err;         // bound on |float coordinate - exact| for node tests
+    // kernel family (psb_kernel): support K in units of h (exact in float),
+    // the 3D norm, and the first q of the piece that reaches the support edge
+    int kern;
+    float Kf;
+    double Kd;
+    double sig;
+    float qedge;
 };
 
 // Host-side helpers -----------------------------------------------------------

@@ -49,9 +49,10 @@ struct psb_ctx {
     double bbox[6] = {0, 0, 0, 0, 0, 0};  // particle min x,y,z, max x,y,z
 
     unsigned* d_err = nullptr;  // device error word
-    double* lut_d = nullptr;    // M4 line-integrated table (4096, double)
+    double* lut_d = nullptr;    // line-integrated kernel table of the context's kernel (4096, double)
     float* lut_f = nullptr;     // the same table rounded to float
     float* lut_fs = nullptr;    // a 1000-entry float table of the same integral (PSB_FLAG_LUT1000_F32)
+    int lut_kern = -1;          // kernel family of the tables above
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };

@@ -22,6 +22,6 @@ int run(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, cons
 
 // M4 line-integrated table on the reference grid Q_k = (k-1) 2/4095
 // (table/line_integrated_kernel_tables.jl:1,1029), regenerated by quadrature.
-void m4_line_table(double* I);
+void line_table(int kernel, double* I, int n);
 
 }  // namespace psb

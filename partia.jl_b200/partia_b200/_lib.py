@@ -23,7 +23,7 @@ PSB_EUNSUPPORTED = -6
 PSB_ESTATE = -7
 
 PSB_F64, PSB_F32 = 0, 1
-PSB_KERNEL_M4 = 0
+PSB_KERNEL_M4, PSB_KERNEL_M5, PSB_KERNEL_M6, PSB_KERNEL_C2, PSB_KERNEL_C4, PSB_KERNEL_C6 = 0, 1, 2, 3, 4, 5
 PSB_GATHER, PSB_SCATTER, PSB_SYMMETRIC = 0, 1, 2
 PSB_PREC_FP64, PSB_PREC_FP32C = 0, 1
 PSB_H_NEAREST, PSB_H_PER_SAMPLE, PSB_H_CONSTANT = 0, 1, 2

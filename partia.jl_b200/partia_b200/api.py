@@ -69,31 +69,32 @@ class itpSymmetric(AbstractInterpolationStrategy):
 
 
 class AbstractSPHKernel:
-    supported = False
+    """Kernel families of kernel_function/kernels/*.jl; code = psb_kernel."""
+    code = None
 
 
 class M4_spline(AbstractSPHKernel):
-    supported = True
+    code = L.PSB_KERNEL_M4
 
 
 class M5_spline(AbstractSPHKernel):
-    pass
+    code = L.PSB_KERNEL_M5
 
 
 class M6_spline(AbstractSPHKernel):
-    pass
+    code = L.PSB_KERNEL_M6
 
 
 class C2_Wendland(AbstractSPHKernel):
-    pass
+    code = L.PSB_KERNEL_C2
 
 
 class C4_Wendland(AbstractSPHKernel):
-    pass
+    code = L.PSB_KERNEL_C4
 
 
 class C6_Wendland(AbstractSPHKernel):
-    pass
+    code = L.PSB_KERNEL_C6
 
 
 # ---------------------------------------------------------------------------
@@ -334,12 +335,12 @@ def _context(backend: B200ComputeBackend) -> Context:
 def LinearBVH_(input: InterpolationInput, backend: B200ComputeBackend | None = None) -> LinearBVH:
     """LinearBVH!(input): build on the device and permute input in place."""
     backend = backend or B200ComputeBackend()
-    if not input.smoothed_kernel.supported:
-        raise ArgumentError(f"{input.smoothed_kernel.__name__} is not provided by the B200 backend (use M4_spline)")
+    if getattr(input.smoothed_kernel, "code", None) is None:
+        raise ArgumentError(f"{input.smoothed_kernel!r} is not a kernel family of this backend")
     if input.Npart < 1:
         raise ArgumentError("BinaryRadixTree: enc.codes must be non-empty (got n=0).")
     ctx = Context(backend.device)
-    ctx.set_particles(*input.coord, input.m, input.h, input.rho, input.quant)
+    ctx.set_particles(*input.coord, input.m, input.h, input.rho, input.quant, kernel=input.smoothed_kernel.code)
     perm, _ = ctx.build()
     for a in (*input.coord, input.m, input.h, input.rho, *input.quant):
         a[:] = a[perm]

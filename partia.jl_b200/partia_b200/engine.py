@@ -84,7 +84,7 @@ class Context:
         L.check(self.h, rc)
 
     # ---- particles / build ----
-    def set_particles(self, x, y, z, m, h, rho, cols=(), dtype=None):
+    def set_particles(self, x, y, z, m, h, rho, cols=(), dtype=None, kernel=L.PSB_KERNEL_M4):
         dev = _is_dev(x)
         if dtype is None:
             dtype = (np.float64 if str(x.dtype).endswith("float64") else np.float32) if dev else np.asarray(x).dtype
@@ -98,7 +98,7 @@ class Context:
         dt = L.PSB_F64 if self.dtype == np.float64 else L.PSB_F32
         colp = _ptr_array(list(cols))
         self._chk(self.lib.psb_set_particles(self.h, n, dt, _ptr(x), _ptr(y), _ptr(z), _ptr(m), _ptr(h), _ptr(rho),
-                                             len(cols), colp, L.PSB_KERNEL_M4,
+                                             len(cols), colp, int(kernel),
                                              L.PSB_FLAG_DEVICE_PTRS if dev else 0))
         self._keep = None
         self.n = n

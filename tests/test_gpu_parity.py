@@ -380,3 +380,69 @@ def test_short_float_line_table():
     p1 = ctx.interp_points(*s, pcat, strategy=L.PSB_SYMMETRIC, prec=L.PSB_PREC_FP32C)
     for a, b in zip(p0, p1):
         assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("kid", [L.PSB_KERNEL_M5, L.PSB_KERNEL_M6, L.PSB_KERNEL_C2, L.PSB_KERNEL_C4,
+                                 L.PSB_KERNEL_C6])
+@pytest.mark.parametrize("strategy", [L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC])
+def test_kernel_families(kid, strategy):
+    """M5, M6 and the Wendland C2/C4/C6 kernels (kernels/*.jl): neighbour sets
+    with each family's support K h bit-exact in both decision modes, every
+    output kind in FP64 and FP32C against the oracle, the density sum, and the
+    line-integrated sum with the family's own table."""
+    arrs, cols = make_particles(30_000, 90 + kid)
+    orc = O.Oracle(*arrs, cols=cols, kernel=kid)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols, kernel=kid)
+    ctx.build(want_perm=False)
+    rng = np.random.default_rng(100 + kid)
+    ns = 4000
+    s = tuple(rng.uniform(-0.05, 1.05, ns) for _ in range(3))
+    co, ho, _ = orc.digest(s, strategy=strategy, hmode=O.H_NEAREST)
+    for fp32c in (False, True):
+        cg, hg, _ = ctx.digest(s, strategy=strategy, hmode=L.PSB_H_NEAREST, fp32c=fp32c)
+        assert np.array_equal(cg, co) and np.array_equal(hg, ho), fp32c
+    spec = CATALOGS["all"]
+    ref = orc.interp_points(*s, O.Catalog(**spec), strategy=strategy, hmode=O.H_NEAREST)
+    for prec, tol in ((L.PSB_PREC_FP64, FP64_TOL), (L.PSB_PREC_FP32C, FP32C_TOL)):
+        g = ctx.interp_points(*s, CatalogC(**spec), strategy=strategy, hmode=L.PSB_H_NEAREST, prec=prec)
+        for k in range(len(ref)):
+            assert rel_err(g[k], ref[k]) <= tol, (prec, k, rel_err(g[k], ref[k]))
+        assert ctx.last_stats.pairs == int(co.sum())
+    hs = rng.uniform(0.02, 0.05, ns)
+    rd = orc.density(*s, strategy=strategy, hmode=O.H_PER_SAMPLE, hs=hs)
+    gd = ctx.density(*s, strategy=strategy, hmode=L.PSB_H_PER_SAMPLE, hs=hs)
+    assert rel_err(gd, rd) <= FP64_TOL
+    if strategy == L.PSB_SCATTER:
+        nl = 1500
+        o = tuple(rng.uniform(-0.2, 1.2, nl) for _ in range(3))
+        d = rng.standard_normal((3, nl))
+        d = tuple(d / np.linalg.norm(d, axis=0))
+        lref = orc.interp_lines(o, d, [0, 1], shepard=[0, 1], strategy=O.SCATTER)
+        for prec, tol in ((L.PSB_PREC_FP64, FP64_TOL), (L.PSB_PREC_FP32C, FP32C_TOL)):
+            gl = ctx.interp_lines(o, d, CatalogC(scalars=[0, 1], shepard=[0, 1]), strategy=L.PSB_SCATTER, prec=prec)
+            for k in range(2):
+                assert rel_err(gl[k], lref[k]) <= tol, (prec, k, rel_err(gl[k], lref[k]))
+
+
+def test_kernel_family_float_inputs_and_adjoint_refusal():
+    """Float particle data with the M6 kernel (the reference's Float32
+    arithmetic), and the adjoint's refusal of a kernel other than M4."""
+    arrs, cols = make_particles(20_000, 97, np.float32)
+    orc = O.Oracle(*arrs, cols=cols, dtype=np.float32, kernel=L.PSB_KERNEL_M6)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols, dtype=np.float32, kernel=L.PSB_KERNEL_M6)
+    ctx.build(want_perm=False)
+    rng = np.random.default_rng(98)
+    s = tuple(rng.random(3000).astype(np.float32) for _ in range(3))
+    spec = CATALOGS["c2"]
+    ref = orc.interp_points(*s, O.Catalog(**spec), strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+    g = ctx.interp_points(*s, CatalogC(**spec), strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                          prec=L.PSB_PREC_FP64)
+    for k in range(len(ref)):
+        assert rel_err(g[k], ref[k]) <= 2e-4, (k, rel_err(g[k], ref[k]))
+    a64, c64 = make_particles(2000, 99)
+    ctx.set_particles(*a64, cols=c64, kernel=L.PSB_KERNEL_C2)
+    ctx.build(want_perm=False)
+    with pytest.raises(L.PsbError):
+        ctx.adjoint_points(np.array([0.5]), np.array([0.5]), np.array([0.5]), CatalogC(scalars=[0]), [np.ones(1)])

@@ -327,6 +327,44 @@ def large_leg(steps, warmup, oracle_check=True, n=64_000_000, ng=256):
             "oracle_subset": ora, "adjoint": res["adjoint"]}
 
 
+def kernel_families(d, axis, steps, warmup):
+    """The Plummer workload (8 fields, symmetric, nearest h, 128^3 grid) with
+    each kernel family of kernels/*.jl: FP32C and FP64 device time, accepted
+    pairs (the support K h sets the neighbour count) and the largest FP32C vs
+    FP64 field error."""
+    import torch
+    from partia_b200 import _lib as L
+    from partia_b200.engine import CatalogC, Context
+    stream = torch.cuda.Stream()
+    cat = CatalogC(**CATALOG)
+    names = ["M4_spline", "M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"]
+    ns = len(axis) ** 3
+    res = {}
+    for kid, name in enumerate(names):
+        ctx = Context(0)
+        L.load().psb_set_stream(ctx.h, stream.cuda_stream)
+        ctx.set_particles(d["x"], d["y"], d["z"], d["m"], d["h"], d["rho"], [d["rho"], d["Ax"], d["Ay"], d["Az"]],
+                          kernel=kid)
+        ctx.build(want_perm=False)
+        outs = {p: [torch.empty(ns, dtype=torch.float64, device="cuda") for _ in range(L_OUT)]
+                for p in (L.PSB_PREC_FP32C, L.PSB_PREC_FP64)}
+        t = {}
+        for prec in outs:
+            def step(prec=prec):
+                ctx.interp_grid(axis, axis, axis, cat, strategy=L.PSB_SYMMETRIC, prec=prec, out=outs[prec])
+            t[prec] = timed_call(step, stream, steps, warmup)
+        err = 0.0
+        for a, b in zip(outs[L.PSB_PREC_FP32C], outs[L.PSB_PREC_FP64]):
+            fin = torch.isfinite(b)
+            err = max(err, ((a[fin] - b[fin]).abs().max() / b[fin].abs().max()).item())
+        res[name] = {"fp32c_ms": t[L.PSB_PREC_FP32C], "fp64_ms": t[L.PSB_PREC_FP64],
+                     "samples_per_s": ns / (t[L.PSB_PREC_FP32C] / 1e3),
+                     "speedup_fp32c_vs_fp64": t[L.PSB_PREC_FP64] / t[L.PSB_PREC_FP32C],
+                     "pairs": int(ctx.last_stats.pairs), "max_fp32c_rel_err_vs_fp64": err}
+        ctx.close()
+    return res
+
+
 def oracle_subset(d, h, rho, cols, ax, frames, bprm, nb, outs, names, nsub=100_000):
     """The FP64 CPU oracle over all particles (the float32 values in double) on
     a random subset of the grid and box samples; relative error of each GPU
@@ -482,6 +520,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-lines", action="store_true", help="skip the line-integrated and adjoint legs")
     ap.add_argument("--no-large", action="store_true", help="skip the 64M-particle leg")
+    ap.add_argument("--no-kernels", action="store_true", help="skip the kernel-family leg")
     ap.add_argument("--large-n", type=int, default=64_000_000,
                     help="particles of the large leg (64M = the workload; fewer only for profiling captures)")
     ap.add_argument("--large-grid", type=int, default=256,
@@ -627,6 +666,9 @@ def main():
     extra = None
     if world == 1 and not args.no_lines:
         extra = lines_and_adjoint(max(3, args.steps // 4), 2)
+    kern = None
+    if world == 1 and not args.no_kernels:
+        kern = kernel_families(d, axis, max(3, args.steps // 4), 2)
     large = None
     if world == 1 and not args.no_large:
         large = large_leg(3, 1, oracle_check=not args.no_cpu, n=args.large_n, ng=args.large_grid)
@@ -660,6 +702,7 @@ def main():
             "grad_fwd_time_ratio": extra["adjoint"]["grad_fwd_time_ratio"] if extra else None,
             "lines": extra["lines"] if extra else None, "adjoint": extra["adjoint"] if extra else None,
             "large": large,
+            "kernel_families": kern,
             "build_ms": build_ms,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

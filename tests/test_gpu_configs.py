@@ -134,27 +134,32 @@ def test_c3_lines_full_size():
 
 
 def test_c4_adjoint_1m_particles():
+    """Column density plus a Shepard-normalised quantity A (the A-gradient
+    check of the configuration) on a 128^2 beam: dL/dm, dL/dA, dL/dx."""
     d = W.clumps(1_000_000, 3)
     h, rho = W.density_h(d)
-    ctx = make_ctx(d, h, rho, [rho])
-    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], h, rho, [rho])
+    rng = np.random.default_rng(41)
+    A = np.sin(5 * d["x"]) + d["y"] + 0.1 * rng.standard_normal(len(d["x"]))
+    ctx = make_ctx(d, h, rho, [rho, A])
+    orc = O.Oracle(d["x"], d["y"], d["z"], d["m"], h, rho, [rho, A])
     fr = W.c3_frame().as_array()
     prm = np.array([0.0, 1.0, 0.0, 1.0])
     npix = 128
-    rng = np.random.default_rng(41)
-    gout = [rng.standard_normal(npix * npix)]
-    g = ctx.adjoint_beam(fr, prm, npix, npix, CatalogC(scalars=[0], shepard=[0]), gout, strategy=L.PSB_SCATTER)
+    gout = [rng.standard_normal(npix * npix), rng.standard_normal(npix * npix)]
+    g = ctx.adjoint_beam(fr, prm, npix, npix, CatalogC(scalars=[0, 1], shepard=[0, 1]), gout,
+                         strategy=L.PSB_SCATTER)
     ox = W.plane_coordinates(fr, (0.0, 1.0, npix), (0.0, 1.0, npix))
     fw = tuple(np.full(npix * npix, fr[9 + c]) for c in range(3))
     threads = O.set_threads(0)
     O.set_threads(min(threads, 4))  # per-thread gradient buffers of 1M particles
     try:
-        r = orc.adjoint_lines(ox, fw, [0], gout, shepard=[0], strategy=O.SCATTER)
+        r = orc.adjoint_lines(ox, fw, [0, 1], gout, shepard=[0, 1], strategy=O.SCATTER)
     finally:
         O.set_threads(threads)
     for key in ("m", "x", "y", "z"):
         assert rel_err(g[key], r[key]) <= 1e-10, key
-    assert rel_err(g["cols"][0], r["cols"][0]) <= 1e-10
+    for c in range(2):
+        assert rel_err(g["cols"][c], r["cols"][c]) <= 1e-10, c
 
 
 def test_c5_shaped_float_inputs():

@@ -268,6 +268,10 @@ PSB_API int psb_destroy(psb_ctx* c) {
         if (ev) cudaEventDestroy(ev);
     for (auto& cs : c->cstream)
         if (cs) cudaStreamDestroy(cs);
+    for (auto& ev : c->sev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ss : c->sstream)
+        if (ss) cudaStreamDestroy(ss);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
     return PSB_OK;

@@ -108,41 +108,84 @@ static float ms_between(cudaEvent_t a, cudaEvent_t b) {
 // Two-kernel point path over batches of tiles: k_collect writes the pair
 // lists of a batch, k_bodies sums them, and k_points takes the tiles whose
 // lists overflowed.  A batch holds at most SPLIT_BATCH tiles, which bounds the
-// list memory at SPLIT_BATCH * RCAP * 32 * 20 bytes (640 MiB).
+// list memory at SPLIT_BATCH * RCAP * 32 * 20 bytes (640 MiB) per stream.
+//
+// A direct call (multi_stream) of at least two batches' worth of tiles
+// spreads its batches over up to SPLIT_STREAMS streams (the context stream and
+// the context's own), each with its own lists, so that the walks and pair sums
+// of different batches run side by side: the walk is bound by compare and vote
+// issue, the pair sums by load latency, and one kernel alone leaves SMs idle in
+// its tail.  On the 2M-particle 128^3 grid this takes the FP32C step from 7.5
+// to 5.9 ms and the FP64 step from 12.0 to 8.0 ms.
 constexpr int64_t SPLIT_BATCH = 32768;
-
+constexpr int SPLIT_STREAMS = 4;
 template <class T>
-static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, int slot_off = 0) {
+static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, int slot_off = 0,
+                     bool multi_stream = true) {
     cudaStream_t s = c->stream;
     const int64_t nt = A.src.ntiles;
-    const int64_t B = std::min<int64_t>(nt, SPLIT_BATCH);
-    float4* ent4 = (float4*)scratch(c, 16 + slot_off, sizeof(float4) * (size_t)RCAP * 32 * B);
-    uint32_t* emask = (uint32_t*)scratch(c, 20 + slot_off, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
-    uint8_t* cnt = (uint8_t*)scratch(c, 17 + slot_off, (size_t)32 * B);
-    void* hab = scratch(c, 18 + slot_off, sizeof(double) * 32 * (size_t)B);
-    char* ovf = (char*)scratch(c, 19 + slot_off, 256 + sizeof(int32_t) * (size_t)B);
-    if (!ent4 || !emask || !cnt || !hab || !ovf) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
-    unsigned* ovf_count = (unsigned*)ovf;
-    int32_t* ovf_tiles = (int32_t*)(ovf + 256);
+    int nsets = 1;
+    int64_t B = std::min<int64_t>(nt, SPLIT_BATCH);
+    if (multi_stream && nt >= 2 * 4096) {
+        nsets = (int)std::min<int64_t>(SPLIT_STREAMS, (nt + 4095) / 4096);
+        B = std::min<int64_t>(SPLIT_BATCH, (nt + nsets - 1) / nsets);
+    }
+    cudaStream_t ss[SPLIT_STREAMS] = {s, s, s, s};
+    if (nsets > 1) {
+        for (auto& e : c->sev)
+            if (!e) PSB_CUDA_TRY(c, cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        PSB_CUDA_TRY(c, cudaEventRecord(c->sev[0], s), "event");
+        for (int k = 1; k < nsets; ++k) {
+            if (!c->sstream[k - 1])
+                PSB_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->sstream[k - 1], cudaStreamNonBlocking), "stream");
+            ss[k] = c->sstream[k - 1];
+            // the other streams start after everything the call staged on s
+            PSB_CUDA_TRY(c, cudaStreamWaitEvent(ss[k], c->sev[0], 0), "stream wait");
+        }
+    }
+    struct Lists { float4* ent4; uint32_t* emask; uint8_t* cnt; void* hab; unsigned* ovf_count; int32_t* ovf_tiles; };
+    Lists ls[SPLIT_STREAMS];
+    for (int k = 0; k < nsets; ++k) {
+        // scratch slots 16-20 (+ slot_off), 48-52, 37-41 and 42-46 (clear of the
+        // build, sort, sample-order and adjoint slots)
+        static const int set_off[SPLIT_STREAMS] = {0, 32, 21, 26};
+        const int so = slot_off + set_off[k];
+        ls[k].ent4 = (float4*)scratch(c, 16 + so, sizeof(float4) * (size_t)RCAP * 32 * B);
+        ls[k].emask = (uint32_t*)scratch(c, 20 + so, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
+        ls[k].cnt = (uint8_t*)scratch(c, 17 + so, (size_t)32 * B);
+        ls[k].hab = scratch(c, 18 + so, sizeof(double) * 32 * (size_t)B);
+        char* ovf = (char*)scratch(c, 19 + so, 256 + sizeof(int32_t) * (size_t)B);
+        if (!ls[k].ent4 || !ls[k].emask || !ls[k].cnt || !ls[k].hab || !ovf)
+            return fail(c, PSB_ENOMEM, "scratch allocation failed (pair lists)");
+        ls[k].ovf_count = (unsigned*)ovf;
+        ls[k].ovf_tiles = (int32_t*)(ovf + 256);
+    }
     // The adjoint's cotangent pass (double particles) collects its pair lists
     // with the FP32C walk: float tests with the exact double test for every
     // undecided pair give the same pairs in the same order as the double
     // walk, at about half its cost; the sums stay in double.
     const int cprec = (sizeof(T) == 8 && A.lam) ? PREC_FP32C : prec;
-    for (int64_t t0 = 0; t0 < nt; t0 += B) {
+    int64_t bi = 0;
+    for (int64_t t0 = 0; t0 < nt; t0 += B, ++bi) {
+        const int k = (int)(bi % nsets);
+        const cudaStream_t sk = ss[k];
         const int64_t nb = std::min<int64_t>(B, nt - t0);
-        PSB_CUDA_TRY(c, cudaMemsetAsync(ovf_count, 0, sizeof(unsigned), s), "memset overflow count");
-        A.sp.ent4 = ent4; A.sp.emask = emask; A.sp.cnt = cnt; A.sp.ha = hab;
-        A.sp.ovf_tiles = ovf_tiles; A.sp.ovf_count = ovf_count;
+        PSB_CUDA_TRY(c, cudaMemsetAsync(ls[k].ovf_count, 0, sizeof(unsigned), sk), "memset overflow count");
+        A.sp.ent4 = ls[k].ent4; A.sp.emask = ls[k].emask; A.sp.cnt = ls[k].cnt; A.sp.ha = ls[k].hab;
+        A.sp.ovf_tiles = ls[k].ovf_tiles; A.sp.ovf_count = ls[k].ovf_count;
         A.sp.tile0 = t0; A.sp.ntiles = nb;
-        PSB_CUDA_TRY(c, launch_split(A, cprec, st, A.rec.kc, false, s), "pair-list kernel launch");
-        PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, true, s), "pair-sum kernel launch");
+        PSB_CUDA_TRY(c, launch_split(A, cprec, st, A.rec.kc, false, sk), "pair-list kernel launch");
+        PSB_CUDA_TRY(c, launch_split(A, prec, st, A.rec.kc, true, sk), "pair-sum kernel launch");
         Args<T> F = A;
-        F.tile_list = ovf_tiles;
-        F.tile_count = ovf_count;
+        F.tile_list = ls[k].ovf_tiles;
+        F.tile_count = ls[k].ovf_count;
         F.src.ntiles = nb;  // grid of the list pass: at most nb tiles
-        PSB_CUDA_TRY(c, launch_points<T>(F, prec, st, A.rec.kc, WHAT_INTERP, s), "overflow pass launch");
+        PSB_CUDA_TRY(c, launch_points<T>(F, prec, st, A.rec.kc, WHAT_INTERP, sk), "overflow pass launch");
         *launches += 3;
+    }
+    for (int k = 1; k < nsets; ++k) {  // the call's later work on s follows every stream
+        PSB_CUDA_TRY(c, cudaEventRecord(c->sev[k], ss[k]), "event");
+        PSB_CUDA_TRY(c, cudaStreamWaitEvent(s, c->sev[k], 0), "stream wait");
     }
     return PSB_OK;
 }
@@ -462,7 +505,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
         }
         const bool split = !(flags & PSB_FLAG_SINGLE_KERNEL);
         if (split) {
-            rc = run_split(c, A, prec, st, &launches, 32 * b);
+            rc = run_split(c, A, prec, st, &launches, 32 * b, false);  // chunks already overlap
             if (rc) return rc;
         } else {
             PSB_CUDA_TRY(c, launch_points<T>(A, prec, st, A.rec.kc, WHAT_INTERP, sc_), "interpolation kernel launch");

@@ -78,6 +78,9 @@ struct psb_ctx {
     // host-memory path (created on first use)
     cudaStream_t cstream[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t pev[8] = {};
+    // the other streams of the two-kernel point path (batches spread over them)
+    cudaStream_t sstream[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t sev[4] = {};
 };
 
 namespace psb {

@@ -387,11 +387,13 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
 // Point samples in host memory, in chunks of PIPE_CHUNK: chunk k+1 is copied
 // in on one copy stream and chunk k-1 copied out on another while chunk k
 // computes, so a large call costs about max(compute, copies) instead of their
-// sum.  Consecutive chunks compute on two streams with their own scratch, so
-// the tail of one chunk's kernels overlaps the start of the next.  Each chunk
-// is Morton-ordered on its own.  Buffers are double-buffered and guarded by
-// events.  (Copies from pageable memory still work, with less overlap.)
+// sum.  Consecutive chunks compute on PIPE_SETS streams, each with its own
+// input, output and list buffers, so the kernels of several chunks share the
+// GPU and a chunk waits only for the copy-out of the chunk PIPE_SETS before it.
+// Each chunk is Morton-ordered on its own.  Buffers are guarded by events.
+// (Copies from pageable memory still work, with less overlap.)
 constexpr int64_t PIPE_CHUNK = int64_t(1) << 19;
+constexpr int PIPE_SETS = 4;
 
 template <class T>
 static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st,
@@ -417,20 +419,22 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
     const bool ph = need_h && hmode == PSB_H_PER_SAMPLE;
 
-    for (int q = 0; q < 3; ++q)
-        if (!c->cstream[q]) PSB_CUDA_TRY(c, cudaStreamCreateWithFlags(&c->cstream[q], cudaStreamNonBlocking), "stream");
-    for (int q = 0; q < 8; ++q)
-        if (!c->pev[q]) PSB_CUDA_TRY(c, cudaEventCreateWithFlags(&c->pev[q], cudaEventDisableTiming), "event");
+    for (auto& q : c->cstream)
+        if (!q) PSB_CUDA_TRY(c, cudaStreamCreateWithFlags(&q, cudaStreamNonBlocking), "stream");
+    for (auto& q : c->pev)
+        if (!q) PSB_CUDA_TRY(c, cudaEventCreateWithFlags(&q, cudaEventDisableTiming), "event");
     cudaStream_t sin = c->cstream[0], sout = c->cstream[1];
-    const cudaStream_t cs[2] = {s, c->cstream[2]};
+    const cudaStream_t cs[PIPE_SETS] = {s, c->cstream[2], c->cstream[3], c->cstream[4]};
     // the launch helpers use c->stream: point it at the chunk's compute stream, restore on exit
     struct StreamRestore {
         psb_ctx* c;
         cudaStream_t s;
         ~StreamRestore() { c->stream = s; }
     } restore{c, s};
-    cudaEvent_t in_ready[2] = {c->pev[0], c->pev[1]}, in_free[2] = {c->pev[2], c->pev[3]};
-    cudaEvent_t done[2] = {c->pev[4], c->pev[5]}, out_free[2] = {c->pev[6], c->pev[7]};
+    cudaEvent_t* in_ready = c->pev;  // [PIPE_SETS] each
+    cudaEvent_t* in_free = c->pev + PIPE_SETS;
+    cudaEvent_t* done = c->pev + 2 * PIPE_SETS;
+    cudaEvent_t* out_free = c->pev + 3 * PIPE_SETS;
 
     A.tv = tree_view<T>(c);
     A.hmode = hmode;
@@ -444,13 +448,23 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
     }
     const int nin = 3 + (ph ? 1 : 0);
-    char* inb = (char*)scratch(c, 0, es * CH * nin * 2);
-    char* outb = (char*)scratch(c, 2, es * CH * (L > 0 ? L : 1) * 2);
-    uint64_t* codes[2] = {(uint64_t*)scratch(c, 3, sizeof(uint64_t) * CH), (uint64_t*)scratch(c, 35, sizeof(uint64_t) * CH)};
-    uint32_t* idx[2] = {(uint32_t*)scratch(c, 4, sizeof(uint32_t) * CH), (uint32_t*)scratch(c, 36, sizeof(uint32_t) * CH)};
+    char* inb = (char*)scratch(c, 0, es * CH * nin * PIPE_SETS);
+    char* outb = (char*)scratch(c, 2, es * CH * (L > 0 ? L : 1) * PIPE_SETS);
+    // per set: sample codes and order (slots), the sample sort's scratch
+    // (slot base, 7 slots) and the pair lists (slot offset: slots 16-20 + off)
+    static const int code_slot[PIPE_SETS] = {3, 35, 53, 55};
+    static const int sort_slot[PIPE_SETS] = {6, 38, 64, 72};
+    static const int list_off[PIPE_SETS] = {0, 32, 14, 41};
+    uint64_t* codes[PIPE_SETS];
+    uint32_t* idx[PIPE_SETS];
+    for (int b = 0; b < PIPE_SETS; ++b) {
+        codes[b] = (uint64_t*)scratch(c, code_slot[b], sizeof(uint64_t) * CH);
+        idx[b] = (uint32_t*)scratch(c, code_slot[b] + 1, sizeof(uint32_t) * CH);
+        if (!codes[b] || !idx[b]) return fail(c, PSB_ENOMEM, "scratch allocation failed (chunked samples)");
+    }
     unsigned long long* dstats = (unsigned long long*)scratch(c, 13, 8 * sizeof(unsigned long long));
     T* hconst = (need_h && !ph) ? (T*)scratch(c, 1, es) : nullptr;
-    if (!inb || !outb || !codes[0] || !codes[1] || !idx[0] || !idx[1] || !dstats || (need_h && !ph && !hconst))
+    if (!inb || !outb || !dstats || (need_h && !ph && !hconst))
         return fail(c, PSB_ENOMEM, "scratch allocation failed (chunked samples)");
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[0], s), "event");
     PSB_CUDA_TRY(c, cudaMemsetAsync(dstats, 0, 8 * sizeof(unsigned long long), s), "memset stats");
@@ -460,7 +474,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[1], s), "event");
     PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, c->ev[1], 0), "stream wait");
     PSB_CUDA_TRY(c, cudaStreamWaitEvent(sout, c->ev[1], 0), "stream wait");
-    PSB_CUDA_TRY(c, cudaStreamWaitEvent(cs[1], c->ev[1], 0), "stream wait");
+    for (int b = 1; b < PIPE_SETS; ++b) PSB_CUDA_TRY(c, cudaStreamWaitEvent(cs[b], c->ev[1], 0), "stream wait");
     double sc[3];
     for (int d = 0; d < 3; ++d) {
         double ext = c->bbox[3 + d] - c->bbox[d];
@@ -470,11 +484,11 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     const double3 sc3 = make_double3(sc[0], sc[1], sc[2]);
 
     for (int64_t k = 0; k < nch; ++k) {
-        const int b = (int)(k & 1);
+        const int b = (int)(k % PIPE_SETS);
         const int64_t off = k * CH, cn = std::min<int64_t>(CH, ns - off);
         char* ib = inb + es * CH * nin * b;
         // in
-        if (k >= 2) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, in_free[b], 0), "stream wait");
+        if (k >= PIPE_SETS) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, in_free[b], 0), "stream wait");
         for (int q = 0; q < 3; ++q)
             PSB_CUDA_TRY(c, cudaMemcpyAsync(ib + es * CH * q, (const char*)rq.a[q] + es * off, es * cn,
                                             cudaMemcpyHostToDevice, sin), "sample H2D");
@@ -486,7 +500,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
         const cudaStream_t sc_ = cs[b];
         c->stream = sc_;
         PSB_CUDA_TRY(c, cudaStreamWaitEvent(sc_, in_ready[b], 0), "stream wait");
-        if (k >= 2) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sc_, out_free[b], 0), "stream wait");
+        if (k >= PIPE_SETS) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sc_, out_free[b], 0), "stream wait");
         SampleSrc<T>& S = A.src;
         S.kind = SRC_ARRAYS;
         S.ns = cn;
@@ -500,12 +514,12 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
                                                                           codes[b], idx[b]);
             PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
             ++launches;
-            PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, 6 + 32 * b, &launches, false), "sample sort");
+            PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, sort_slot[b], &launches, false), "sample sort");
             S.order = idx[b];
         }
         const bool split = !(flags & PSB_FLAG_SINGLE_KERNEL);
         if (split) {
-            rc = run_split(c, A, prec, st, &launches, 32 * b, false);  // chunks already overlap
+            rc = run_split(c, A, prec, st, &launches, list_off[b], false);  // chunks already overlap
             if (rc) return rc;
         } else {
             PSB_CUDA_TRY(c, launch_points<T>(A, prec, st, A.rec.kc, WHAT_INTERP, sc_), "interpolation kernel launch");
@@ -522,7 +536,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     }
     // join the copy streams and the second compute stream back into the compute stream
     c->stream = s;
-    PSB_CUDA_TRY(c, cudaStreamWaitEvent(s, out_free[(nch - 1) & 1], 0), "stream wait");
+    PSB_CUDA_TRY(c, cudaStreamWaitEvent(s, out_free[(nch - 1) % PIPE_SETS], 0), "stream wait");
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[4], s), "event");
     unsigned long long hst[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     unsigned herr = 0;

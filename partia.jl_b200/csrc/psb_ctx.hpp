@@ -56,7 +56,7 @@ struct psb_ctx {
 
     // reusable scratch (grown on demand, freed with the context)
     struct Slot { void* p = nullptr; size_t bytes = 0; };
-    Slot scratch[64];
+    Slot scratch[96];
     // sizes of the particle and tree buffers above, keyed by the address of
     // the pointer member: they are kept across set_particles and builds and
     // reallocated only to grow, so repeated builds of the same size (the
@@ -74,10 +74,10 @@ struct psb_ctx {
     struct psb_ctx* sctx = nullptr;  // LBVH over the samples of the last adjoint call
 
     cudaEvent_t ev[8] = {};
-    // copy streams (in, out) and a second compute stream of the chunked
+    // copy streams (in, out) and three more compute streams of the chunked
     // host-memory path (created on first use)
-    cudaStream_t cstream[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t pev[8] = {};
+    cudaStream_t cstream[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t pev[16] = {};
     // the other streams of the two-kernel point path (batches spread over them)
     cudaStream_t sstream[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t sev[4] = {};

@@ -222,11 +222,12 @@ __device__ __forceinline__ float lb_d2_line_box(const float o[3], const float m[
 // ---------------------------------------------------------------------------
 // _lin_lut, kernel_function/line_integrated_kernel.jl:13-19, with the
 // q >= q_max cut (:90-94) and the 1/h factor (:132-137).
-// n = entries of the table, dq its spacing, K the kernel's support.
-template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq, int n, C K) {
+// n = entries of the table, dq its spacing (idq = 1/dq: the float path
+// multiplies, FP64 divides as the reference does), K the kernel's support.
+template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C* lut, C dq, C idq, int n, C K) {
     C q = r * invh;
     if (q >= K) return C(0);
-    C idxf = q / dq + C(1);
+    C idxf = (sizeof(C) == 4 ? q * idq : q / dq) + C(1);
     int i = (int)idxf;  // q >= 0
     i = i < 1 ? 1 : (i > n - 1 ? n - 1 : i);
     C t = idxf - C(i);
@@ -237,6 +238,7 @@ template <class C> __device__ __forceinline__ C line_W(C r, C h, C invh, const C
 // Per-warp shared-memory stage of a span of leaves (FP32C line path).
 template <int KC> struct LStage {
     float4 L[SPAN];
+    float ih[SPAN];  // 1/h (float)
     float mr[SPAN];
     float col[KC][SPAN];
 };
@@ -261,6 +263,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     // dq = Q[2] - Q[1] of the n-point table over [0, K] = K/(n-1) rounded to CT
     const CT dq = (CT)(A.tv.Kd / (double)(nlut - 1));
     const CT Kc = (CT)A.tv.Kd;
+    const CT idq = CT(1) / dq;
 
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
@@ -304,19 +307,19 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     const int kc = A.rec.kc;
 
     // line-integrated weight of one accepted pair (s = squared distance)
-    auto body = [&](int64_t li, CT s, CT hb, CT mr, const CT* cols) {
+    // dr = the line's distance from the particle, ib = 1/hb
+    auto body = [&](int64_t li, CT dr, CT hb, CT ib, CT mr, const CT* cols) {
         ++n_pairs;
         if (WHAT == WHAT_DIGEST) {
             ++hcount;
             hsum += mix64((uint64_t)(li + 1));
             return;
         }
-        const CT dr = sqrt(s < CT(0) ? CT(0) : s);
         CT W;
-        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut, Kc);
+        if (ST == ST_GATHER) W = line_W<CT>(dr, (CT)ha, ia, lut, dq, idq, nlut, Kc);
         else {
-            CT Wb = line_W<CT>(dr, hb, CT(1) / hb, lut, dq, nlut, Kc);
-            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq, nlut, Kc) + Wb);
+            CT Wb = line_W<CT>(dr, hb, ib, lut, dq, idq, nlut, Kc);
+            W = (ST == ST_SCATTER) ? Wb : CT(0.5) * (line_W<CT>(dr, (CT)ha, ia, lut, dq, idq, nlut, Kc) + Wb);
         }
         const CT w = mr * W;
         S1.add(w);
@@ -350,6 +353,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
                 const int64_t li = lo + lane;
                 st.L[lane] = __ldg(&tv.leaf4[li]);
                 if (WHAT != WHAT_DIGEST) {
+                    st.ih[lane] = __ldg(&tv.leafK[li]).x;
                     st.mr[lane] = __ldg(&tv.mrho[li]);
 #pragma unroll
                     for (int c = 0; c < KC; ++c)
@@ -360,14 +364,17 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
             if (!part) return;
             float cf[3], cerr;
             perp_anchor(lo, cf, cerr);
+            // one error bound for every leaf of the span: |v|_1 <= |L|_1 + |cf|_1
+            // with |L|_1 <= spanb.x (the span's largest, rounded up)
+            const float sbx = __ldg(&tv.spanb[lo]).x;
+            const float ev = 8.f * U1 * (2.f * sbx + fabsf(cf[0]) + fabsf(cf[1]) + fabsf(cf[2])) * (1.f + 4.f * U1) +
+                             cerr + 1e-30f;
             for (int j = 0; j < cnt; ++j) {
                 const float4 L = st.L[j];
                 float v0 = L.x + cf[0], v1 = L.y + cf[1], v2 = L.z + cf[2];
                 float vm = v0 * mf3[0] + v1 * mf3[1] + v2 * mf3[2];
                 float w0 = v0 - vm * mf3[0], w1 = v1 - vm * mf3[1], w2 = v2 - vm * mf3[2];
                 float fs = w0 * w0 + w1 * w1 + w2 * w2;
-                float vn = fabsf(v0) + fabsf(v1) + fabsf(v2);
-                float ev = 8.f * U1 * (vn + fabsf(L.x) + fabsf(L.y) + fabsf(L.z)) + cerr + 1e-30f;
                 float r = sqrtf(fs);
                 float up = r + ev, dn = fmaxf(r - ev, 0.f);
                 const float kb = tv.Kf * L.w;
@@ -392,7 +399,7 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
                 CT cols[KC];
 #pragma unroll
                 for (int c = 0; c < KC; ++c) cols[c] = (c < kc) ? (CT)st.col[c][j] : CT(0);
-                body(lo + j, (CT)fs, (CT)L.w, (CT)st.mr[j], cols);
+                body(lo + j, (CT)r, (CT)L.w, (CT)st.ih[j], (CT)st.mr[j], cols);
             }
         };
         ok = warp_traverse_spans(start, tv.n, tv.links, tv.escape, valid, node_fn, span_fn, steps);
@@ -411,7 +418,8 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
 #pragma unroll
             for (int c = 0; c < KC; ++c) cols[c] = (c < kc) ? (CT)__ldg(&A.colT[c][li]) : CT(0);
             CT mr = (WHAT == WHAT_DIGEST) ? CT(0) : (CT)((double)tv.m[li] / (double)tv.rho[li]);
-            body(li, (CT)e2, (CT)hb, mr, cols);
+            const CT s2 = (CT)e2;
+            body(li, sqrt(s2 < CT(0) ? CT(0) : s2), (CT)hb, CT(1) / (CT)hb, mr, cols);
         };
         ok = warp_traverse(start, tv.n, tv.left, tv.escape, valid, node_fn, leaf_fn);
     }

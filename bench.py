@@ -602,6 +602,7 @@ def main():
         tot32, steps32, kern32, pairs = timed(L.PSB_PREC_FP32C, args.steps, args.warmup)
     launches_per_step = ctx.last_stats.launches
     ctx_steps = ctx.last_stats.warp_steps
+    ctx_spans, ctx_span_tests = ctx.last_stats.spans, ctx.last_stats.span_tests
     tot = torch.tensor([tot32], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(tot, op=dist.ReduceOp.MAX)
@@ -700,7 +701,8 @@ def main():
                          "traffic": (tr or {}).get("bytes_per_launch") if tr else None,
                          "kernel": "k_collect + k_bodies <double,FP32C,SYMMETRIC,4> (pair lists, pair sums)", "kernel_ms": kern_ms,
                          "pairs_per_launch": int(pairs), "alg_bytes_per_launch": int(b_alg),
-                         "warp_steps_per_launch": int(ctx_steps)},
+                         "warp_steps_per_launch": int(ctx_steps), "span_visits_per_launch": int(ctx_spans),
+                         "samples_per_span_visit": ctx_span_tests / max(ctx_spans, 1)},
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs,
             "grad_fwd_time_ratio": extra["adjoint"]["grad_fwd_time_ratio"] if extra else None,
             "lines": extra["lines"] if extra else None, "adjoint": extra["adjoint"] if extra else None,

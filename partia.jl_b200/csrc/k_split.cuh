@@ -23,7 +23,8 @@ template <class T> struct CStage<T, true> {
     float4 Q[SPAN];   // leaf position relative to the warp anchor, h (nearest search)
     float4 P[SPAN];   // sample position relative to the warp anchor, error bound
     float2 R[SPAN];   // sample radius bounds
-    float2 AB[SPAN];  // per-span squared thresholds of each sample
+    float2 AB[SPAN];  // per-span squared thresholds of each leaf
+    float2 SAB[SPAN]; // per-span squared thresholds of each sample
     float thr[SPAN];  // nearest search: candidate threshold
 };
 
@@ -172,28 +173,50 @@ __global__ void __launch_bounds__(128, 8) k_collect(const Args<T> A) {
             float rmax = rahimax;
             if (ST != ST_GATHER) rmax = fmaxf(rmax, tv.Kf * sb.y * (1.f + 3.f * U1));
             const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
+            // this lane's sample thresholds
+            float As = 0.f, Bs = 0.f;
+            if (ST != ST_SCATTER) {
+                const float il = fmaxf((Rme.x - E) * (1.f - 4.f * U1), 0.f), ih2 = (Rme.y + E) * (1.f + 4.f * U1);
+                As = il * il;
+                Bs = ih2 * ih2;
+            }
+            // few samples take part: lane j tests leaf j against each of them;
+            // otherwise each taking lane tests its sample against every leaf
+            const bool by_sample = 3 * __popc(parts) >= 2 * cnt;  // warp-uniform
             // the span's leaves (and their radius thresholds) in shared memory
             __syncwarp();
+            float4 Qme = make_float4(0.f, 0.f, 0.f, 0.f);
+            float Aj = 0.f, Bj = 0.f;
             if (lane < cnt) {
                 const float4 L = __ldg(&tv.leaf4[lo + lane]);
-                st.Q[lane] = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
+                Qme = make_float4(L.x + o0, L.y + o1, L.z + o2, L.w);
+                st.Q[lane] = Qme;
                 if (ST != ST_GATHER) {
                     const float rbhi = tv.Kf * L.w * (1.f + 3.f * U1), rblo = tv.Kf * L.w * (1.f - 3.f * U1);
                     const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih2 = (rbhi + E) * (1.f + 4.f * U1);
-                    st.AB[lane] = make_float2(il * il, ih2 * ih2);
+                    Aj = il * il;
+                    Bj = ih2 * ih2;
+                    st.AB[lane] = make_float2(Aj, Bj);
                 }
             }
+            if (!by_sample) st.SAB[lane] = make_float2(As, Bs);
             __syncwarp();
-            // surely in: d2 < A; maybe in: d2 <= B (undecided = maybe and not surely);
-            // each lane tests its own sample against every leaf of the span
+            // surely in: d2 < A; maybe in: d2 <= B (undecided = maybe and not surely)
             unsigned myacc = 0, mymaybe = 0;
-            if (part) {
-                float As = 0.f, Bs = 0.f;
-                if (ST != ST_SCATTER) {
-                    const float il = fmaxf((Rme.x - E) * (1.f - 4.f * U1), 0.f), ih2 = (Rme.y + E) * (1.f + 4.f * U1);
-                    As = il * il;
-                    Bs = ih2 * ih2;
+            if (!by_sample) {
+                for (unsigned pp = parts; pp; pp &= pp - 1) {
+                    const int s = __ffs(pp) - 1;
+                    const float4 Ps = st.P[s];
+                    const float2 sab = st.SAB[s];
+                    const float dx = Ps.x - Qme.x, dy = Ps.y - Qme.y, dz = Ps.z - Qme.z;
+                    const float d2 = dx * dx + dy * dy + dz * dz;
+                    const float At = (ST == ST_GATHER) ? sab.x : ((ST == ST_SCATTER) ? Aj : fmaxf(sab.x, Aj));
+                    const float Bt = (ST == ST_GATHER) ? sab.y : ((ST == ST_SCATTER) ? Bj : fmaxf(sab.y, Bj));
+                    const unsigned bi = __ballot_sync(PSB_FULL, lane < cnt && d2 < At);
+                    const unsigned bm = __ballot_sync(PSB_FULL, lane < cnt && d2 <= Bt);
+                    if (lane == s) { myacc = bi; mymaybe = bm; }
                 }
+            } else if (part) {
 #pragma unroll 4
                 for (int j = 0; j < cnt; ++j) {
                     const float4 Q = st.Q[j];

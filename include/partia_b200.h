@@ -18,7 +18,11 @@
  *    sample, smoothing-length and output pointers are caller-owned HOST
  *    buffers; the library copies them to and from the device inside the call.
  *    With PSB_FLAG_DEVICE_PTRS they are device pointers on the context's device
- *    and no host<->device copy happens.
+ *    and no host<->device copy happens.  Each is checked on the host before
+ *    any work is queued: pageable host memory or another device's memory is
+ *    refused with PSB_EINVAL (managed memory and page-locked host memory
+ *    mapped at the same address are accepted).  Buffer lengths cannot be
+ *    checked this way and remain the caller's contract.
  *  - Element type of particle, sample and output arrays is the context dtype
  *    chosen in psb_set_particles (double for PSB_F64, float for PSB_F32),
  *    matching Partia's single float type TF per InterpolationInput.

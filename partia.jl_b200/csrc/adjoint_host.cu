@@ -99,6 +99,17 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
     if (!gm || !gx || !gy || !gz) return fail(c, PSB_EINVAL, "gradient outputs must not be NULL");
     const bool need_h = st != ST_SCATTER && hmode != PSB_H_NEAREST;
     if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+    if (dev) {  // pointers used in device copies, memsets and kernels
+        int rc = PSB_OK;
+        for (int q = 0; !rc && ns > 0 && rq0.kind == SRC_ARRAYS && q < (line ? 6 : 3); ++q)
+            rc = check_device_ptr(c, rq0.a[q], "a sample coordinate array");
+        if (!rc && ns > 0 && need_h) rc = check_device_ptr(c, hs, "hs");
+        for (int k = 0; !rc && ns > 0 && k < L; ++k) rc = check_device_ptr(c, gout[k], "a gout array");
+        for (const double* p : {gm, gx, gy, gz})
+            if (!rc && n > 0) rc = check_device_ptr(c, p, "a gradient output");
+        for (int k = 0; !rc && n > 0 && gcols && k < c->ncol; ++k) rc = check_device_ptr(c, gcols[k], "a column gradient");
+        if (rc) return rc;
+    }
     if (rq0.kind == SRC_BEAM) {
         if (rq0.nx < 2 || rq0.ny < 2) return fail(c, PSB_EUNSUPPORTED, "the beam adjoint needs nx, ny >= 2");
         const double* f = (const double*)rq0.frame;

@@ -40,6 +40,30 @@ void* scratch(psb_ctx* c, int k, size_t bytes) {
     return sl.p;
 }
 
+int check_device_ptr(psb_ctx* c, const void* p, const char* what) {
+    if (!p) return PSB_OK;
+    cudaPointerAttributes at;
+    memset(&at, 0, sizeof(at));
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, PSB_EINVAL, std::string(what) + " is not a device pointer (PSB_FLAG_DEVICE_PTRS is set)");
+    }
+    switch (at.type) {
+        case cudaMemoryTypeManaged:
+            return PSB_OK;
+        case cudaMemoryTypeHost:
+            if (at.devicePointer == p) return PSB_OK;
+            return fail(c, PSB_EINVAL, std::string(what) + " is page-locked host memory not mapped at the same "
+                                                           "device address (PSB_FLAG_DEVICE_PTRS is set)");
+        case cudaMemoryTypeDevice:
+            if (at.device == c->device) return PSB_OK;
+            return fail(c, PSB_EINVAL, std::string(what) + " is memory of device " + std::to_string(at.device) +
+                                           ", the context is on device " + std::to_string(c->device));
+        default:
+            return fail(c, PSB_EINVAL, std::string(what) + " is a pageable host pointer, but PSB_FLAG_DEVICE_PTRS is set");
+    }
+}
+
 static cudaError_t grow_buf(psb_ctx* c, void*& p, size_t& cap, size_t bytes) {
     if (bytes < 256) bytes = 256;
     if (p && cap >= bytes) return cudaSuccess;
@@ -303,6 +327,13 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
     for (int k = 0; n > 0 && k < ncol; ++k)
         if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
     cudaSetDevice(c->device);
+    if ((flags & PSB_FLAG_DEVICE_PTRS) && n > 0) {
+        int rc = PSB_OK;
+        for (const void* p : {x, y, z, m, h, rho})
+            if (!rc) rc = check_device_ptr(c, p, "a particle array");
+        for (int k = 0; !rc && k < ncol; ++k) rc = check_device_ptr(c, cols[k], "a particle column");
+        if (rc) return rc;
+    }
     reset_tree(c);
     PSB_CUDA_TRY(c, load_line_tables(c, (int)kernel), "line table upload");
     c->dt = dt;

@@ -218,6 +218,18 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     if (what == WHAT_DIGEST && ns > 0 && (!dcount || !dhash)) return fail(c, PSB_EINVAL, "digest outputs are NULL");
     const bool need_h = (st != ST_SCATTER) && !(hmode == PSB_H_NEAREST && !rq.line);
     if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+    if (dev && ns > 0) {  // pointers the kernels dereference directly
+        int rc = PSB_OK;
+        for (int q = 0; !rc && rq.kind == SRC_ARRAYS && q < (rq.line ? 6 : 3); ++q)
+            rc = check_device_ptr(c, rq.a[q], "a sample coordinate array");
+        if (!rc && need_h) rc = check_device_ptr(c, hs, "hs");
+        for (int k = 0; !rc && what == WHAT_INTERP && !adj && k < L; ++k) rc = check_device_ptr(c, out[k], "an output array");
+        if (!rc && what == WHAT_DENSITY) rc = check_device_ptr(c, out[0], "the density output");
+        if (!rc && what == WHAT_DIGEST) rc = check_device_ptr(c, dcount, "the digest counts");
+        if (!rc && what == WHAT_DIGEST) rc = check_device_ptr(c, dhash, "the digest hashes");
+        if (!rc && what == WHAT_DIGEST) rc = check_device_ptr(c, ha_out, "the digest smoothing lengths");
+        if (rc) return rc;
+    }
 
     A.tv = tree_view<T>(c);
     A.hmode = hmode;

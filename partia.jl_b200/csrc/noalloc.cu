@@ -132,6 +132,13 @@ int noalloc_typed(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const 
     }
     const bool need_h = (st != ST_SCATTER) && hmode != PSB_H_NEAREST;
     if (need_h && !hs) return fail(c, PSB_EINVAL, "hs must not be NULL for this strategy and hmode");
+    if (ns > 0) {  // the kernels dereference these directly
+        for (const void* p : {sx, sy, sz})
+            if (!rc) rc = check_device_ptr(c, p, "a sample coordinate array");
+        if (!rc && need_h) rc = check_device_ptr(c, hs, "hs");
+        for (int k = 0; !rc && k < L; ++k) rc = check_device_ptr(c, out[k], "an output array");
+        if (rc) return rc;
+    }
 
     // carve the static scratch: counters | sample codes | sample order | sort scratch
     void* base = nullptr;

@@ -91,7 +91,13 @@ int fail(psb_ctx* c, int code, const std::string& msg);
 int cuda_fail(psb_ctx* c, cudaError_t e, const char* what);
 // Grow-on-demand scratch slot k to at least `bytes`; returns nullptr on failure.
 void* scratch(psb_ctx* c, int k, size_t bytes);
-// Free every particle and tree buffer (not the scratch).
+// With PSB_FLAG_DEVICE_PTRS the kernels read or write a caller's pointer
+// directly, so it must be reachable from the context's device: device memory
+// of that device, managed memory, or page-locked host memory mapped at the
+// same address.  Anything else (pageable host memory, another device's
+// memory) would fault inside a kernel; it is refused here with PSB_EINVAL.
+// A null pointer passes (the callers check for NULL where it matters).
+int check_device_ptr(psb_ctx* c, const void* p, const char* what);
 // Device buffer *p with room for at least `bytes`, reallocated only when it
 // must grow (after the context's stream has finished with the old one).
 cudaError_t dgrow(psb_ctx* c, void** p, size_t bytes);

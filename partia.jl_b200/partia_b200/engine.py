@@ -62,6 +62,7 @@ class Context:
         if rc != 0:
             raise L.PsbError(rc, "psb_create failed (is a CUDA device visible?)")
         self.h = h
+        self.device = int(device)
         # OR-ed into the flags of the interpolation calls (e.g. PSB_FLAG_SINGLE_KERNEL)
         self.extra_flags = 0
         self.dtype = np.dtype(np.float64)
@@ -127,11 +128,17 @@ class Context:
             return a
         return np.ascontiguousarray(np.asarray(a, dtype=self.dtype))
 
-    def _hs(self, hmode, hs):
+    def _hs(self, hmode, hs, dev):
+        """hs where the call's pointers live: on this context's GPU when the
+        call passes device pointers, in host memory otherwise."""
         if hs is None:
             return None
+        if dev:
+            import torch
+            tdt = torch.float64 if self.dtype == np.float64 else torch.float32
+            return torch.as_tensor(hs, dtype=tdt).reshape(-1).to(f"cuda:{self.device}").contiguous()
         if _is_dev(hs):
-            return hs
+            hs = hs.detach().cpu().numpy()
         return np.ascontiguousarray(np.atleast_1d(np.asarray(hs, dtype=self.dtype)))
 
     def _outs(self, ns, L_, like_dev, out=None):
@@ -149,7 +156,7 @@ class Context:
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
         ns = len(sx)
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, dev)
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_points(self.h, ns, _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy,
                                              C.byref(cat.c), prec, _ptr_array(outs),
@@ -177,7 +184,7 @@ class Context:
         """dL/dm, dL/dA_c, dL/dx.. for L = sum_k sum_s gout[k][s] out_k(s), in the particles' given order."""
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, dev)
         go = self._gout(gout, dev)
         g = self._grad_outs(dev)
         self._chk(self.lib.psb_adjoint_points(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa),
@@ -189,7 +196,7 @@ class Context:
     def adjoint_grid(self, ax, ay, az, cat: CatalogC, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
                      hs=None, device=False):
         ax, ay, az = (np.ascontiguousarray(np.asarray(a, dtype=np.float64)) for a in (ax, ay, az))
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, device)
         go = self._gout(gout, device)
         g = self._grad_outs(device)
         self._chk(self.lib.psb_adjoint_grid(self.h, ax.ctypes.data, len(ax), ay.ctypes.data, len(ay),
@@ -203,7 +210,7 @@ class Context:
                      hmode=L.PSB_H_PER_SAMPLE, hs=None, device=False):
         fr = np.ascontiguousarray(np.asarray(frame, dtype=np.float64).reshape(12))
         pa = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(4))
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, device)
         go = self._gout(gout, device)
         g = self._grad_outs(device)
         self._chk(self.lib.psb_adjoint_beam(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, hmode, _ptr(hsa),
@@ -216,8 +223,8 @@ class Context:
                     prec=L.PSB_PREC_FP64, out=None, device_out=False):
         ax, ay, az = (np.ascontiguousarray(np.asarray(a, dtype=self.dtype)) for a in (ax, ay, az))
         ns = len(ax) * len(ay) * len(az)
-        hsa = self._hs(hmode, hs)
         dev = device_out or (out is not None and _is_dev(out[0]))
+        hsa = self._hs(hmode, hs, dev)
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_grid(self.h, ax.ctypes.data, len(ax), ay.ctypes.data, len(ay),
                                            az.ctypes.data, len(az), hmode, _ptr(hsa), strategy, C.byref(cat.c), prec,
@@ -230,8 +237,8 @@ class Context:
         fr = np.ascontiguousarray(np.asarray(frame, dtype=self.dtype).reshape(12))
         pa = np.ascontiguousarray(np.asarray(params, dtype=self.dtype).reshape(6))
         ns = nx * ny * nz
-        hsa = self._hs(hmode, hs)
         dev = device_out or (out is not None and _is_dev(out[0]))
+        hsa = self._hs(hmode, hs, dev)
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_box(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, nz, hmode, _ptr(hsa),
                                           strategy, C.byref(cat.c), prec, _ptr_array(outs),
@@ -243,7 +250,7 @@ class Context:
         arrs = [self._arr(a) for a in (*o, *d)]
         dev = _is_dev(arrs[0])
         nl = len(arrs[0])
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, dev)
         outs = self._outs(nl, cat.L, dev, out)
         self._chk(self.lib.psb_interp_lines(self.h, nl, *[_ptr(a) for a in arrs], hmode, _ptr(hsa), strategy,
                                             C.byref(cat.c), prec, _ptr_array(outs),
@@ -254,8 +261,8 @@ class Context:
                     hs=None, prec=L.PSB_PREC_FP64, out=None, device_out=False):
         fr = np.ascontiguousarray(np.asarray(frame, dtype=self.dtype).reshape(12))
         pa = np.ascontiguousarray(np.asarray(params, dtype=self.dtype).reshape(4))
-        hsa = self._hs(hmode, hs)
         dev = device_out or (out is not None and _is_dev(out[0]))
+        hsa = self._hs(hmode, hs, dev)
         outs = self._outs(nx * ny, cat.L, dev, out)
         self._chk(self.lib.psb_interp_beam(self.h, fr.ctypes.data, pa.ctypes.data, nx, ny, hmode, _ptr(hsa), strategy,
                                            C.byref(cat.c), prec, _ptr_array(outs),
@@ -266,7 +273,7 @@ class Context:
                 out=None):
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, dev)
         o = out if out is not None else self._outs(len(sx), 1, dev)[0]
         self._chk(self.lib.psb_density(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy, prec,
                                        _ptr(o), (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
@@ -277,7 +284,7 @@ class Context:
         arrs = [self._arr(v) for v in a]
         darrs = [self._arr(v) for v in d] if d is not None else [None, None, None]
         ns = len(arrs[0])
-        hsa = self._hs(hmode, hs)
+        hsa = self._hs(hmode, hs, False)
         cnt = np.zeros(ns, dtype=np.int64)
         hsh = np.zeros(ns, dtype=np.uint64)
         ha = np.zeros(ns, dtype=self.dtype)

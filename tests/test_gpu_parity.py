@@ -351,6 +351,56 @@ def test_error_paths():
     assert e.value.code == L.PSB_EINVAL
 
 
+def _pageable(ptr):
+    """True when CUDA reports ptr as pageable (unregistered) host memory."""
+    from cuda.bindings import runtime as rt
+    err, at = rt.cudaPointerGetAttributes(ptr)
+    return err != rt.cudaError_t.cudaSuccess or at.type == rt.cudaMemoryType.cudaMemoryTypeUnregistered
+
+
+def test_device_ptr_flag_refuses_host_pointers():
+    """With PSB_FLAG_DEVICE_PTRS a pageable host pointer is refused on the host
+    (PSB_EINVAL) before any copy or launch, and the context stays usable."""
+    import ctypes as C
+    import torch
+    arrs, cols = make_particles(2000, 93)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build()
+    cat = CatalogC(scalars=[0])
+    rng = np.random.default_rng(94)
+    s = [rng.random(500) for _ in range(3)]
+    hs_host = np.full(500, 0.05)
+    ts = [torch.from_numpy(a).cuda() for a in s]
+    out = [torch.empty(500, dtype=torch.float64, device="cuda")]
+    assert _pageable(hs_host.ctypes.data) and _pageable(s[0].ctypes.data)
+    lib = L.load()
+
+    optr = (C.c_void_p * 1)(out[0].data_ptr())
+
+    def call(sx, sy, sz, hs):
+        return lib.psb_interp_points(ctx.h, 500, sx, sy, sz, L.PSB_H_PER_SAMPLE, hs, L.PSB_GATHER, C.byref(cat.c),
+                                     L.PSB_PREC_FP64, optr, L.PSB_FLAG_DEVICE_PTRS, None)
+
+    dptr = [t.data_ptr() for t in ts]
+    assert call(*dptr, hs_host.ctypes.data) == L.PSB_EINVAL
+    assert b"hs" in lib.psb_last_error(ctx.h)
+    assert call(s[0].ctypes.data, dptr[1], dptr[2], torch.from_numpy(hs_host).cuda().data_ptr()) == L.PSB_EINVAL
+    assert b"sample" in lib.psb_last_error(ctx.h)
+    torch.cuda.synchronize()
+    # the engine places a host hs on the device for device outputs; results
+    # equal the host-pointer call's
+    got = ctx.interp_points(*ts, cat, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=hs_host)
+    ref = ctx.interp_points(*s, cat, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=hs_host)
+    assert np.array_equal(got[0].cpu().numpy(), ref[0], equal_nan=True)
+    ax = np.linspace(0.1, 0.9, 8)
+    dout = [torch.empty(8 ** 3, dtype=torch.float64, device="cuda")]
+    hg = np.full(8 ** 3, 0.04)
+    got = ctx.interp_grid(ax, ax, ax, cat, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=hg, out=dout)
+    ref = ctx.interp_grid(ax, ax, ax, cat, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=hg)
+    assert np.array_equal(got[0].cpu().numpy(), ref[0], equal_nan=True)
+
+
 def test_short_float_line_table():
     """PSB_FLAG_LUT1000_F32: line integrals from the 1000-entry float table
     stay within its interpolation error of the 4096-entry table (spacing

@@ -228,15 +228,29 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
                 st.thr[lane] = isinf(best) ? INFINITY : t * t;
             }
             __syncwarp();
-            const float4 Q = st.Q[lane < cnt ? lane : 0];
-            for (unsigned pp = parts; pp; pp &= pp - 1) {
-                const int s = __ffs(pp) - 1;
-                const float4 P = st.P[s];
-                const float thr = st.thr[s];
-                float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
-                bool c = (lane < cnt) && (dx * dx + dy * dy + dz * dz <= thr);
-                unsigned b = __ballot_sync(PSB_FULL, c);
-                if (lane == s) cand = b;
+            if (3 * __popc(parts) >= 2 * cnt) {  // warp-uniform: many samples take part
+                // each taking lane tests its sample against every leaf
+                if (part) {
+                    const float4 P = st.P[lane];
+                    const float thr = st.thr[lane];
+#pragma unroll 4
+                    for (int j = 0; j < cnt; ++j) {
+                        const float4 Q = st.Q[j];
+                        float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                        cand |= (unsigned)(dx * dx + dy * dy + dz * dz <= thr) << j;
+                    }
+                }
+            } else {  // lane j tests leaf j against each taking sample
+                const float4 Q = st.Q[lane < cnt ? lane : 0];
+                for (unsigned pp = parts; pp; pp &= pp - 1) {
+                    const int s = __ffs(pp) - 1;
+                    const float4 P = st.P[s];
+                    const float thr = st.thr[s];
+                    float dx = P.x - Q.x, dy = P.y - Q.y, dz = P.z - Q.z;
+                    bool c = (lane < cnt) && (dx * dx + dy * dy + dz * dz <= thr);
+                    unsigned b = __ballot_sync(PSB_FULL, c);
+                    if (lane == s) cand = b;
+                }
             }
             for (; cand; cand &= cand - 1) {
                 const int64_t li = lo + __ffs(cand) - 1;

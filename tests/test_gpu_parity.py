@@ -401,6 +401,42 @@ def test_device_ptr_flag_refuses_host_pointers():
     assert np.array_equal(got[0].cpu().numpy(), ref[0], equal_nan=True)
 
 
+@pytest.mark.parametrize("nx", [8, 12])
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+def test_traversal_analytic_mean_errors(nx, prec):
+    """The analytic lattice regression of test/traversal_analytic.jl:48-101
+    through the library: the reference's mean-error bounds, and the oracle's
+    values (FP64 to 1e-12, FP32C to 1e-6 of each field's max)."""
+    from test_oracle_fixtures import ANALYTIC_BOUNDS, ANALYTIC_CAT, analytic_errors, analytic_refs, lattice
+    P, cols = lattice(nx, variable_h=False)
+    arrs = [P[k] for k in ("x", "y", "z", "m", "h", "rho")]
+    orc = O.Oracle(*arrs, cols=cols)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build()
+    h, sx, sy, sz = analytic_refs(nx)
+    hs = np.array([h])
+    tol = FP64_TOL if prec == L.PSB_PREC_FP64 else FP32C_SMOOTH_TOL
+    pooled = {k: [] for k in ANALYTIC_BOUNDS}
+    for st in (L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC):
+        got = ctx.interp_points(sx, sy, sz, CatalogC(**ANALYTIC_CAT), strategy=st, hmode=L.PSB_H_CONSTANT, hs=hs,
+                                prec=prec)
+        rho = ctx.density(sx, sy, sz, strategy=st, hmode=L.PSB_H_CONSTANT, hs=hs, prec=prec)
+        ref = orc.interp_points(sx, sy, sz, O.Catalog(**ANALYTIC_CAT), strategy=st, hmode=O.H_CONSTANT, hs=hs)
+        rref = orc.density(sx, sy, sz, strategy=st, hmode=O.H_CONSTANT, hs=hs)
+        for k in range(len(ref)):
+            # grad rho vanishes up to rounding, so every field is compared on at
+            # least the scale of its pair terms: 1 for q and rho, 1/h for the
+            # gradients, divergence and curl of O(1) fields
+            scale = max(np.max(np.abs(ref[k])), 1.0 if k == 0 else 1.0 / h)
+            assert np.max(np.abs(got[k] - ref[k])) <= tol * scale, k
+        assert rel_err(rho, rref) <= tol
+        for k, v in analytic_errors(got, rho, sx, sy, sz).items():
+            pooled[k].append(v)
+    for k, bound in ANALYTIC_BOUNDS.items():
+        assert float(np.mean(np.concatenate(pooled[k]))) <= bound, k
+
+
 def test_short_float_line_table():
     """PSB_FLAG_LUT1000_F32: line integrals from the 1000-entry float table
     stay within its interpolation error of the 4096-entry table (spacing

@@ -11,6 +11,9 @@
    strategies, the reference's atol/rtol
    (test/point_samples_interpolation_tests.jl:211-239,
     test/interpolation_analytic_test_common.jl:31-75)
+ * uniform 8^3 and 12^3 lattices, constant h: mean errors of Shepard q,
+   grad q, div v, curl v, rho and grad rho against the analytic fields,
+   pooled over the three strategies (test/traversal_analytic.jl:48-101)
  * uniform vector field: divergence = curl = 0 to 1e-12
    (test/interpolation_tests.jl:305-336)
  * empty neighbourhoods: density 0, every other field NaN
@@ -90,13 +93,16 @@ def test_line_fixture_scatter():
         assert out[1][i] == pytest.approx(ref[1], rel=1e-10, abs=1e-12)
 
 
-def lattice(nx=12, eta=1.2):
+def lattice(nx=12, eta=1.2, variable_h=True):
     dx = 1.0 / nx
     c = np.arange(dx / 2, 1.0 - dx / 2 + 1e-12, dx)
     X, Y, Z = np.meshgrid(c, c, c, indexing="ij")   # x outermost, z fastest, as the Julia loop
     x, y, z = X.ravel(), Y.ravel(), Z.ravel()
     n = len(x)
-    h = eta * dx * (1.0 + 0.18 * (x - 0.5) - 0.10 * (y - 0.5) + 0.08 * (z - 0.5))
+    if variable_h:
+        h = eta * dx * (1.0 + 0.18 * (x - 0.5) - 0.10 * (y - 0.5) + 0.08 * (z - 0.5))
+    else:
+        h = np.full(n, eta * dx)
     P = dict(x=x, y=y, z=z, m=np.full(n, dx ** 3), h=h, rho=np.ones(n))
     cols = [x + y + z, x.copy(), y.copy(), z.copy()]
     return P, cols
@@ -117,6 +123,55 @@ def test_analytic_linear_fields(strategy):
         assert out[4][i] == pytest.approx(3.0, abs=1e-1, rel=2e-2)
         for k in (5, 6, 7):
             assert out[k][i] == pytest.approx(0.0, abs=5e-2)
+
+
+# catalog of the analytic traversal regression: Shepard q, grad q, grad rho,
+# div v, curl v (outputs 0 | 1-3 | 4-6 | 7 | 8-10)
+ANALYTIC_CAT = dict(scalars=[0], shepard=[1], grads=[0, -1], divs=[1, 2, 3], curls=[1, 2, 3])
+# mean-absolute-error bounds of test/traversal_analytic.jl:94-99
+ANALYTIC_BOUNDS = dict(scalar=2e-2, grad=6e-2, div=1e-1, curl=5e-2, rho=5e-2, grad_rho=5e-2)
+
+
+def analytic_refs(nx, eta=1.2, n=12, seed=0xA11CE):
+    """n reference points at least 1.5 K h from the cube's faces (K = 2 for
+    M4), as sample_reference_points (test/interpolation_analytic_test_common.jl:75-87),
+    drawn from numpy's PCG64 instead of Julia's Xoshiro."""
+    h = eta / nx
+    lo, hi = 1.5 * 2.0 * h, 1.0 - 1.5 * 2.0 * h
+    r = np.random.default_rng(seed).random((n, 3)) * (hi - lo) + lo
+    return h, r[:, 0].copy(), r[:, 1].copy(), r[:, 2].copy()
+
+
+def analytic_errors(outs, rho, sx, sy, sz):
+    """Per-sample errors against q = x + y + z, grad q = (1,1,1), v = r
+    (div 3, curl 0) and the uniform density 1 with zero gradient."""
+    o = [np.asarray(a, dtype=np.float64) for a in outs]
+    return dict(scalar=np.abs(o[0] - (sx + sy + sz)),
+                grad=np.sqrt((o[1] - 1) ** 2 + (o[2] - 1) ** 2 + (o[3] - 1) ** 2),
+                div=np.abs(o[7] - 3.0),
+                curl=np.sqrt(o[8] ** 2 + o[9] ** 2 + o[10] ** 2),
+                rho=np.abs(np.asarray(rho, dtype=np.float64) - 1.0),
+                grad_rho=np.sqrt(o[4] ** 2 + o[5] ** 2 + o[6] ** 2))
+
+
+@pytest.mark.parametrize("nx", [8, 12])
+def test_traversal_analytic_mean_errors(nx):
+    """test/traversal_analytic.jl:48-101: uniform lattice (eta 1.2, constant h),
+    12 interior reference points, errors pooled over the three strategies."""
+    P, cols = lattice(nx, variable_h=False)
+    orc = make_oracle(P, cols)
+    h, sx, sy, sz = analytic_refs(nx)
+    cat = O.Catalog(**ANALYTIC_CAT)
+    pooled = {k: [] for k in ANALYTIC_BOUNDS}
+    for st in (O.GATHER, O.SCATTER, O.SYMMETRIC):
+        outs = orc.interp_points(sx, sy, sz, cat, strategy=st, hmode=O.H_CONSTANT, hs=np.array([h]))
+        rho = orc.density(sx, sy, sz, strategy=st, hmode=O.H_CONSTANT, hs=np.array([h]))
+        for k, v in analytic_errors(outs, rho, sx, sy, sz).items():
+            pooled[k].append(v)
+    for k, bound in ANALYTIC_BOUNDS.items():
+        err = np.concatenate(pooled[k])
+        assert np.all(np.isfinite(err)), k
+        assert float(np.mean(err)) <= bound, (k, float(np.mean(err)))
 
 
 @pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])

@@ -437,6 +437,35 @@ def test_traversal_analytic_mean_errors(nx, prec):
         assert float(np.mean(np.concatenate(pooled[k]))) <= bound, k
 
 
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+def test_structured_grid_analytic_regression(prec):
+    """test/structured_grid_interpolation_tests.jl:322-370 (Cartesian): a 3^3
+    StructuredGrid over [0.35, 0.55]^3 (grid_interpolation_test_common.jl:153-160)
+    on the 12^3 lattice with variable h, nearest-particle h, every strategy:
+    each point within the reference's atol/rtol of the analytic fields, and the
+    grid equal to its flattened point samples."""
+    from partia_b200 import linrange
+    from test_oracle_fixtures import lattice
+    P, cols = lattice(12)
+    arrs = [P[k] for k in ("x", "y", "z", "m", "h", "rho")]
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build()
+    ax = linrange(0.35, 0.55, 3)
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    px, py, pz = X.ravel(order="F"), Y.ravel(order="F"), Z.ravel(order="F")
+    cat = CatalogC(scalars=[0], shepard=[1], grads=[0], divs=[1, 2, 3], curls=[1, 2, 3])
+    for st in (L.PSB_GATHER, L.PSB_SCATTER, L.PSB_SYMMETRIC):
+        g = ctx.interp_grid(ax, ax, ax, cat, strategy=st, hmode=L.PSB_H_NEAREST, prec=prec)
+        p = ctx.interp_points(px, py, pz, cat, strategy=st, hmode=L.PSB_H_NEAREST, prec=prec)
+        for a, b in zip(g, p):
+            assert np.allclose(a, b, atol=1e-12, rtol=1e-10)
+        want = [(px + py + pz, 2e-2, 1e-2)] + [(np.ones(27), 6e-2, 1e-2)] * 3 + [(np.full(27, 3.0), 1e-1, 2e-2)] + \
+               [(np.zeros(27), 5e-2, 1e-2)] * 3
+        for k, (ref, atol, rtol) in enumerate(want):
+            assert np.all(np.abs(g[k] - ref) <= atol + rtol * np.abs(ref)), (st, k)
+
+
 def test_short_float_line_table():
     """PSB_FLAG_LUT1000_F32: line integrals from the 1000-entry float table
     stay within its interpolation error of the 4096-entry table (spacing

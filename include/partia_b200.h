@@ -64,8 +64,8 @@ typedef enum { PSB_F64 = 0, PSB_F32 = 1 } psb_dtype;
 /* SPH kernel families of src/julia/KernelInterpolation/kernel_function/kernels/ (one file each):
  * support K h (KernelFunctionValid: 2, 2.5, 3, 2, 2, 2), the 3D norm and f, f'
  * of each file, and each family's line-integrated table
- * (table/line_integrated_kernel_tables.jl).  The adjoint calls evaluate
- * PSB_KERNEL_M4 only and return PSB_EUNSUPPORTED for the others. */
+ * (table/line_integrated_kernel_tables.jl).  The adjoint calls differentiate
+ * whichever of them the particles were set with. */
 typedef enum {
     PSB_KERNEL_M4 = 0,
     PSB_KERNEL_M5 = 1,

@@ -914,6 +914,64 @@ template <class T> static inline void m4_g12(T q, T& g1, T& g2) {
     }
 }
 
+// g1 = f'(q)/q and g2 = d g1/dq of the current kernel (g_kern), from the f'
+// of kern_df and f'' of each piece: g2 = (f'' - g1)/q.  The pieces that
+// contain q = 0 are written without the division: M5 on q < 1/2 and M6 on
+// q < 1 are even polynomials there (f = 14.375 - 15 q^2 + 6 q^4 and
+// 66 - 60 q^2 + 30 q^4 - 10 q^5), and the Wendland f' = q P(q) a^n factor
+// exactly (a = 1 - q/2).
+template <class T> static inline void kern_g12(T q, T& g1, T& g2) {
+    g1 = T(0);
+    g2 = T(0);
+    T d1 = T(0), d2 = T(0);
+    switch (g_kern) {
+    case KERN_M5:
+        if (q < T(0.5)) { g1 = T(-30) + T(24) * q * q; g2 = T(48) * q; return; }
+        if (q < T(1.5)) {
+            d1 = T(-4) * pw3(T(2.5) - q) + T(20) * pw3(T(1.5) - q);
+            d2 = T(12) * pw2(T(2.5) - q) - T(60) * pw2(T(1.5) - q);
+        } else if (q < T(2.5)) {
+            d1 = T(-4) * pw3(T(2.5) - q);
+            d2 = T(12) * pw2(T(2.5) - q);
+        } else {
+            return;
+        }
+        break;
+    case KERN_M6:
+        if (q < T(1)) { g1 = T(-120) + q * q * (T(120) - T(50) * q); g2 = q * (T(240) - T(150) * q); return; }
+        if (q < T(2)) {
+            d1 = T(-5) * pw4(T(3) - q) + T(30) * pw4(T(2) - q);
+            d2 = T(20) * pw3(T(3) - q) - T(120) * pw3(T(2) - q);
+        } else if (q < T(3)) {
+            d1 = T(-5) * pw4(T(3) - q);
+            d2 = T(20) * pw3(T(3) - q);
+        } else {
+            return;
+        }
+        break;
+    case KERN_C2: case KERN_C4: case KERN_C6: {
+        if (!(q < T(2))) return;
+        const T a = T(1) - T(0.5) * q;
+        if (g_kern == KERN_C2) {         // f' = -5 q a^3
+            g1 = T(-5) * pw3(a);
+            g2 = T(7.5) * pw2(a);
+        } else if (g_kern == KERN_C4) {  // f' = -14/3 q (1 + 5q/2) a^5
+            g1 = (T(-14) / T(3)) * (T(1) + T(2.5) * q) * pw5(a);
+            g2 = T(35) * q * pw4(a);
+        } else {                         // f' = -11/2 q (1 + 7q/2 + 4q^2) a^7
+            g1 = T(-5.5) * (T(1) + T(3.5) * q + T(4) * q * q) * pw4(a) * pw3(a);
+            g2 = T(33) * q * (T(1) + T(3) * q) * pw3(a) * pw3(a);
+        }
+        return;
+    }
+    default:
+        m4_g12(q, g1, g2);
+        return;
+    }
+    g1 = d1 / q;
+    g2 = (d2 - g1) / q;
+}
+
 // W, gradW and the Hessian (xx, yy, zz, xy, xz, yz) with respect to delta
 template <class T> static inline void kernel_whess(T dx, T dy, T dz, T h, T& W, T g[3], T H[6]) {
     T r2 = dx * dx + dy * dy + dz * dz;
@@ -921,8 +979,8 @@ template <class T> static inline void kernel_whess(T dx, T dy, T dz, T h, T& W, 
     W = kernel_W(r, h);
     kernel_gradW(dx, dy, dz, h, g[0], g[1], g[2]);
     T g1, g2;
-    m4_g12(r / h, g1, g2);
-    T s5 = m4_norm3<T>() / (h * h * h * h * h);
+    kern_g12(r / h, g1, g2);
+    T s5 = kern_norm3<T>() / (h * h * h * h * h);
     T c = s5 * g1;
     T e = (r2 > T(0)) ? s5 * g2 * (r / h) / r2 : T(0);
     H[0] = c + e * dx * dx; H[1] = c + e * dy * dy; H[2] = c + e * dz * dz;
@@ -1495,7 +1553,6 @@ ORC_API int orc_adjoint_points(orc_ctx* c, int64_t ns, const void* sx, const voi
                                void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
     if (!c->built) return -7;
     if (c->dtype != 0) return -6;
-    if (g_kern != KERN_M4) return -5;  // the adjoint is restated for M4
     Catalog cat = make_cat(nsc, ss, sh, ng, gs, nd, ds, nc, cs);
     const int L = cat.L();
     const double* X = (const double*)sx; const double* Y = (const double*)sy; const double* Z = (const double*)sz;
@@ -1513,7 +1570,6 @@ ORC_API int orc_adjoint_points(orc_ctx* c, int64_t ns, const void* sx, const voi
 ORC_API int orc_adjoint_lines(orc_ctx* c, int64_t nl, const void* const* od, int hmode, const void* hs, int mode,
                               int nsc, const int32_t* ss, const uint8_t* sh, const void* const* gout,
                               void* gm, void* const* gcols, void* gx, void* gy, void* gz) {
-    if (g_kern != KERN_M4) return -5;  // the adjoint is restated for M4
     if (!c->built) return -7;
     if (c->dtype != 0) return -6;
     if (mode != SCATTER && hmode == 0) return -1;

@@ -22,16 +22,22 @@ namespace psb {
 
 int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu);
 
-template <int KC, bool SCAL>
+template <int KC, bool SCAL, int KF>
 static void launch_adj_points_ks(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
-    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL><<<g, 128, 0, s>>>(a);
-    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL><<<g, 128, 0, s>>>(a);
-    else k_adj_points<ST_SYMMETRIC, KC, SCAL><<<g, 128, 0, s>>>(a);
+    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+    else k_adj_points<ST_SYMMETRIC, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
 }
+// kf: 0 = the M4 code, 1 = the other kernel families
 template <int KC>
-static void launch_adj_points_k(const AdjArgs& a, int st, bool scal, unsigned g, cudaStream_t s) {
-    if (scal) launch_adj_points_ks<KC, true>(a, st, g, s);
-    else launch_adj_points_ks<KC, false>(a, st, g, s);
+static void launch_adj_points_k(const AdjArgs& a, int st, bool scal, int kf, unsigned g, cudaStream_t s) {
+    if (kf == 0) {
+        if (scal) launch_adj_points_ks<KC, true, 0>(a, st, g, s);
+        else launch_adj_points_ks<KC, false, 0>(a, st, g, s);
+    } else {
+        if (scal) launch_adj_points_ks<KC, true, 1>(a, st, g, s);
+        else launch_adj_points_ks<KC, false, 1>(a, st, g, s);
+    }
 }
 template <int KC>
 static void launch_adj_beam_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
@@ -74,7 +80,6 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
                 uint32_t flags, psb_stats* stats) {
     if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before the adjoint");
     if (c->dt != PSB_F64) return fail(c, PSB_EUNSUPPORTED, "the adjoint needs double particle data");
-    if (c->kern != PSB_KERNEL_M4) return fail(c, PSB_EUNSUPPORTED, "the adjoint evaluates the M4_spline kernel only");
     if (st < 0 || st > 2) return fail(c, PSB_EINVAL, "unknown interpolation strategy");
     if (hmode < 0 || hmode > 2) return fail(c, PSB_EINVAL, "unknown smoothing-length mode");
     const bool line = rq0.line;
@@ -266,10 +271,11 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             J.sv = tree_view<double>(c->sctx);
             J.lam = lams;
             const unsigned g = (unsigned)((n + 127) / 128);
-            if (kcl == 1) launch_adj_points_k<1>(J, st, scal, g, s);
-            else if (kcl == 2) launch_adj_points_k<2>(J, st, scal, g, s);
-            else if (kcl == 4) launch_adj_points_k<4>(J, st, scal, g, s);
-            else launch_adj_points_k<8>(J, st, scal, g, s);
+            const int kf = (c->kern == PSB_KERNEL_M4) ? 0 : 1;
+            if (kcl == 1) launch_adj_points_k<1>(J, st, scal, kf, g, s);
+            else if (kcl == 2) launch_adj_points_k<2>(J, st, scal, kf, g, s);
+            else if (kcl == 4) launch_adj_points_k<4>(J, st, scal, kf, g, s);
+            else launch_adj_points_k<8>(J, st, scal, kf, g, s);
             PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
             launches += 2;
         } else {

@@ -1,5 +1,6 @@
-// k_adjoint.cuh -- adjoint (vector-Jacobian product) kernels (M4 kernel: its
-// support 2 and Hessian are written out below; the host refuses other kernels).
+// k_adjoint.cuh -- adjoint (vector-Jacobian product) kernels for every kernel
+// family: M4's Hessian is written out below (m4_whess), the others take f'/q
+// and its q-derivative from kern_g12; the support K enters every radius rule.
 //
 // For a loss L = sum_s sum_k gout_k(s) out_k(s) the forward pass in FP64 first
 // writes, per sample, the cotangents lambda of its sums (S1, G, Dm, Dg, Sw_c,
@@ -85,6 +86,34 @@ __device__ __forceinline__ void m4_whess(const double dl[3], double r, double ir
     H[3] = e * dl[0] * dl[1]; H[4] = e * dl[0] * dl[2]; H[5] = e * dl[1] * dl[2];
 }
 
+// The same for a kernel other than M4 (id k, 3D norm sig): f from kern_fdf,
+// g1 = f'(q)/q and g2 = d g1/dq from kern_g12, with 1/q = h ir.
+template <bool HESS = true>
+__device__ __forceinline__ void kern_whess(int k, double sig, const double dl[3], double r, double ir, double h,
+                                           double invh, double& W, double g[3], double H[6]) {
+    const double q = r * invh;
+    double f, df, g1, g2;
+    kern_fdf<double>(k, q, f, df);
+    kern_g12(k, q, h * ir, g1, g2);
+    const double ih3 = invh * invh * invh, ih5 = ih3 * invh * invh;
+    W = sig * ih3 * f;
+    const double c = sig * ih5 * g1;
+    g[0] = c * dl[0]; g[1] = c * dl[1]; g[2] = c * dl[2];
+    if (!HESS) return;
+    const double e = sig * ih5 * g2 * q * (ir * ir);  // 0 at r = 0 (ir = 0)
+    H[0] = c + e * dl[0] * dl[0]; H[1] = c + e * dl[1] * dl[1]; H[2] = c + e * dl[2] * dl[2];
+    H[3] = e * dl[0] * dl[1]; H[4] = e * dl[0] * dl[2]; H[5] = e * dl[1] * dl[2];
+}
+
+// W, gradW (and H) of the context's kernel: KF = 0 is the M4 code, KF = 1 any
+// other family (the warp-uniform id in pt.kern)
+template <int KF, bool HESS>
+__device__ __forceinline__ void whess(const TreeView<double>& pt, const double dl[3], double r, double ir, double h,
+                                      double invh, double& W, double g[3], double H[6]) {
+    if constexpr (KF == 0) m4_whess<HESS>(dl, r, ir, h, invh, W, g, H);
+    else kern_whess<HESS>(pt.kern, (double)pt.sig, dl, r, ir, h, invh, W, g, H);
+}
+
 __device__ __forceinline__ void hmul(const double H[6], const double v[3], double o[3]) {
     o[0] = H[0] * v[0] + H[3] * v[1] + H[4] * v[2];
     o[1] = H[3] * v[0] + H[1] * v[1] + H[5] * v[2];
@@ -104,7 +133,7 @@ struct AStage {
 // lambda_S1 and lambda_Sw_c can be non-zero: the pair terms drop the Hessian
 // and the gradient cotangents (the same values as the general form, which
 // adds exact zeros).
-template <int ST, int KC, bool SCAL>
+template <int ST, int KC, bool SCAL, int KF>
 __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs A) {
     __shared__ AStage stage_all[4];
     const TreeView<double>& pt = A.pt;
@@ -126,8 +155,13 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         for (int c = 0; c < KC; ++c)
             if (c < A.kc) Ab[c] = A.colT[c][b];
     }
+    // the support K (2 for M4) in double and float, and the float margin of
+    // K h: 2 h is exact in float, K h in general one rounding away
+    const double Kd = (KF == 0) ? 2.0 : pt.Kd;
+    const float Kf = (KF == 0) ? 2.f : pt.Kf;
+    const float km = (KF == 0) ? 2.f * U1 : 3.f * U1;
     // this particle's own support radius^2, with the forward's operation order
-    const double rb = X<double>::mul(2.0, hb);
+    const double rb = X<double>::mul(Kd, hb);
     const double rb2 = X<double>::mul(rb, rb);
     // float pair tests against a band (as in the forward's float walk): the
     // particle relative to the warp anchor (the first valid particle) with its
@@ -170,13 +204,13 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         const double r = r2 * ir;
         double W, g[3], H[6];
         if (ST == ST_GATHER) {
-            m4_whess<!SCAL>(dl, r, ir, ha, iha, W, g, H);
+            whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, W, g, H);
         } else if (ST == ST_SCATTER) {
-            m4_whess<!SCAL>(dl, r, ir, hb, ihb, W, g, H);
+            whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, W, g, H);
         } else {
             double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
-            m4_whess<!SCAL>(dl, r, ir, ha, iha, Wa, ga3, Ha);
-            m4_whess<!SCAL>(dl, r, ir, hb, ihb, Wb, gb3, Hb);
+            whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, Wa, ga3, Ha);
+            whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, Wb, gb3, Hb);
             W = 0.5 * (Wa + Wb);
             for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
             if (!SCAL)
@@ -236,7 +270,7 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     constexpr int SN = (ST == ST_GATHER) ? ST_SCATTER : ((ST == ST_SCATTER) ? ST_GATHER : ST_SYMMETRIC);
     auto node_fn = [&](int ni) -> bool {
         const float4 lo = __ldg(&sv.node_lo[ni]), hi = __ldg(&sv.node_hi[ni]);
-        return !(lb_d2_pbox(pf, pem, lo, hi) > hi_r2_node<SN>(rb2_hi, lo.w, 2.f));
+        return !(lb_d2_pbox(pf, pem, lo, hi) > hi_r2_node<SN>(rb2_hi, lo.w, Kf));
     };
     auto span_fn = [&](int64_t lo, int cnt, bool part) {
         const unsigned parts = __ballot_sync(PSB_FULL, part);
@@ -252,12 +286,12 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         const float2 sb = __ldg(&sv.spanb[lo]);
         const float eqm = U1 * (2.f * sb.x + 2.f * (fabsf(o0) + fabsf(o1) + fabsf(o2))) * (1.f + 4.f * U1);
         float rmax = rbmax;
-        if (ST != ST_SCATTER) rmax = fmaxf(rmax, 2.f * sb.y * (1.f + 2.f * U1));
+        if (ST != ST_SCATTER) rmax = fmaxf(rmax, Kf * sb.y * (1.f + km));
         const float E = 1.7320508f * (esmax + eqm) + 4.f * U1 * rmax + 1e-30f;
         // squared radius thresholds of this lane's particle and of sample
         // `lane` (surely in: d2 < A; maybe in: d2 <= B)
         float As = 0.f, Bs = 0.f, Aj = 0.f, Bj = 0.f;
-        if (ST != ST_GATHER) {  // the particle's own radius 2 h_b
+        if (ST != ST_GATHER) {  // the particle's own radius K h_b
             const float il = fmaxf((rblo - E) * (1.f - 4.f * U1), 0.f), ih = (rbhi + E) * (1.f + 4.f * U1);
             As = il * il;
             Bs = ih * ih;
@@ -271,8 +305,8 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             const float4 Lq = __ldg(&sv.leaf4[lo + lane]);
             Qme = make_float4(Lq.x + o0, Lq.y + o1, Lq.z + o2, Lq.w);
             st.Q[lane] = Qme;
-            if (ST != ST_SCATTER) {  // the sample's radius 2 h_a
-                const float rahi = 2.f * Lq.w * (1.f + 2.f * U1), ralo = 2.f * Lq.w * (1.f - 2.f * U1);
+            if (ST != ST_SCATTER) {  // the sample's radius K h_a
+                const float rahi = Kf * Lq.w * (1.f + km), ralo = Kf * Lq.w * (1.f - km);
                 const float il = fmaxf((ralo - E) * (1.f - 4.f * U1), 0.f), ih = (rahi + E) * (1.f + 4.f * U1);
                 Aj = il * il;
                 Bj = ih * ih;
@@ -322,10 +356,10 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         for (unsigned u = maybe & ~acc; u; u &= u - 1) {
             const int jj = __ffs(u) - 1;
             const double ps[3] = {st.sx[jj], st.sy[jj], st.sz[jj]};
-            const double ra = X<double>::mul(2.0, st.sh[jj]);
+            const double ra = X<double>::mul(Kd, st.sh[jj]);
             const double ra2 = X<double>::mul(ra, ra);
             const double e2 = ex_d2_pp<double>(ps, xb[0], xb[1], xb[2]);
-            if (e2 <= ex_r2<ST, double>(ra2, hb, 2.0)) acc |= 1u << jj;
+            if (e2 <= ex_r2<ST, double>(ra2, hb, Kd)) acc |= 1u << jj;
         }
         for (; acc; acc &= acc - 1) {
             const int jj = __ffs(acc) - 1;
@@ -359,12 +393,12 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
 }
 
 // line-integrated kernel and its r-derivative: the slope of the table segment
-// that line_W interpolates on
-__device__ __forceinline__ void line_Wd(double r, double h, const double* lut, double& W, double& dW) {
+// that line_W interpolates on (LUT_N entries over [0, K], K the support)
+__device__ __forceinline__ void line_Wd(double r, double h, const double* lut, double K, double& W, double& dW) {
     const double invh = 1.0 / h;
     const double q = r * invh;
-    if (q >= 2.0) { W = 0.0; dW = 0.0; return; }
-    const double dq = 2.0 / 4095.0;
+    if (q >= K) { W = 0.0; dW = 0.0; return; }
+    const double dq = K / (double)(LUT_N - 1);
     const double idxf = q / dq + 1.0;
     int i = (int)idxf;
     i = i < 1 ? 1 : (i > LUT_N - 1 ? LUT_N - 1 : i);
@@ -390,7 +424,8 @@ __global__ void __launch_bounds__(128) k_adj_beam(const AdjArgs A) {
     const double v[3] = {xb[0] - f[0], xb[1] - f[1], xb[2] - f[2]};
     const double xi = v[0] * f[3] + v[1] * f[4] + v[2] * f[5];
     const double eta = v[0] * f[6] + v[1] * f[7] + v[2] * f[8];
-    const double R = 2.0 * fmax(hb, A.ha_max) * (1.0 + 1e-9) + 1e-300;
+    const double K = pt.Kd;  // the support (2 for M4)
+    const double R = K * fmax(hb, A.ha_max) * (1.0 + 1e-9) + 1e-300;
     const double dxi = (B.params[1] - B.params[0]) / (double)(B.nx - 1);
     const double deta = (B.params[3] - B.params[2]) / (double)(B.ny - 1);
     auto range = [](double c, double R, double lo0, double d, int64_t n, int64_t& a, int64_t& z) {
@@ -404,8 +439,6 @@ __global__ void __launch_bounds__(128) k_adj_beam(const AdjArgs A) {
     int64_t i0, i1, j0, j1;
     range(xi, R, B.params[0], dxi, B.nx, i0, i1);
     range(eta, R, B.params[2], deta, B.ny, j0, j1);
-    const double rb = X<double>::mul(2.0, hb);
-    (void)rb;
     double gm = 0.0, gx[3] = {0.0, 0.0, 0.0}, ga[KC];
 #pragma unroll
     for (int c = 0; c < KC; ++c) ga[c] = 0.0;
@@ -418,21 +451,21 @@ __global__ void __launch_bounds__(128) k_adj_beam(const AdjArgs A) {
             sample_coords(B, k, o, m);
             double ha = 0.0;
             if (ST != ST_SCATTER) ha = (A.hmode == PSB_H_PER_SAMPLE) ? A.hs[k] : A.hs[0];
-            const double ra = X<double>::mul(2.0, ha);
+            const double ra = X<double>::mul(K, ha);
             const double ra2 = X<double>::mul(ra, ra);
             const double e2 = ex_d2_line<double>(o, m, xb[0], xb[1], xb[2]);
-            if (!(e2 <= ex_r2<ST, double>(ra2, hb, 2.0))) continue;
+            if (!(e2 <= ex_r2<ST, double>(ra2, hb, K))) continue;
             ++n_pairs;
             const double dr = sqrt(e2 < 0.0 ? 0.0 : e2);
             double W, dW;
             if (ST == ST_GATHER) {
-                line_Wd(dr, ha, A.lut, W, dW);
+                line_Wd(dr, ha, A.lut, K, W, dW);
             } else if (ST == ST_SCATTER) {
-                line_Wd(dr, hb, A.lut, W, dW);
+                line_Wd(dr, hb, A.lut, K, W, dW);
             } else {
                 double Wa, da, Wb, db;
-                line_Wd(dr, ha, A.lut, Wa, da);
-                line_Wd(dr, hb, A.lut, Wb, db);
+                line_Wd(dr, ha, A.lut, K, Wa, da);
+                line_Wd(dr, hb, A.lut, K, Wb, db);
                 W = 0.5 * (Wa + Wb);
                 dW = 0.5 * (da + db);
             }

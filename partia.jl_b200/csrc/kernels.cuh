@@ -2,8 +2,9 @@
 // (kernel_function/kernels/M5_spline.jl, M6_spline.jl, C2_Wendland.jl,
 // C4_Wendland.jl, C6_Wendland.jl): support K in units of h
 // (KernelFunctionValid), the 3D norm (KernelFunctionnorm(K, Val(3), T)) and
-// f, f' of the dimensionless kernel.  Ids follow psb_kernel.  M4 keeps its own
-// functions (m4_fdf, m4_fdf_edge in interp.cuh).
+// f, f' of the dimensionless kernel (and f'/q with its q-derivative for the
+// adjoint).  Ids follow psb_kernel.  M4 keeps its own functions (m4_fdf,
+// m4_fdf_edge in interp.cuh, m4_whess in k_adjoint.cuh).
 #pragma once
 
 namespace psb {
@@ -162,6 +163,67 @@ __device__ __forceinline__ void kern_fdf_f32(int k, float q, float r, float num,
     default:
         break;
     }
+}
+
+// g1 = f'(q)/q and g2 = d g1/dq for k != M4 (the adjoint's gradient and
+// Hessian factors): g2 = (f'' - g1)/q on the pieces away from q = 0; the
+// pieces that contain q = 0 are written without the division (M5 on q < 1/2
+// and M6 on q < 1 are even polynomials there; the Wendland f' = q P(q) a^n
+// factor exactly).  iq = 1/q (unused where q = 0 is possible).
+__device__ __forceinline__ void kern_g12(int k, double q, double iq, double& g1, double& g2) {
+    g1 = 0.0;
+    g2 = 0.0;
+    double d1 = 0.0, d2 = 0.0;
+    switch (k) {
+    case KERN_M5: {
+        if (q < 0.5) { g1 = -30.0 + 24.0 * q * q; g2 = 48.0 * q; return; }
+        const double a = 2.5 - q, b = 1.5 - q;
+        if (q < 1.5) {
+            d1 = -4.0 * (a * a * a) + 20.0 * (b * b * b);
+            d2 = 12.0 * (a * a) - 60.0 * (b * b);
+        } else if (q < 2.5) {
+            d1 = -4.0 * (a * a * a);
+            d2 = 12.0 * (a * a);
+        } else {
+            return;
+        }
+        break;
+    }
+    case KERN_M6: {
+        if (q < 1.0) { g1 = -120.0 + q * q * (120.0 - 50.0 * q); g2 = q * (240.0 - 150.0 * q); return; }
+        const double a = 3.0 - q, b = 2.0 - q;
+        const double a2 = a * a, b2 = b * b;
+        if (q < 2.0) {
+            d1 = -5.0 * (a2 * a2) + 30.0 * (b2 * b2);
+            d2 = 20.0 * (a2 * a) - 120.0 * (b2 * b);
+        } else if (q < 3.0) {
+            d1 = -5.0 * (a2 * a2);
+            d2 = 20.0 * (a2 * a);
+        } else {
+            return;
+        }
+        break;
+    }
+    case KERN_C2: case KERN_C4: case KERN_C6: {
+        if (!(q < 2.0)) return;
+        const double a = 1.0 - 0.5 * q, a2 = a * a, a3 = a2 * a, a4 = a2 * a2;
+        if (k == KERN_C2) {         // f' = -5 q a^3
+            g1 = -5.0 * a3;
+            g2 = 7.5 * a2;
+        } else if (k == KERN_C4) {  // f' = -14/3 q (1 + 5q/2) a^5
+            g1 = (-14.0 / 3.0) * (1.0 + 2.5 * q) * (a4 * a);
+            g2 = 35.0 * q * a4;
+        } else {                    // f' = -11/2 q (1 + 7q/2 + 4q^2) a^7
+            g1 = -5.5 * (1.0 + 3.5 * q + 4.0 * q * q) * (a4 * a3);
+            g2 = 33.0 * q * (1.0 + 3.0 * q) * (a3 * a3);
+        }
+        return;
+    }
+    default:
+        return;
+    }
+    g1 = d1 * iq;
+    g2 = (d2 - g1) * iq;
 }
 
 }  // namespace psb

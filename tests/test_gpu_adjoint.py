@@ -2,7 +2,8 @@
 
 dL/dm, dL/dA_c and dL/dx for L = sum_k sum_s gout[k][s] out_k(s): point
 samples for every strategy and h mode, every output kind; structured grids;
-parallel-beam line-integrated samples.  The GPU sums the pair terms per
+parallel-beam line-integrated samples; each of the kernel families M5, M6 and
+Wendland C2/C4/C6 besides M4.  The GPU sums the pair terms per
 particle over an LBVH of the samples (or the pixel lattice); the oracle sums
 them per sample.  Tolerance: 1e-10 of each gradient array's max |value| (the
 two sum in different orders).
@@ -35,11 +36,11 @@ def particles(n, seed):
     return [x, y, z, m, h, rho], cols
 
 
-def setup(n, seed):
+def setup(n, seed, kernel=L.PSB_KERNEL_M4):
     arrs, cols = particles(n, seed)
-    orc = O.Oracle(*arrs, cols=cols)
+    orc = O.Oracle(*arrs, cols=cols, kernel=kernel)
     ctx = Context(0)
-    ctx.set_particles(*arrs, cols=cols)
+    ctx.set_particles(*arrs, cols=cols, kernel=kernel)
     ctx.build(want_perm=False)
     return orc, ctx
 
@@ -72,6 +73,50 @@ def test_point_adjoint_matches_oracle(strategy, hmode):
     gout = [rng.standard_normal(ns) for _ in range(nl)]
     r = orc.adjoint_points(*s, O.Catalog(**CAT), gout, strategy=strategy, hmode=hmode, hs=hs)
     g = ctx.adjoint_points(*s, CatalogC(**CAT), gout, strategy=strategy, hmode=hmode, hs=hs)
+    compare(g, r, 4)
+    assert ctx.last_stats.pairs > 0
+
+
+KERNELS = [L.PSB_KERNEL_M5, L.PSB_KERNEL_M6, L.PSB_KERNEL_C2, L.PSB_KERNEL_C4, L.PSB_KERNEL_C6]
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+@pytest.mark.parametrize("strategy,hmode,spec", [
+    (L.PSB_SYMMETRIC, L.PSB_H_NEAREST, CAT),
+    (L.PSB_GATHER, L.PSB_H_PER_SAMPLE, CAT),
+    (L.PSB_SCATTER, L.PSB_H_NEAREST, dict(scalars=[0, 2], shepard=[1, 0]))])  # scalar catalog: no Hessian
+def test_point_adjoint_kernel_families(kernel, strategy, hmode, spec):
+    orc, ctx = setup(5000, 121, kernel)
+    rng = np.random.default_rng(122)
+    ns = 2000
+    s = tuple(rng.uniform(-0.05, 1.05, ns) for _ in range(3))
+    hs = rng.uniform(0.02, 0.05, ns) if hmode == L.PSB_H_PER_SAMPLE else None
+    nl = O.Catalog(**spec).L
+    gout = [rng.standard_normal(ns) for _ in range(nl)]
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=strategy, hmode=hmode, hs=hs)
+    g = ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy, hmode=hmode, hs=hs)
+    compare(g, r, 4)
+    assert ctx.last_stats.pairs > 0
+
+
+@pytest.mark.parametrize("kernel", KERNELS)
+def test_beam_adjoint_kernel_families(kernel):
+    from partia_b200 import workloads as W
+    orc, ctx = setup(6000, 123, kernel)
+    fr = W.Frame((0.5, 0.5, 0.5), (0.3, -0.2, 1.0), (1.0, 0.0, -0.3))
+    farr = fr.as_array()
+    prm = np.array([-0.35, 0.3, -0.25, 0.3])
+    nx, ny = 30, 27
+    nl = nx * ny
+    rng = np.random.default_rng(124)
+    scal, shep = [0, 1], [0, 1]
+    gout = [rng.standard_normal(nl) for _ in scal]
+    hs = np.array([0.03])
+    ox = W.plane_coordinates(farr, (prm[0], prm[1], nx), (prm[2], prm[3], ny))
+    fw = tuple(np.full(nl, farr[9 + c]) for c in range(3))
+    r = orc.adjoint_lines(ox, fw, scal, gout, shepard=shep, strategy=O.SYMMETRIC, hmode=O.H_CONSTANT, hs=hs)
+    g = ctx.adjoint_beam(farr, prm, nx, ny, CatalogC(scalars=scal, shepard=shep), gout, strategy=L.PSB_SYMMETRIC,
+                         hmode=L.PSB_H_CONSTANT, hs=hs)
     compare(g, r, 4)
     assert ctx.last_stats.pairs > 0
 

@@ -540,9 +540,9 @@ def test_kernel_families(kid, strategy):
                 assert rel_err(gl[k], lref[k]) <= tol, (prec, k, rel_err(gl[k], lref[k]))
 
 
-def test_kernel_family_float_inputs_and_adjoint_refusal():
+def test_kernel_family_float_inputs_and_adjoint_dtype_refusal():
     """Float particle data with the M6 kernel (the reference's Float32
-    arithmetic), and the adjoint's refusal of a kernel other than M4."""
+    arithmetic), and the adjoint's refusal of float particle data."""
     arrs, cols = make_particles(20_000, 97, np.float32)
     orc = O.Oracle(*arrs, cols=cols, dtype=np.float32, kernel=L.PSB_KERNEL_M6)
     ctx = Context(0)
@@ -556,8 +556,6 @@ def test_kernel_family_float_inputs_and_adjoint_refusal():
                           prec=L.PSB_PREC_FP64)
     for k in range(len(ref)):
         assert rel_err(g[k], ref[k]) <= 2e-4, (k, rel_err(g[k], ref[k]))
-    a64, c64 = make_particles(2000, 99)
-    ctx.set_particles(*a64, cols=c64, kernel=L.PSB_KERNEL_C2)
-    ctx.build(want_perm=False)
-    with pytest.raises(L.PsbError):
+    with pytest.raises(L.PsbError) as e:
         ctx.adjoint_points(np.array([0.5]), np.array([0.5]), np.array([0.5]), CatalogC(scalars=[0]), [np.ones(1)])
+    assert e.value.code == L.PSB_EUNSUPPORTED

@@ -4,7 +4,8 @@ The reference has no adjoint.  The oracle's vector-Jacobian product (the
 checker of the GPU adjoint) is pinned here by central differences of the
 restated forward pass for L = sum_k sum_s gout[k][s] out_k(s), with respect to
 particle masses, columns and positions, for point samples (all three
-strategies, every output kind, given h_a) and for line-integrated samples.
+strategies, every output kind, given h_a) and for line-integrated samples,
+with the M4 kernel and with each of M5, M6 and Wendland C2/C4/C6.
 Position steps re-run the LBVH build on the perturbed coordinates.
 """
 import numpy as np
@@ -25,8 +26,8 @@ def particles(n, seed):
     return [x, y, z, m, h, rho], cols
 
 
-def loss_points(arrs, cols, s, cat, gout, strategy, hs):
-    orc = O.Oracle(*arrs, cols=cols)
+def loss_points(arrs, cols, s, cat, gout, strategy, hs, kernel=O.M4):
+    orc = O.Oracle(*arrs, cols=cols, kernel=kernel)
     out = orc.interp_points(*s, O.Catalog(**cat), strategy=strategy, hmode=O.H_PER_SAMPLE, hs=hs)
     return sum(float(np.sum(np.nan_to_num(o) * g)) for o, g in zip(out, gout))
 
@@ -35,8 +36,10 @@ def fd(fun, base, eps):
     return (fun(base + eps) - fun(base - eps)) / (2 * eps)
 
 
-@pytest.mark.parametrize("strategy", [O.GATHER, O.SCATTER, O.SYMMETRIC])
-def test_point_adjoint_matches_central_differences(strategy):
+@pytest.mark.parametrize("strategy,kernel", [(O.GATHER, O.M4), (O.SCATTER, O.M4), (O.SYMMETRIC, O.M4),
+                                             (O.SYMMETRIC, O.M5), (O.SYMMETRIC, O.M6), (O.GATHER, O.C2),
+                                             (O.SYMMETRIC, O.C4), (O.SCATTER, O.C6)])
+def test_point_adjoint_matches_central_differences(strategy, kernel):
     arrs, cols = particles(500, 11)
     rng = np.random.default_rng(12)
     ns = 80
@@ -44,7 +47,7 @@ def test_point_adjoint_matches_central_differences(strategy):
     hs = rng.uniform(0.06, 0.1, ns)
     L = O.Catalog(**CAT).L
     gout = [rng.standard_normal(ns) for _ in range(L)]
-    orc = O.Oracle(*arrs, cols=cols)
+    orc = O.Oracle(*arrs, cols=cols, kernel=kernel)
     g = orc.adjoint_points(*s, O.Catalog(**CAT), gout, strategy=strategy, hmode=O.H_PER_SAMPLE, hs=hs)
     # particles that sit inside some support
     cand = np.flatnonzero(np.abs(g["m"]) > 0)
@@ -53,12 +56,12 @@ def test_point_adjoint_matches_central_differences(strategy):
         def with_arr(k, eps):
             a2 = [a.copy() for a in arrs]
             a2[k][b] += eps
-            return loss_points(a2, cols, s, CAT, gout, strategy, hs)
+            return loss_points(a2, cols, s, CAT, gout, strategy, hs, kernel)
 
         def with_col(c, eps):
             c2 = [cc.copy() for cc in cols]
             c2[c][b] += eps
-            return loss_points(arrs, c2, s, CAT, gout, strategy, hs)
+            return loss_points(arrs, c2, s, CAT, gout, strategy, hs, kernel)
 
         em = 1e-6 * arrs[3][b]
         assert fd(lambda e: with_arr(3, e), 0.0, em) == pytest.approx(g["m"][b], rel=1e-5, abs=1e-7 * abs(g["m"]).max())
@@ -70,7 +73,8 @@ def test_point_adjoint_matches_central_differences(strategy):
             assert got == pytest.approx(g["cols"][c][b], rel=1e-5, abs=1e-8 * abs(g["cols"][c]).max() + 1e-14)
 
 
-def test_line_adjoint_matches_central_differences():
+@pytest.mark.parametrize("kernel", [O.M4, O.M5, O.C4])
+def test_line_adjoint_matches_central_differences(kernel):
     arrs, cols = particles(600, 21)
     rng = np.random.default_rng(22)
     nl = 120
@@ -82,11 +86,11 @@ def test_line_adjoint_matches_central_differences():
     gout = [rng.standard_normal(nl) for _ in scal]
 
     def loss(a2, c2):
-        orc = O.Oracle(*a2, cols=c2)
+        orc = O.Oracle(*a2, cols=c2, kernel=kernel)
         out = orc.interp_lines(o, tuple(d), scal, shepard=shep, strategy=O.SCATTER)
         return sum(float(np.sum(np.nan_to_num(v) * g)) for v, g in zip(out, gout))
 
-    orc = O.Oracle(*arrs, cols=cols)
+    orc = O.Oracle(*arrs, cols=cols, kernel=kernel)
     g = orc.adjoint_lines(o, tuple(d), scal, gout, shepard=shep, strategy=O.SCATTER)
     cand = np.flatnonzero(np.abs(g["m"]) > 0)
     assert len(cand) > 50

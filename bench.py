@@ -331,12 +331,17 @@ def kernel_families(d, axis, steps, warmup):
     """The Plummer workload (8 fields, symmetric, nearest h, 128^3 grid) with
     each kernel family of kernels/*.jl: FP32C and FP64 device time, accepted
     pairs (the support K h sets the neighbour count) and the largest FP32C vs
-    FP64 field error."""
+    FP64 field error; and the adjoint of L = sum_k <gout_k, out_k> (seeded
+    normal gout, all 8 fields, the gradients with respect to m_b, A_b and r_b)
+    against the FP32C forward.  Every field is linear in the columns, so
+    sum_c <dL/dA_c, A_c> = L at any size: its relative residual is reported."""
     import torch
     from partia_b200 import _lib as L
     from partia_b200.engine import CatalogC, Context
     stream = torch.cuda.Stream()
     cat = CatalogC(**CATALOG)
+    colsd = [torch.from_numpy(np.ascontiguousarray(d[k])).cuda() for k in ("rho", "Ax", "Ay", "Az")]
+    gen = torch.Generator(device="cuda").manual_seed(7)
     names = ["M4_spline", "M5_spline", "M6_spline", "C2_Wendland", "C4_Wendland", "C6_Wendland"]
     ns = len(axis) ** 3
     res = {}
@@ -359,11 +364,23 @@ def kernel_families(d, axis, steps, warmup):
             nan_diff += int((fa != fb).sum())
             both = fa & fb
             errs.append(((a[both] - b[both]).abs().max() / b[both].abs().max()).item() if both.any() else 0.0)
+        pairs = int(ctx.last_stats.pairs)
+        gout = [torch.randn(ns, generator=gen, device="cuda", dtype=torch.float64) for _ in range(L_OUT)]
+        g = {}
+
+        def bwd():
+            g.update(ctx.adjoint_grid(axis, axis, axis, cat, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                                      device=True))
+        t_bwd = timed_call(bwd, stream, 3, 2)
+        lhs = float(sum((gc * c).sum() for gc, c in zip(g["cols"], colsd)))
+        rhs = float(sum((go * torch.nan_to_num(o, nan=0.0)).sum() for go, o in zip(gout, outs[L.PSB_PREC_FP64])))
         res[name] = {"fp32c_ms": t[L.PSB_PREC_FP32C], "fp64_ms": t[L.PSB_PREC_FP64],
                      "samples_per_s": ns / (t[L.PSB_PREC_FP32C] / 1e3),
                      "speedup_fp32c_vs_fp64": t[L.PSB_PREC_FP64] / t[L.PSB_PREC_FP32C],
-                     "pairs": int(ctx.last_stats.pairs), "max_fp32c_rel_err_vs_fp64": max(errs),
-                     "nan_mask_differences": nan_diff}
+                     "pairs": pairs, "max_fp32c_rel_err_vs_fp64": max(errs),
+                     "nan_mask_differences": nan_diff,
+                     "adjoint_ms": t_bwd, "grad_fwd_time_ratio": t_bwd / t[L.PSB_PREC_FP32C],
+                     "adjoint_linearity_in_A_rel_residual": abs(lhs - rhs) / abs(rhs)}
         ctx.close()
     return res
 

@@ -133,9 +133,23 @@ struct AStage {
 // lambda_S1 and lambda_Sw_c can be non-zero: the pair terms drop the Hessian
 // and the gradient cotangents (the same values as the general form, which
 // adds exact zeros).
+// A pair reads 8 + 4 kc sum cotangents of its sample (1 + kc for scalar
+// catalogs: lambda_S1 and lambda_Sw_c).  Every particle of the warp that pairs
+// with a sample reads the same ones, so they are staged in shared memory once
+// per span, one coalesced load per row.  The general form stages up to 4
+// columns (24 rows of 32 doubles per warp); with 8 it would pass the 48 KB of
+// static shared memory of a block and reads them from global memory instead.
+template <int KC, bool SCAL> struct ALam {
+    double q[(SCAL ? 1 + KC : 8 + 4 * KC) * SPAN];  // staged row r of span sample j at r * SPAN + j
+};
+// the cotangent row (in A.lam) of staged row r
+template <bool SCAL> __device__ __forceinline__ int lam_row(int r) { return SCAL ? (r == 0 ? 0 : 7 + r) : r; }
+
 template <int ST, int KC, bool SCAL, int KF>
 __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs A) {
     __shared__ AStage stage_all[4];
+    constexpr bool STAGE = SCAL || KC <= 4;
+    __shared__ ALam<STAGE ? KC : 1, SCAL> lam_all[STAGE ? 4 : 1];
     const TreeView<double>& pt = A.pt;
     const TreeView<double>& sv = A.sv;
     const int lane = threadIdx.x & 31;
@@ -196,7 +210,9 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     unsigned long long n_pairs = 0, n_spans = 0, n_parts = 0, n_leaves = 0;  // work counters (warp-uniform)
     int64_t steps = 0;
 
-    auto pair = [&](int64_t li, double sxv, double syv, double szv, double ha, double iha) {
+    const double* lst = lam_all[STAGE ? wib : 0].q;  // the span's staged cotangents
+    // li: the sample; jj: its slot in the span
+    auto pair = [&](int64_t li, int jj, double sxv, double syv, double szv, double ha, double iha) {
         ++n_pairs;
         const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
         const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
@@ -216,13 +232,13 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             if (!SCAL)
                 for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
         }
-        const double* lam = A.lam + li;
         if constexpr (SCAL) {
-            double aS = __ldg(&lam[0]);
+            const double* ls = lst + jj;
+            double aS = ls[0];
 #pragma unroll
             for (int c = 0; c < KC; ++c) {
                 if (c < kc) {
-                    const double lsw = __ldg(&lam[(8 + c) * L]);
+                    const double lsw = ls[(1 + c) * SPAN];
                     aS += lsw * Ab[c];
                     sA[c] += lsw * W;
                 }
@@ -231,17 +247,20 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             for (int d = 0; d < 3; ++d) vS[d] += aS * g[d];
             return;
         }
-        const double lS1 = __ldg(&lam[0]);
-        const double lG[3] = {__ldg(&lam[L]), __ldg(&lam[2 * L]), __ldg(&lam[3 * L])};
-        const double lDm = __ldg(&lam[4 * L]);
-        const double lDg[3] = {__ldg(&lam[5 * L]), __ldg(&lam[6 * L]), __ldg(&lam[7 * L])};
+        // row r of this sample: staged, or from global memory
+        const double* ls = STAGE ? lst + jj : A.lam + li;
+        const int64_t rs = STAGE ? (int64_t)SPAN : L;
+        const double lS1 = ls[0];
+        const double lG[3] = {ls[rs], ls[2 * rs], ls[3 * rs]};
+        const double lDm = ls[4 * rs];
+        const double lDg[3] = {ls[5 * rs], ls[6 * rs], ls[7 * rs]};
         double aS = lS1, aG[3] = {lG[0], lG[1], lG[2]};
 #pragma unroll
         for (int c = 0; c < KC; ++c) {
             if (c < kc) {
-                const double lsw = __ldg(&lam[(8 + c) * L]);
-                const double lsg[3] = {__ldg(&lam[(8 + kc + 3 * c) * L]), __ldg(&lam[(9 + kc + 3 * c) * L]),
-                                       __ldg(&lam[(10 + kc + 3 * c) * L])};
+                const double lsw = ls[(8 + c) * rs];
+                const double lsg[3] = {ls[(8 + kc + 3 * c) * rs], ls[(9 + kc + 3 * c) * rs],
+                                       ls[(10 + kc + 3 * c) * rs]};
                 aS += lsw * Ab[c];
                 aG[0] += Ab[c] * lsg[0]; aG[1] += Ab[c] * lsg[1]; aG[2] += Ab[c] * lsg[2];
                 sA[c] += lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2];
@@ -361,10 +380,20 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             const double e2 = ex_d2_pp<double>(ps, xb[0], xb[1], xb[2]);
             if (e2 <= ex_r2<ST, double>(ra2, hb, Kd)) acc |= 1u << jj;
         }
+        if constexpr (STAGE) {  // stage the span's cotangent rows (a warp-uniform decision)
+            if (__any_sync(PSB_FULL, acc != 0)) {
+                double* lw = lam_all[wib].q;
+                const int nq = SCAL ? 1 + kc : 8 + 4 * kc;
+                if (lane < cnt)
+                    for (int r = 0; r < nq; ++r) lw[r * SPAN + lane] = __ldg(&A.lam[lam_row<SCAL>(r) * L + lo + lane]);
+                __syncwarp();
+            }
+        }
         for (; acc; acc &= acc - 1) {
             const int jj = __ffs(acc) - 1;
-            pair(lo + jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj], st.sih[jj]);
+            pair(lo + jj, jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj], st.sih[jj]);
         }
+        if constexpr (STAGE) __syncwarp();  // the rows are read before the next span's
     };
     const int32_t start = (sv.root == 0) ? (int32_t)sv.n : sv.root;
     const bool ok = warp_traverse_spans(start, sv.n, sv.links, sv.escape, valid, node_fn, span_fn, steps);

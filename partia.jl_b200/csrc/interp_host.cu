@@ -415,7 +415,22 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     const size_t es = sizeof(T);
     const int64_t ns = rq.ns;
     const int64_t CH = PIPE_CHUNK;
-    const int64_t nch = (ns + CH - 1) / CH;
+    // Chunk k covers samples [cb[k], cb[k+1]).  The first chunk's copy-in and
+    // the last one's copy-out overlap no kernel, so the two chunks at each end
+    // take a quarter and a half of CH; those between share the rest evenly
+    // (at most CH each).  The caller guarantees ns >= 2 CH.
+    std::vector<int64_t> cb;
+    {
+        const int64_t q = CH / 4, h = CH / 2, mid = ns - 2 * (q + h);
+        const int64_t nm = (mid + CH - 1) / CH;
+        cb.push_back(0);
+        cb.push_back(q);
+        cb.push_back(q + h);
+        for (int64_t i = 1; i <= nm; ++i) cb.push_back(q + h + mid * i / nm);
+        cb.push_back(ns - q);
+        cb.push_back(ns);
+    }
+    const int64_t nch = (int64_t)cb.size() - 1;
     int launches = 0;
 
     Args<T> A;
@@ -497,7 +512,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
 
     for (int64_t k = 0; k < nch; ++k) {
         const int b = (int)(k % PIPE_SETS);
-        const int64_t off = k * CH, cn = std::min<int64_t>(CH, ns - off);
+        const int64_t off = cb[k], cn = cb[k + 1] - cb[k];
         char* ib = inb + es * CH * nin * b;
         // in
         if (k >= PIPE_SETS) PSB_CUDA_TRY(c, cudaStreamWaitEvent(sin, in_free[b], 0), "stream wait");

@@ -232,17 +232,19 @@ def test_two_kernel_path_overflow_tiles(prec):
     assert ctx.last_stats.pairs == int(co.sum())
 
 
-@pytest.mark.parametrize("prec,hmode", [(L.PSB_PREC_FP32C, L.PSB_H_NEAREST), (L.PSB_PREC_FP64, L.PSB_H_PER_SAMPLE)])
-def test_chunked_host_path_matches_device_path(prec, hmode):
-    """A host-memory call of more than two chunks is copied in and out in
-    chunks on copy streams that overlap the kernels; results equal the
-    device-pointer call on the same samples."""
+@pytest.mark.parametrize("prec,hmode,ns", [(L.PSB_PREC_FP32C, L.PSB_H_NEAREST, 1_200_000),
+                                           (L.PSB_PREC_FP64, L.PSB_H_PER_SAMPLE, 1_200_000),
+                                           (L.PSB_PREC_FP32C, L.PSB_H_PER_SAMPLE, 2 ** 20 + 3)])
+def test_chunked_host_path_matches_device_path(prec, hmode, ns):
+    """A host-memory call of at least two chunks of 2^19 samples is copied in
+    and out in chunks (smaller at both ends) on copy streams that overlap the
+    kernels; results equal the device-pointer call on the same samples.
+    2^20 + 3 samples is the smallest such call, with an odd middle chunk."""
     import torch
     arrs, cols = make_particles(20_000, 75)
     ctx = Context(0)
     ctx.set_particles(*arrs, cols=cols)
     ctx.build(want_perm=False)
-    ns = 1_200_000  # 3 chunks of 2^19
     s = _samples(ns, 76)
     hs = np.random.default_rng(77).uniform(0.02, 0.04, ns) if hmode == L.PSB_H_PER_SAMPLE else None
     cat = CatalogC(**CATALOGS["all"])

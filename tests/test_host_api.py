@@ -97,3 +97,23 @@ def test_workload_generators_are_seeded():
     assert np.array_equal(a["x"], b["x"]) and np.all(np.sqrt(a["x"] ** 2 + a["y"] ** 2 + a["z"] ** 2) <= 1.0)
     c = W.clumps(2000, seed=2)
     assert len(c["x"]) == 2000 and c["m"].sum() == pytest.approx(1.0)
+
+
+def test_hs_follows_the_call_pointers_on_the_host():
+    """Context._hs: for a call with host pointers, hs becomes a contiguous
+    host array of the context dtype (lists, scalars and tensors alike)."""
+    import types
+
+    import torch
+    from partia_b200.engine import Context
+    fake = types.SimpleNamespace(dtype=np.dtype(np.float64), device=0)
+    assert Context._hs(fake, 1, None, False) is None
+    a = Context._hs(fake, 1, [0.1, 0.2], False)
+    assert isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+    assert np.array_equal(a, [0.1, 0.2])
+    assert np.array_equal(Context._hs(fake, 2, 0.05, False), [0.05])
+    t = torch.tensor([0.25, 0.5], dtype=torch.float32)
+    b = Context._hs(fake, 1, t, False)
+    assert isinstance(b, np.ndarray) and b.dtype == np.float64 and np.array_equal(b, [0.25, 0.5])
+    fake32 = types.SimpleNamespace(dtype=np.dtype(np.float32), device=0)
+    assert Context._hs(fake32, 1, np.array([0.1, 0.2]), False).dtype == np.float32

@@ -468,6 +468,34 @@ def test_structured_grid_analytic_regression(prec):
             assert np.all(np.abs(g[k] - ref) <= atol + rtol * np.abs(ref)), (st, k)
 
 
+def test_zero_samples_and_zero_particles():
+    """Calls with no samples return empty outputs (points, lines, density,
+    digests, the adjoint with zero gradients); a build over no particles is
+    refused with the reference's error (BinaryRadixTree needs non-empty
+    codes)."""
+    arrs, cols = make_particles(500, 95)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build()
+    e = np.zeros(0)
+    cat = CatalogC(**CATALOGS["all"])
+    for prec in (L.PSB_PREC_FP64, L.PSB_PREC_FP32C):
+        out = ctx.interp_points(e, e, e, cat, strategy=L.PSB_SYMMETRIC, prec=prec)
+        assert len(out) == cat.L and all(len(o) == 0 for o in out)
+    lo = ctx.interp_lines((e, e, e), (e, e, e), CatalogC(scalars=[0, 1], shepard=[0, 1]))
+    assert all(len(o) == 0 for o in lo)
+    assert len(ctx.density(e, e, e, hs=np.array([0.05]), hmode=L.PSB_H_CONSTANT)) == 0
+    cnt, hsh, ha = ctx.digest((e, e, e))
+    assert len(cnt) == 0 and len(hsh) == 0
+    g = ctx.adjoint_points(e, e, e, cat, [e] * cat.L, strategy=L.PSB_SYMMETRIC)
+    assert all(np.all(g[k] == 0) for k in ("m", "x", "y", "z")) and all(np.all(c == 0) for c in g["cols"])
+    empty = [np.zeros(0) for _ in range(6)]
+    ctx.set_particles(*empty, cols=[np.zeros(0)])
+    with pytest.raises(L.PsbError) as err:
+        ctx.build()
+    assert err.value.code == L.PSB_EINVAL and "non-empty" in str(err.value)
+
+
 def test_short_float_line_table():
     """PSB_FLAG_LUT1000_F32: line integrals from the 1000-entry float table
     stay within its interpolation error of the 4096-entry table (spacing

@@ -138,6 +138,27 @@ class ClockSampler:
                 "samples": len(self.samples), "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
+def bench_config():
+    """The workload description both arms print (the driver compares them)."""
+    return {"workload": f"plummer-2M symmetric rho,grad rho,div A,curl A on {NGRID}^3 grid",
+            "N": 2_000_000, "samples": NGRID ** 3, "fields": L_OUT, "strategy": "symmetric",
+            "h": "nearest particle", "l2": "flushed (256 MB write) between GPU steps"}
+
+
+def host_cpu():
+    """nproc and the CPU model name of this host (lscpu)."""
+    model = None
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                model = ln.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"nproc": os.cpu_count(), "model": model}
+
+
 def make_workload():
     from partia_b200 import workloads as W
     from partia_b200 import linrange
@@ -504,9 +525,9 @@ def cpu_reference(args, d, axis, steps, warmup, threads=None):
         if k >= warmup:
             times.append(dt)
     val = ns / float(np.median(times))
-    return dict(value=val, unit=UNIT, cores=nthr, kind="port",
-                sample=f"{ns} random grid points of the 128^3 grid per step (of 2,097,152), FP64 oracle, "
-                       f"median of {steps}; LBVH build {build_s:.2f} s not timed"), times
+    return dict(value=val, unit=UNIT, cores=nthr, kind="port", host=host_cpu(),
+                sample=f"{ns} random grid points of the {NGRID}^3 grid per step (of {NGRID ** 3:,}), FP64 oracle, "
+                       f"median of {steps} steps after {warmup} warm-up; LBVH build {build_s:.2f} s not timed"), times
 
 
 def run_reference(args):
@@ -514,13 +535,17 @@ def run_reference(args):
     if rank != 0:
         return
     d, axis = make_workload()
-    cb, times = cpu_reference(args, d, axis, max(args.steps, 1), max(min(args.warmup, 1), 0))
+    steps = max(args.steps, 5)
+    args.cpu_seconds = max(1.0, min(args.cpu_seconds, 150.0 / (steps + 1)))  # whole run within a few minutes
+    cb, times = cpu_reference(args, d, axis, steps, 1)
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(times)),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Plummer sphere, N=2e6)",
-            "config": {"workload": f"plummer-2M symmetric rho,grad rho,div A,curl A on {NGRID}^3 grid", "N": 2_000_000,
-                       "samples": NGRID ** 3},
+            "higher_is_better": True, "scaling": "strong" if args.gpus > 1 else "weak", "vs_baseline": None,
+            "dtype": "f64", "precision": "FP64 (CPU restatement of the reference's algorithm)",
+            "data": "synthetic (seeded Plummer sphere, N=2e6, numpy PCG64 seed 1)",
+            "config": bench_config(),
+            "sampled": "each step times a random subset of the grid's samples and reports it as a rate "
+                       "(see cpu_baseline.sample)",
             "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
                                         "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
@@ -659,20 +684,40 @@ def main():
                           prec=L.PSB_PREC_FP32C, out=houtn)
         return ctx.last_stats
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_ms = []
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
+    def e2e_timed(fn):
+        """Host-clock seconds of each call (after a synchronise), plus the
+        library's own event span of the call."""
+        for _ in range(max(1, args.warmup)):
+            fn()
         torch.cuda.synchronize()
-        st = e2e_step()
-        e2e_ms.append(st.total_ms)
-    e2e_tot = torch.tensor([float(np.sum(e2e_ms))], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_tot, op=dist.ReduceOp.MAX)
-    e2e_val = total_samples * args.steps / (e2e_tot.item() / 1e3)
+        host_s, lib_ms = [], []
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            st = fn()
+            host_s.append(time.perf_counter() - t0)
+            lib_ms.append(st.total_ms)
+        tot = torch.tensor([float(np.sum(host_s))], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(tot, op=dist.ReduceOp.MAX)
+        return total_samples * args.steps / tot.item(), float(np.median(host_s)) * 1e3, float(np.median(lib_ms))
+
+    e2e_val, e2e_host_ms, e2e_lib_ms = e2e_timed(e2e_step)
+    # the same call with pageable numpy buffers (what a Julia caller passes)
+    pxn, pyn, pzn = (np.array(a, copy=True) for a in (hxn, hyn, hzn))
+    poutn = [np.empty(ns, dtype=np.float64) for _ in range(L_OUT)]
+
+    def e2e_pageable():
+        ctx.interp_points(pxn, pyn, pzn, cat, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
+                          prec=L.PSB_PREC_FP32C, out=poutn)
+        return ctx.last_stats
+
+    e2e_pg_val, e2e_pg_host_ms, e2e_pg_lib_ms = e2e_timed(e2e_pageable)
+    for a, b in zip(houtn, poutn):
+        assert np.array_equal(np.isnan(a), np.isnan(b)) and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)]), \
+            "pageable and pinned host calls disagree"
 
     # roofline of the point kernel (algorithmic bytes per launch)
     hbm, peak_kind = peaks()
@@ -697,7 +742,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            cpu, _ = cpu_reference(args, d, axis, 1, 0)
+            cpu, _ = cpu_reference(args, d, axis, 5, 1)
         except Exception as e:  # the oracle build needs g++
             cpu = {"value": None, "unit": UNIT, "cores": None, "kind": "port", "sample": f"failed: {e}"}
 
@@ -705,13 +750,18 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot.item() / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32c",
+            "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32c",
+            "precision": "FP32C (float pair sums with compensated accumulation; double inclusion test and "
+                         "finalisation)",
             "data": "synthetic (seeded Plummer sphere, N=2e6, numpy PCG64 seed 1)",
-            "config": {"workload": f"plummer-2M symmetric rho,grad rho,div A,curl A on {NGRID}^3 grid",
-                       "N": 2_000_000, "samples": NGRID ** 3, "fields": L_OUT, "strategy": "symmetric",
-                       "h": "nearest particle", "precision": "FP32C", "l2": "flushed (256 MB write) between steps"},
+            "config": bench_config(),
             "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": 3 * 8 * ns,
-                    "d2h_bytes_per_step": L_OUT * 8 * ns},
+                    "d2h_bytes_per_step": L_OUT * 8 * ns,
+                    "timing": "host clock (time.perf_counter) around each psb_interp_points call, after a "
+                              "synchronise; pinned host buffers",
+                    "host_ms_per_call": e2e_host_ms, "library_event_ms_per_call": e2e_lib_ms,
+                    "pageable": {"value": e2e_pg_val, "unit": UNIT, "host_ms_per_call": e2e_pg_host_ms,
+                                 "library_event_ms_per_call": e2e_pg_lib_ms}},
             "gpu_launches": int(args.steps * launches_per_step),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
                          "peak_kind": peak_kind,

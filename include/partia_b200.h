@@ -110,6 +110,19 @@ typedef enum { PSB_H_NEAREST = 0, PSB_H_PER_SAMPLE = 1, PSB_H_CONSTANT = 2 } psb
  * come from the same quadrature; the short table adds its interpolation and
  * float rounding error.  No effect on point samples or the adjoint. */
 #define PSB_FLAG_LUT1000_F32 0x400u
+/* Point samples: the density gradient (catalog grad slot -1) in the form of
+ * the standalone _gradient_density_kernel
+ * (src/julia/KernelInterpolation/single_point_interpolation/kernels/gradient_interpolation.jl:1-170):
+ * grad rho = sum m gradW - rho(r) sum (m/rho_b) gradW with the plain density
+ * sum rho(r) = sum m W, NaN where rho(r) = 0; without the flag the catalog
+ * form of general_interpolation.jl:147-169 subtracts the Shepard-normalised
+ * density (sum m W) / S1 instead.  Also honoured by the adjoint calls. */
+#define PSB_FLAG_DENSITY_GRADIENT_PLAIN 0x800u
+/* psb_density only: the number density sum_b W (every mass taken as 1) of
+ * _number_density_kernel
+ * (src/julia/KernelInterpolation/single_point_interpolation/kernels/scalar_interpolation.jl:86-166),
+ * 0 where there is no neighbour. */
+#define PSB_FLAG_NUMBER_DENSITY 0x1000u
 
 /* InterpolationCatalogConcise
  * (src/julia/KernelInterpolation/interpolation_setup/InterpolationCatalog.jl:26-32),
@@ -183,6 +196,20 @@ int psb_set_particles(psb_ctx* ctx, int64_t n, psb_dtype dt,
  * caller that mirrors Partia's in-place contract applies perm_out to its own
  * arrays. */
 int psb_build_lbvh(psb_ctx* ctx, int64_t* perm_out, uint64_t* codes_out);
+
+/* New masses, densities and quantity columns for the particles of a built
+ * LBVH, keeping the tree.  The tree depends on the coordinates and smoothing
+ * lengths only, so an input whose coordinates and h still equal the LBVH's
+ * leaves (matches_lbvh_leaf_order,
+ * src/julia/KernelInterpolation/interpolation_setup/InterpolationInput.jl:265-267)
+ * can be interpolated with that LBVH after only its values are replaced, as
+ * Partia's external-LBVH driver overloads do
+ * (src/julia/KernelInterpolation/grid_interpolation/drivers/PointSamples_driver.jl:98-118).
+ * The arrays hold n values each in the LBVH's leaf (Morton) order, the order
+ * of psb_build_lbvh's perm_out; ncol may differ from psb_set_particles'.
+ * Host pointers unless PSB_FLAG_DEVICE_PTRS. */
+int psb_set_values(psb_ctx* ctx, const void* m, const void* rho,
+                   int32_t ncol, const void* const* cols, uint32_t flags);
 
 /* Tree export for parity checks (LinearBVH fields,
  * src/julia/LinearBoundingVolumeHierarchy/LinearBVH/LinearBVH.jl:8-14).
@@ -260,7 +287,8 @@ int psb_interp_beam(psb_ctx* ctx, const void* frame, const void* params,
                     void* const* out, uint32_t flags, psb_stats* stats);
 
 /* _density_kernel (src/julia/KernelInterpolation/single_point_interpolation/kernels/scalar_interpolation.jl:1-75):
- * sum_b m_b W at each sample, 0 where there is no neighbour. */
+ * sum_b m_b W at each sample, 0 where there is no neighbour.  With
+ * PSB_FLAG_NUMBER_DENSITY: _number_density_kernel (:86-166), sum_b W. */
 int psb_density(psb_ctx* ctx, int64_t ns,
                 const void* sx, const void* sy, const void* sz,
                 psb_hmode hmode, const void* hs, psb_strategy strategy,
@@ -322,6 +350,17 @@ int psb_adjoint_beam(psb_ctx* ctx, const void* frame, const void* params,
                      double* gm, double* const* gcols, double* gx, double* gy, double* gz,
                      uint32_t flags, psb_stats* stats);
 
+/* ---- failure injection (tests) ------------------------------------------------ */
+
+/* No counterpart in the reference, which has no device walks to bound.  For
+ * failure-detection tests: every escape link of the built LBVH that ends a
+ * traversal (the right spine and the last leaf, escape 0) is pointed at the
+ * root.  Node ids stay valid, so every memory access of a walk stays in
+ * bounds; each walk then cycles until its step bound (4n + 8 steps), and the
+ * interpolation, density, digest and adjoint calls return PSB_ETRAVERSAL.
+ * psb_build_lbvh restores a correct tree.  Needs n >= 2. */
+int psb_test_loop_escapes(psb_ctx* ctx);
+
 /* ---- interpolation without device allocation -------------------------------- */
 
 /* No counterpart in the reference: an addition of this library.
@@ -336,13 +375,16 @@ int psb_adjoint_beam(psb_ctx* ctx, const void* frame, const void* params,
  * library.
  *  - ns <= PSB_NOALLOC_MAX_SAMPLES, else PSB_EINVAL (split the call);
  *  - the first call on a device looks the array's address up once, with that
- *    device current; make it before any stream capture begins;
+ *    device current (again after a cudaDeviceReset gives the device a new
+ *    context); make that first call before any stream capture begins;
  *  - all calls on a device share the array: calls whose GPU work overlaps
  *    (several streams or contexts on one device) race and must be serialised
  *    by the caller;
  *  - particles and LBVH must already be on the device (psb_set_particles and
  *    psb_build_lbvh allocate; this call does not).
- * Results equal psb_interp_points' for the same arguments. */
+ * It runs the single-kernel form of the point interpolation
+ * (PSB_FLAG_SINGLE_KERNEL), so its results agree with psb_interp_points' to
+ * rounding. */
 #define PSB_NOALLOC_MAX_SAMPLES 262144
 #define PSB_NOALLOC_SCRATCH_BYTES (8u << 20)
 int psb_interp_points_noalloc(psb_ctx* ctx, int64_t ns,

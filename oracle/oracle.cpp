@@ -863,8 +863,11 @@ static bool interp_line(const Particles<T>& P, const Tree<T>& tr, const Catalog&
 }
 
 // _density_kernel, single_point_interpolation/kernels/scalar_interpolation.jl:1-75
+// (mb * W per pair, accumulations/scalar_accumulation.jl:6-28); with number
+// set, _number_density_kernel (:86-166), W per pair (scalar_accumulation.jl:31-52).
 template <class T>
-static bool density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3], T ha, int mode, T& out) {
+static bool density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3], T ha, int mode, T& out,
+                          bool number = false) {
     const T K = kern_support<T>();
     const T radius = K * ha;
     const T radius2 = radius * radius;
@@ -877,9 +880,48 @@ static bool density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3
             if (mode == GATHER) W = kernel_W(dr, ha);
             else if (mode == SCATTER) W = kernel_W(dr, hb);
             else W = T(0.5) * (kernel_W(dr, ha) + kernel_W(dr, hb));
-            rho += mb * W;
+            rho += number ? W : mb * W;
         });
     out = rho;
+    return ok;
+}
+
+// _gradient_density_kernel, single_point_interpolation/kernels/gradient_interpolation.jl:1-170:
+// f = sum mb gradW, b = sum (mb gradW) / rho_b (accumulations/gradient_accumulation.jl:7-100),
+// rho = sum mb W; NaN if rho == 0, else f - b rho.
+template <class T>
+static bool gradient_density_point(const Particles<T>& P, const Tree<T>& tr, const T pa[3], T ha, int mode, T out[3]) {
+    const T K = kern_support<T>();
+    const T radius = K * ha;
+    const T radius2 = radius * radius;
+    T f[3] = {0, 0, 0}, b[3] = {0, 0, 0}, rho = 0;
+    bool ok = traverse<T, false>(tr, pa, pa, mode, K, [&]() { return radius2; },
+        [&](int64_t li, T d2, T hb) {
+            T dx = pa[0] - P.x[li], dy = pa[1] - P.y[li], dz = pa[2] - P.z[li];
+            T dr = std::sqrt(d2);
+            T mb = P.m[li], invrb = T(1) / P.rho[li];
+            T g[3], W;
+            if (mode == GATHER) {
+                kernel_gradW(dx, dy, dz, ha, g[0], g[1], g[2]);
+                W = kernel_W(dr, ha);
+            } else if (mode == SCATTER) {
+                kernel_gradW(dx, dy, dz, hb, g[0], g[1], g[2]);
+                W = kernel_W(dr, hb);
+            } else {
+                T a[3], c[3];
+                kernel_gradW(dx, dy, dz, ha, a[0], a[1], a[2]);
+                kernel_gradW(dx, dy, dz, hb, c[0], c[1], c[2]);
+                for (int d = 0; d < 3; ++d) g[d] = T(0.5) * (a[d] + c[d]);
+                W = T(0.5) * (kernel_W(dr, ha) + kernel_W(dr, hb));
+            }
+            for (int d = 0; d < 3; ++d) {
+                T mg = mb * g[d];
+                f[d] += mg;
+                b[d] += mg * invrb;
+            }
+            rho += mb * W;
+        });
+    for (int d = 0; d < 3; ++d) out[d] = rho == T(0) ? std::numeric_limits<T>::quiet_NaN() : f[d] - b[d] * rho;
     return ok;
 }
 
@@ -1276,6 +1318,23 @@ ORC_API int orc_build(orc_ctx* c, int64_t* perm, uint64_t* codes) {
     return c->dtype == 0 ? build_impl<double>(c, perm, codes) : build_impl<float>(c, perm, codes);
 }
 
+// Failure injection for the tests: every escape link that ends a walk (0:
+// the right spine and the last leaf) is pointed at the root, so every
+// traversal cycles until its step bound and the call reports it (-5).
+// orc_build restores the tree.
+template <class T> static int loop_escapes_impl(orc_ctx* c) {
+    Tree<T>& tr = tree<T>(c);
+    if (tr.root == 0) return -1;
+    for (auto& e : tr.escape)
+        if (e == 0) e = tr.root;
+    return 0;
+}
+
+ORC_API int orc_test_loop_escapes(orc_ctx* c) {
+    if (!c->built) return -7;
+    return c->dtype == 0 ? loop_escapes_impl<double>(c) : loop_escapes_impl<float>(c);
+}
+
 template <class T> static void get_tree_impl(orc_ctx* c, int32_t* root, int32_t* l, int32_t* r, int32_t* e, int32_t* p,
                                              double* nmin, double* nmax, double* nscale) {
     Tree<T>& tr = tree<T>(c);
@@ -1387,7 +1446,7 @@ ORC_API int orc_interp_lines(orc_ctx* c, int64_t nl, const void* const* od, int 
 }
 
 template <class T> static int density_impl(orc_ctx* c, int64_t ns, const T* sx, const T* sy, const T* sz,
-                                           int hmode, const T* hs, int mode, T* out) {
+                                           int hmode, const T* hs, int mode, T* out, int what) {
     Particles<T>& P = parts<T>(c);
     Tree<T>& tr = tree<T>(c);
     std::atomic<int> bad(0);
@@ -1396,22 +1455,31 @@ template <class T> static int density_impl(orc_ctx* c, int64_t ns, const T* sx, 
         T p[3] = {sx[i], sy[i], sz[i]};
         bool ok1 = true;
         T ha = (mode == SCATTER) ? T(0) : sample_h(tr, p, hmode, hs, i, ok1);
-        T v;
-        bool ok2 = density_point(P, tr, p, ha, mode, v);
+        bool ok2;
+        if (what == 2) {  // gradient of the density: out holds 3 ns values, component-major
+            T g[3];
+            ok2 = gradient_density_point(P, tr, p, ha, mode, g);
+            for (int d = 0; d < 3; ++d) out[d * ns + i] = g[d];
+        } else {
+            T v;
+            ok2 = density_point(P, tr, p, ha, mode, v, what == 1);
+            out[i] = v;
+        }
         if (!ok1 || !ok2) bad = 1;
-        out[i] = v;
     }
     return bad ? -5 : 0;
 }
 
+// what: 0 _density_kernel, 1 _number_density_kernel, 2 _gradient_density_kernel
 ORC_API int orc_density(orc_ctx* c, int64_t ns, const void* sx, const void* sy, const void* sz,
-                int hmode, const void* hs, int mode, void* out) {
+                int hmode, const void* hs, int mode, void* out, int what) {
     if (!c->built) return -7;
+    if (what < 0 || what > 2) return -1;
     if (c->dtype == 0)
         return density_impl<double>(c, ns, (const double*)sx, (const double*)sy, (const double*)sz, hmode,
-                                    (const double*)hs, mode, (double*)out);
+                                    (const double*)hs, mode, (double*)out, what);
     return density_impl<float>(c, ns, (const float*)sx, (const float*)sy, (const float*)sz, hmode,
-                               (const float*)hs, mode, (float*)out);
+                               (const float*)hs, mode, (float*)out, what);
 }
 
 // Neighbour digest through the stackless traversal (kind 0 points, 1 lines).

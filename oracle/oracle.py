@@ -65,6 +65,8 @@ def lib():
         L.orc_destroy.restype = None
         L.orc_build.argtypes = [_vp, _vp, _vp]
         L.orc_build.restype = C.c_int
+        L.orc_test_loop_escapes.argtypes = [_vp]
+        L.orc_test_loop_escapes.restype = C.c_int
         L.orc_get_tree.argtypes = [_vp] * 9
         L.orc_get_tree.restype = C.c_int
         L.orc_interp_points.argtypes = [_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int,
@@ -72,7 +74,7 @@ def lib():
         L.orc_interp_points.restype = C.c_int
         L.orc_interp_lines.argtypes = [_vp, _i64, _vp, C.c_int, _vp, C.c_int, C.c_int, _vp, _vp, _vp]
         L.orc_interp_lines.restype = C.c_int
-        L.orc_density.argtypes = [_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp]
+        L.orc_density.argtypes = [_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int]
         L.orc_density.restype = C.c_int
         L.orc_neighbor_digest.argtypes = [_vp, C.c_int, _i64, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp]
         L.orc_neighbor_digest.restype = C.c_int
@@ -206,6 +208,18 @@ class Oracle:
         if rc != 0:
             raise ValueError(f"oracle build failed ({rc})")
 
+    def test_loop_escapes(self):
+        """Failure injection: every walk-ending escape link points at the root."""
+        rc = lib().orc_test_loop_escapes(self.ctx)
+        if rc != 0:
+            raise ValueError(f"oracle escape injection failed ({rc})")
+
+    def rebuild(self):
+        """orc_build again on the (already Morton-ordered) particles."""
+        rc = lib().orc_build(self.ctx, None, None)
+        if rc != 0:
+            raise ValueError(f"oracle build failed ({rc})")
+
     def __del__(self):
         if getattr(self, "ctx", None):
             lib().orc_destroy(self.ctx)
@@ -291,15 +305,28 @@ class Oracle:
             raise RuntimeError(f"oracle adjoint_lines failed ({rc})")
         return g
 
-    def density(self, sx, sy, sz, strategy=GATHER, hmode=H_PER_SAMPLE, hs=None):
+    def density(self, sx, sy, sz, strategy=GATHER, hmode=H_PER_SAMPLE, hs=None, number=False):
+        """_density_kernel (sum m W), or _number_density_kernel (sum W) with number=True."""
         sx, sy, sz = self._s(sx), self._s(sy), self._s(sz)
         hsa = None if hs is None else self._s(np.atleast_1d(hs))
         out = np.zeros(len(sx), dtype=self.dtype)
         set_kernel(self.kernel)
-        rc = lib().orc_density(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy, _p(out))
+        rc = lib().orc_density(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy, _p(out),
+                               1 if number else 0)
         if rc != 0:
             raise RuntimeError(f"oracle density failed ({rc})")
         return out
+
+    def gradient_density(self, sx, sy, sz, strategy=GATHER, hmode=H_PER_SAMPLE, hs=None):
+        """_gradient_density_kernel: sum m gradW - rho(r) sum (m/rho_b) gradW, NaN where rho(r) = 0."""
+        sx, sy, sz = self._s(sx), self._s(sy), self._s(sz)
+        hsa = None if hs is None else self._s(np.atleast_1d(hs))
+        out = np.zeros(3 * len(sx), dtype=self.dtype)
+        set_kernel(self.kernel)
+        rc = lib().orc_density(self.ctx, len(sx), _p(sx), _p(sy), _p(sz), hmode, _p(hsa), strategy, _p(out), 2)
+        if rc != 0:
+            raise RuntimeError(f"oracle gradient density failed ({rc})")
+        return out.reshape(3, len(sx))
 
     def digest(self, a, d=None, strategy=SYMMETRIC, hmode=H_NEAREST, hs=None):
         kind = 0 if d is None else 1

@@ -230,7 +230,8 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             memset(&fst, 0, sizeof(fst));
             // (a grid runs as a grid: its sample index is that of the coordinate arrays)
             rc = run(c, rq0.kind == SRC_GRID ? rq0 : rq, hmode, need_h ? (const void*)hsd : nullptr, st, cat,
-                     PREC_FP64, nullptr, PSB_FLAG_DEVICE_PTRS, &fst, WHAT_INTERP, nullptr, nullptr, nullptr);
+                     PREC_FP64, nullptr, PSB_FLAG_DEVICE_PTRS | (flags & PSB_FLAG_DENSITY_GRADIENT_PLAIN), &fst,
+                     WHAT_INTERP, nullptr, nullptr, nullptr);
             if (rc) return rc;
             launches += fst.launches;
         }

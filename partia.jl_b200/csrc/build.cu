@@ -342,6 +342,19 @@ __global__ void k_to_float(const double* src, int64_t n, float* dst) {
     if (i < n) dst[i] = (float)src[i];
 }
 
+// The mass-dependent parts of the leaf records (m/rho, m and leafK.w), with
+// k_pack_leaves' arithmetic: a values-only update leaves them as a full
+// build over the same particles would.
+template <class T>
+__global__ void k_pack_values(int64_t n, const T* m, const T* rho, float* mrho, float* mf, float4* leafK) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float mr = (float)((double)m[i] / (double)rho[i]);
+    mrho[i] = mr;
+    mf[i] = (float)m[i];
+    reinterpret_cast<float*>(leafK + i)[3] = mr;
+}
+
 // ---------------------------------------------------------------------------
 template <class T>
 static int build_typed(psb_ctx* c) {
@@ -478,6 +491,44 @@ static int build_typed(psb_ctx* c) {
     // |float(v) - v| <= 2^-24 |v|; the node tests allow twice that
     c->coord_err = (float)(maxabs * 1.1920928955078125e-07);
     c->built = true;
+    return PSB_OK;
+}
+
+template <class T>
+static int repack_values_typed(psb_ctx* c) {
+    const int64_t n = c->n;
+    cudaStream_t s = c->stream;
+    k_pack_values<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->m, (const T*)c->rho, c->mrho, c->mf, c->leafK);
+    if (sizeof(T) == 8 && c->ncol > 0) {
+        PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
+        for (int k = 0; k < c->ncol; ++k)
+            k_to_float<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], n, c->colsf + (size_t)k * n);
+    }
+    PSB_CUDA_TRY(c, cudaGetLastError(), "value pack kernels");
+    return PSB_OK;
+}
+
+int repack_values(psb_ctx* c) {
+    return c->dt == PSB_F64 ? repack_values_typed<double>(c) : repack_values_typed<float>(c);
+}
+
+// Every escape link that ends a traversal (escape 0: the right spine and the
+// last leaf) is pointed at the root instead.  Ids stay within 1..2n-1 and the
+// ranges are untouched, so every access of a walk stays in bounds; the walks
+// simply cycle until their step bound.
+__global__ void k_loop_escapes(int64_t n, int4* links, int32_t* escape) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 2 * n - 1) return;
+    if (escape[i] == 0) escape[i] = 1;
+    if (i < n - 1 && links[i].y == 0) links[i].y = 1;
+}
+
+int loop_escapes(psb_ctx* c) {
+    if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run first");
+    if (c->n < 2) return fail(c, PSB_EINVAL, "the LBVH needs at least two particles (a root node)");
+    k_loop_escapes<<<grid_for(2 * c->n - 1), BT, 0, c->stream>>>(c->n, c->links, c->escape);
+    PSB_CUDA_TRY(c, cudaGetLastError(), "escape kernel");
+    PSB_CUDA_TRY(c, cudaStreamSynchronize(c->stream), "synchronize");
     return PSB_OK;
 }
 

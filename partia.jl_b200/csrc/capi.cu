@@ -379,6 +379,56 @@ PSB_API int psb_build_lbvh(psb_ctx* c, int64_t* perm_out, uint64_t* codes_out) {
     return PSB_OK;
 }
 
+PSB_API int psb_set_values(psb_ctx* c, const void* m, const void* rho, int32_t ncol, const void* const* cols,
+                           uint32_t flags) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before psb_set_values");
+    if (ncol < 0) return fail(c, PSB_EINVAL, "ncol must be non-negative");
+    if (!m || !rho) return fail(c, PSB_EINVAL, "mass and density arrays must not be NULL");
+    if (ncol > 0 && !cols) return fail(c, PSB_EINVAL, "column pointer array must not be NULL");
+    for (int k = 0; k < ncol; ++k)
+        if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
+    cudaSetDevice(c->device);
+    if (flags & PSB_FLAG_DEVICE_PTRS) {
+        int rc = check_device_ptr(c, m, "the mass array");
+        if (!rc) rc = check_device_ptr(c, rho, "the density array");
+        for (int k = 0; !rc && k < ncol; ++k) rc = check_device_ptr(c, cols[k], "a particle column");
+        if (rc) return rc;
+    }
+    const int64_t n = c->n;
+    const size_t bytes = c->es * (size_t)n;
+    const cudaMemcpyKind kind = (flags & PSB_FLAG_DEVICE_PTRS) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(c->m, m, bytes, kind, c->stream), "mass copy");
+    PSB_CUDA_TRY(c, cudaMemcpyAsync(c->rho, rho, bytes, kind, c->stream), "density copy");
+    if ((int32_t)c->colpool.size() < ncol) {
+        c->colpool.resize(ncol, nullptr);
+        c->colcap.resize(ncol, 0);
+    }
+    c->cols.assign(ncol, nullptr);
+    for (int k = 0; k < ncol; ++k) {
+        PSB_CUDA_TRY(c, grow_buf(c, c->colpool[k], c->colcap[k], bytes), "cudaMalloc columns");
+        c->cols[k] = c->colpool[k];
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(c->cols[k], cols[k], bytes, kind, c->stream), "column copy");
+    }
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->d_cols, sizeof(void*) * (ncol > 0 ? ncol : 1)), "cudaMalloc column table");
+    if (ncol > 0)
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(c->d_cols, c->cols.data(), sizeof(void*) * ncol, cudaMemcpyHostToDevice, c->stream),
+                     "column table copy");
+    c->ncol = ncol;
+    int rc = repack_values(c);
+    if (rc) return rc;
+    PSB_CUDA_TRY(c, cudaStreamSynchronize(c->stream), "synchronize");
+    return PSB_OK;
+}
+
+PSB_API int psb_test_loop_escapes(psb_ctx* c) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    cudaSetDevice(c->device);
+    return loop_escapes(c);
+}
+
 PSB_API int psb_get_tree(psb_ctx* c, int32_t* root, int32_t* left, int32_t* right, int32_t* escape, int32_t* parent,
                          double* node_min, double* node_max, double* node_scale) {
     if (!c) return PSB_EINVAL;

@@ -206,8 +206,12 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     if (what == WHAT_INTERP) {
         int rc = make_recipe(c, cat, rq.line, A.rec, colu);
         if (rc) return rc;
+        if (flags & PSB_FLAG_DENSITY_GRADIENT_PLAIN)
+            for (int o = 0; o < A.rec.L; ++o)
+                if (A.rec.op[o] == OP_GRADD) A.rec.a2[o] = 1;
     } else {
         A.rec.L = (what == WHAT_DENSITY) ? 1 : 0;
+        A.unit_mass = (what == WHAT_DENSITY && (flags & PSB_FLAG_NUMBER_DENSITY)) ? 1 : 0;
     }
     const int L = A.rec.L;
     const bool adj = (what == WHAT_INTERP) && c->adj_lam;  // adjoint sum-cotangent pass: no fields written

@@ -72,6 +72,9 @@ template <class T> struct Args {
     // single-kernel path over a device list of tiles (nullptr: every tile)
     const int32_t* tile_list;
     const unsigned* tile_count;
+    // WHAT_DENSITY: every particle mass taken as 1, the number density
+    // sum W of _number_density_kernel (scalar_interpolation.jl:86-166)
+    int unit_mass;
 };
 
 // ---------------------------------------------------------------------------

@@ -84,9 +84,13 @@ __device__ __forceinline__ void write_sum_cotangents(const Args<T>& A, int64_t k
             } else if (op == OP_GRADC) {  // Sg_c[d] - G[d] Sw_c / S1
                 lSg[3 * a0i + a1] += go; lG[a1] -= go * sw[a0i] * inv; lSw[a0i] -= go * g[a1] * inv;
                 *lS1 += go * g[a1] * sw[a0i] * inv2;
-            } else if (op == OP_GRADD) {  // Dg[d] - G[d] Dm / S1
-                lDg[a1] += go; lG[a1] -= go * dm * inv; *lDm -= go * g[a1] * inv;
-                *lS1 += go * g[a1] * dm * inv2;
+            } else if (op == OP_GRADD) {
+                if (a2) {  // plain form Dg[d] - G[d] Dm (NaN, no cotangent, where Dm = 0)
+                    if (dm != 0.0) { lDg[a1] += go; lG[a1] -= go * dm; *lDm -= go * g[a1]; }
+                } else {   // Dg[d] - G[d] Dm / S1
+                    lDg[a1] += go; lG[a1] -= go * dm * inv; *lDm -= go * g[a1] * inv;
+                    *lS1 += go * g[a1] * dm * inv2;
+                }
             } else if (op == OP_DIV) {
                 const int cs[3] = {a0i, a1, a2};
                 for (int d = 0; d < 3; ++d) {
@@ -147,7 +151,10 @@ __device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k
             } else if (op == OP_GRADC) {
                 v = sg[a0i][a1] - g[a1] * (sw[a0i] * inv);
             } else if (op == OP_GRADD) {
-                v = Dg[a1].get() - g[a1] * (Dm.get() * inv);
+                // a2 set: the plain density rho(r) = Dm replaces the Shepard-normalised
+                // Dm / S1 (_gradient_density_kernel, gradient_interpolation.jl:1-170)
+                const double dm = Dm.get();
+                v = a2 ? (dm == 0.0 ? (double)NAN : Dg[a1].get() - g[a1] * dm) : Dg[a1].get() - g[a1] * (dm * inv);
             } else if (op == OP_DIV) {
                 double f = sg[a0i][0] + sg[a1][1] + sg[a2][2];
                 double b = (sw[a0i] * inv) * g[0] + (sw[a1] * inv) * g[1] + (sw[a2] * inv) * g[2];
@@ -452,7 +459,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             mr = (CT)((double)st.m[j] / (double)st.rho[j]);
         }
         if (WHAT == WHAT_DENSITY) {
-            dens += mb * Wsum;
+            dens += (A.unit_mass ? CT(1) : mb) * Wsum;
             return;
         }
         const CT w = mr * Wsum;
@@ -551,7 +558,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             }
             csum *= invr;
             if (WHAT == WHAT_DENSITY) {
-                Dm.add(st.mf[slot] * Wsum);
+                Dm.add((A.unit_mass ? 1.f : st.mf[slot]) * Wsum);
                 return;
             }
             const float w = K.w * Wsum;

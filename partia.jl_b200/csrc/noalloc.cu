@@ -23,7 +23,10 @@
 //    the array and must be serialised by the caller;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) once, with that device current; make that first
-//    call before any stream capture begins.
+//    call before any stream capture begins.  The address is kept with the
+//    CUDA context it belongs to: after a cudaDeviceReset the device gets a new
+//    context (and a new copy of the array), and the next call looks the
+//    address up again instead of handing the kernels a stale one.
 // The particles and the LBVH must already be on the device (psb_set_particles
 // and psb_build_lbvh allocate; this call does not).
 #include <cstring>
@@ -40,18 +43,45 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mutex;
 void* g_noalloc_addr[kMaxDevices] = {};
+void* g_noalloc_owner[kMaxDevices] = {};  // the CUDA context each address belongs to
+
+// cuCtxGetCurrent, reached through the runtime so that the library does not
+// link the driver library (it must load on machines without a GPU).
+typedef int (*ctx_get_current_fn)(void** pctx);
+ctx_get_current_fn g_ctx_get_current = nullptr;
+
+// Handle of the CUDA context current on this thread (nullptr if unknown).
+void* current_cuda_context() {
+    if (!g_ctx_get_current) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        g_ctx_get_current = (ctx_get_current_fn)fn;
+    }
+    void* cur = nullptr;
+    if (g_ctx_get_current(&cur) != 0) return nullptr;
+    return cur;
+}
 
 // Device address of g_noalloc_scratch on the current device.  In host code
 // the symbol name is only a host-side handle; the address the kernels use is
-// looked up once per device with that device current.
+// looked up once per device with that device current, and again only if the
+// device's CUDA context has changed since (cudaDeviceReset).
 cudaError_t noalloc_scratch_address(int device, void** out) {
     if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[device]) {
+    void* owner = current_cuda_context();
+    if (!g_noalloc_addr[device] || !owner || owner != g_noalloc_owner[device]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
         g_noalloc_addr[device] = p;
+        // the runtime has made the device's context current by now
+        g_noalloc_owner[device] = owner ? owner : current_cuda_context();
     }
     *out = g_noalloc_addr[device];
     return cudaSuccess;
@@ -235,6 +265,7 @@ extern "C" __attribute__((visibility("default"))) int psb_interp_points_noalloc(
     psb_strategy strategy, const psb_catalog* cat, psb_precision prec, void* const* out, psb_stats* stats) {
     using namespace psb;
     if (!c) return PSB_EINVAL;
+    c->err.clear();
     if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run before interpolation");
     if (ns < 0) return fail(c, PSB_EINVAL, "sample count must be non-negative");
     if (ns > PSB_NOALLOC_MAX_SAMPLES)

@@ -109,6 +109,11 @@ void release_buffers(psb_ctx* c);
 
 // build.cu
 int build_lbvh(psb_ctx* c);
+// Re-derive the leaf records that depend on m, rho and the columns (after a
+// values-only update of a built LBVH); queued on the context stream.
+int repack_values(psb_ctx* c);
+// Test hook: turn every end-of-walk escape link into a link to the root.
+int loop_escapes(psb_ctx* c);
 
 // scan.cu helpers used by the build and the interpolation drivers
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, psb_ctx* c, int slot_base);

@@ -31,6 +31,8 @@ PSB_FLAG_DEVICE_PTRS = 1
 PSB_FLAG_FP32C_DECISIONS = 0x100
 PSB_FLAG_SINGLE_KERNEL = 0x200
 PSB_FLAG_LUT1000_F32 = 0x400
+PSB_FLAG_DENSITY_GRADIENT_PLAIN = 0x800
+PSB_FLAG_NUMBER_DENSITY = 0x1000
 PSB_NOALLOC_MAX_SAMPLES = 262144
 
 
@@ -73,6 +75,8 @@ _SIGS = {
     "psb_set_stream": ([_vp, _vp], C.c_int),
     "psb_set_particles": ([_vp, _i64, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp, C.c_int, _u32], C.c_int),
     "psb_build_lbvh": ([_vp, _vp, _vp], C.c_int),
+    "psb_set_values": ([_vp, _vp, _vp, _i32, _vp, _u32], C.c_int),
+    "psb_test_loop_escapes": ([_vp], C.c_int),
     "psb_get_tree": ([_vp] * 9, C.c_int),
     "psb_interp_points": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, C.c_int, _vp, _u32, _vp], C.c_int),
     "psb_adjoint_points": ([_vp, _i64, _vp, _vp, _vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp,

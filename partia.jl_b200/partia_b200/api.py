@@ -122,6 +122,17 @@ class InterpolationInput:
         self.coord = tuple(arrs[:3])
         self.m, self.h, self.rho = arrs[3], arrs[4], arrs[5]
         self.quant = quant
+        # the device context that holds this input's particles and LBVH, and
+        # the LBVH last built from it (kept across driver calls)
+        self._b200_ctx = None
+        self._b200_lbvh = None
+
+    def __deepcopy__(self, memo):
+        """A copy of the arrays; the copy gets its own device state when used."""
+        import copy
+        return InterpolationInput(*[copy.deepcopy(a, memo) for a in (*self.coord, self.m, self.h, self.rho)],
+                                  tuple(copy.deepcopy(q, memo) for q in self.quant),
+                                  smoothed_kernel=self.smoothed_kernel)
 
     @property
     def dtype(self):
@@ -308,43 +319,64 @@ def restore_struct(coord, grid: PointSamples, axes, atol=1e-8, rtol=1e-8) -> Str
 # LBVH handle and the drivers
 # ---------------------------------------------------------------------------
 class LinearBVH:
-    """Device-resident LBVH of one InterpolationInput (held by a context)."""
+    """Device-resident LBVH of one InterpolationInput.
 
-    def __init__(self, ctx: Context, leaf_coor, leaf_scale, perm):
+    ``leaf_coor`` and ``leaf_scale`` are copies of the Morton-ordered
+    coordinates and smoothing lengths, as LinearBVH keeps them
+    (LinearBoundingVolumeHierarchy/LinearBVH/LinearBVH.jl:8-14); the tree
+    itself lives on the device context ``ctx``.  ``generation`` names the
+    build of ``ctx`` this handle describes: a context rebuilt from other
+    particles no longer holds this tree.
+    """
+
+    def __init__(self, ctx: Context, leaf_coor, leaf_scale, perm, generation: int):
         self.ctx = ctx
         self.leaf_coor = leaf_coor
         self.leaf_scale = leaf_scale
         self.perm = perm
+        self.generation = generation
 
     @property
     def nleaf(self):
         return len(self.leaf_scale)
 
 
-_ctx_cache: dict[int, Context] = {}
+def _check_kernel(input: InterpolationInput):
+    if getattr(input.smoothed_kernel, "code", None) is None:
+        raise ArgumentError(f"{input.smoothed_kernel!r} is not a kernel family of this backend")
 
 
-def _context(backend: B200ComputeBackend) -> Context:
-    ctx = _ctx_cache.get(backend.device)
-    if ctx is None:
+def _input_context(input: InterpolationInput, backend: B200ComputeBackend) -> Context:
+    """The context that holds this input on the backend's device (made once)."""
+    ctx = input._b200_ctx
+    if ctx is None or ctx.device != backend.device or ctx.h is None:
         ctx = Context(backend.device)
-        _ctx_cache[backend.device] = ctx
+        input._b200_ctx = ctx
     return ctx
 
 
+def _upload(ctx: Context, input: InterpolationInput):
+    ctx.set_particles(*input.coord, input.m, input.h, input.rho, input.quant, kernel=input.smoothed_kernel.code)
+
+
 def LinearBVH_(input: InterpolationInput, backend: B200ComputeBackend | None = None) -> LinearBVH:
-    """LinearBVH!(input): build on the device and permute input in place."""
+    """LinearBVH!(input): build on the device and permute input in place.
+
+    The build runs on the input's own context, made on first use and kept:
+    later builds of the same input reuse its device buffers (no allocation)."""
     backend = backend or B200ComputeBackend()
-    if getattr(input.smoothed_kernel, "code", None) is None:
-        raise ArgumentError(f"{input.smoothed_kernel!r} is not a kernel family of this backend")
+    _check_kernel(input)
     if input.Npart < 1:
         raise ArgumentError("BinaryRadixTree: enc.codes must be non-empty (got n=0).")
-    ctx = Context(backend.device)
-    ctx.set_particles(*input.coord, input.m, input.h, input.rho, input.quant, kernel=input.smoothed_kernel.code)
+    ctx = _input_context(input, backend)
+    _upload(ctx, input)
     perm, _ = ctx.build()
     for a in (*input.coord, input.m, input.h, input.rho, *input.quant):
         a[:] = a[perm]
-    return LinearBVH(ctx, tuple(c.copy() for c in input.coord), input.h.copy(), perm)
+    ctx.generation += 1
+    lbvh = LinearBVH(ctx, tuple(c.copy() for c in input.coord), input.h.copy(), perm, ctx.generation)
+    input._b200_lbvh = lbvh
+    return lbvh
 
 
 def matches_lbvh_leaf_order(input: InterpolationInput, lbvh: LinearBVH) -> bool:
@@ -352,15 +384,54 @@ def matches_lbvh_leaf_order(input: InterpolationInput, lbvh: LinearBVH) -> bool:
         input.h, lbvh.leaf_scale)
 
 
+def _bind(lbvh: LinearBVH, input: InterpolationInput):
+    """Put ``input``'s values on ``lbvh``'s context, whose leaf order it matches.
+
+    The tree depends on coordinates and h only, which the leaf-order check
+    has compared, so only m, rho and the columns are replaced
+    (psb_set_values).  A context rebuilt from other particles since
+    ``lbvh`` was made, or set with another kernel or float type, is rebuilt
+    from ``input``: its coordinates are already in Morton order, so the build
+    permutes nothing."""
+    ctx = lbvh.ctx
+    _check_kernel(input)
+    same = (ctx.generation == lbvh.generation and ctx.kernel == input.smoothed_kernel.code
+            and ctx.dtype == np.dtype(input.dtype) and ctx.n == input.Npart)
+    if same:
+        ctx.set_values(input.m, input.rho, input.quant)
+        return
+    _upload(ctx, input)
+    perm, _ = ctx.build()
+    if not np.array_equal(perm, np.arange(input.Npart)):
+        raise ArgumentError("Provided LBVH leaf order does not match the current input ordering. "
+                            "Ensure the LBVH was built from the same Morton-reordered input.")
+    ctx.generation += 1
+    lbvh.generation = ctx.generation
+
+
+def _input_lbvh(backend: B200ComputeBackend, input: InterpolationInput) -> LinearBVH:
+    """LinearBVH!(input) as the drivers call it (initialize_interpolation.jl:50).
+
+    An input already in the leaf order of the LBVH last built from it would be
+    permuted by the identity and get the same tree again; that LBVH is reused
+    with the input's current values instead of being rebuilt."""
+    lbvh = input._b200_lbvh
+    if (lbvh is not None and lbvh.ctx is input._b200_ctx and lbvh.ctx.h is not None
+            and lbvh.ctx.device == backend.device and matches_lbvh_leaf_order(input, lbvh)):
+        _bind(lbvh, input)
+        return lbvh
+    return LinearBVH_(input, backend)
+
+
 def initialize_interpolation(backend, grid_template, input=None, catalog=None):
-    """Allocate outputs, build the LBVH (when input is given), concise catalog."""
+    """Allocate outputs, build (or reuse) the LBVH when input is given, concise catalog."""
     if catalog is None:
         input, catalog = None, input
     grids = tuple(grid_template.similar() for _ in range(catalog.L))
     conc = catalog.concise()
     if input is None:
         return grids, catalog.ordered_names, conc
-    lbvh = LinearBVH_(input, backend)
+    lbvh = _input_lbvh(backend, input)
     return grids, lbvh, catalog.ordered_names, conc
 
 
@@ -370,6 +441,10 @@ def _strategy(s):
     raise ArgumentError(f"unknown interpolation strategy {s!r}")
 
 
+_LEAF_ORDER_MSG = ("Provided LBVH leaf order does not match the current input ordering. "
+                   "Ensure the LBVH was built from the same Morton-reordered input.")
+
+
 def PointSamples_interpolation(backend, grid_template: PointSamples, input: InterpolationInput, *args,
                                precision=None):
     """PointSamples_interpolation(backend, grid, input, [LBVH,] catalog, itp_strategy=itpSymmetric)."""
@@ -377,8 +452,8 @@ def PointSamples_interpolation(backend, grid_template: PointSamples, input: Inte
         lbvh, catalog = args[0], args[1]
         strategy = args[2] if len(args) > 2 else itpSymmetric
         if not matches_lbvh_leaf_order(input, lbvh):
-            raise ArgumentError("Provided LBVH leaf order does not match the current input ordering. "
-                                "Ensure the LBVH was built from the same Morton-reordered input.")
+            raise ArgumentError(_LEAF_ORDER_MSG)
+        _bind(lbvh, input)
         grids, names, conc = initialize_interpolation(backend, grid_template, catalog)
     else:
         catalog = args[0]
@@ -407,8 +482,8 @@ def LineSamples_interpolation(backend, grid_template: LineSamples, input: Interp
         raise ArgumentError("LineSamples_interpolation supports scalar quantities only")
     if lbvh is not None:
         if not matches_lbvh_leaf_order(input, lbvh):
-            raise ArgumentError("Provided LBVH leaf order does not match the current input ordering. "
-                                "Ensure the LBVH was built from the same Morton-reordered input.")
+            raise ArgumentError(_LEAF_ORDER_MSG)
+        _bind(lbvh, input)
         grids, names, conc = initialize_interpolation(backend, grid_template, catalog)
     else:
         grids, lbvh, names, conc = initialize_interpolation(backend, grid_template, input, catalog)
@@ -421,9 +496,23 @@ def LineSamples_interpolation(backend, grid_template: LineSamples, input: Interp
 
 def StructuredGrid_interpolation(backend, coord, grid_template: StructuredGrid, input: InterpolationInput, catalog,
                                  itp_strategy=itpSymmetric, precision=None):
-    """StructuredGrid_driver.jl:46-64: flatten, interpolate, restore."""
-    flat = flatten(coord, grid_template)
-    bundle = PointSamples_interpolation(backend, flat, input, catalog, itp_strategy, precision=precision)
-    axes = tuple(np.asarray(a, dtype=input.dtype) for a in grid_template.axes)
-    grids = tuple(restore_struct(coord, g, axes) for g in bundle.grids)
-    return GridBundle(grids, bundle.names)
+    """StructuredGrid_driver.jl:46-64 for Cartesian grids.
+
+    The reference flattens the grid into PointSamples, interpolates and
+    restores the structure.  Here the column-major sample coordinates are
+    generated on the device from the axes (psb_interp_grid), which gives the
+    flattened samples' results bit for bit, written straight into the
+    column-major output grids."""
+    if coord is not Cartesian:
+        raise ArgumentError("only Cartesian structured grids are provided by the B200 backend")
+    T = np.dtype(input.dtype)
+    axes = tuple(np.asarray(a, dtype=T) for a in grid_template.axes)
+    size = tuple(len(a) for a in axes)
+    names = catalog.ordered_names
+    conc = catalog.concise()
+    lbvh = _input_lbvh(backend, input)
+    prec = backend.precision if precision is None else precision
+    flat = [np.empty(int(np.prod(size)), dtype=T) for _ in range(catalog.L)]
+    lbvh.ctx.interp_grid(*axes, conc, strategy=_strategy(itp_strategy), hmode=L.PSB_H_NEAREST, prec=prec, out=flat)
+    grids = tuple(StructuredGrid(f.reshape(size, order="F"), axes, size) for f in flat)
+    return GridBundle(grids, names)

@@ -69,6 +69,9 @@ class Context:
         self.n = 0
         self.ncol = 0
         self.last_stats = L.Stats()
+        self.builds = 0  # psb_build_lbvh calls made through this object
+        self.kernel = L.PSB_KERNEL_M4
+        self.generation = 0  # LBVH builds made through the Partia-API layer on this context
 
     def close(self):
         if getattr(self, "h", None):
@@ -104,11 +107,28 @@ class Context:
         self._keep = None
         self.n = n
         self.ncol = len(cols)
+        self.kernel = int(kernel)
+
+    def set_values(self, m, rho, cols=()):
+        """New m, rho and columns (in the LBVH's leaf order) for the built tree."""
+        dev = _is_dev(m)
+        if not dev:
+            cv = lambda a: np.ascontiguousarray(np.asarray(a, dtype=self.dtype))
+            m, rho = cv(m), cv(rho)
+            cols = [cv(c) for c in cols]
+        cols = list(cols)
+        for a in (m, rho, *cols):
+            if len(a) != self.n:
+                raise ValueError(f"value arrays must hold {self.n} entries (got {len(a)})")
+        self._chk(self.lib.psb_set_values(self.h, _ptr(m), _ptr(rho), len(cols), _ptr_array(cols),
+                                          L.PSB_FLAG_DEVICE_PTRS if dev else 0))
+        self.ncol = len(cols)
 
     def build(self, want_perm=True, want_codes=False):
         perm = np.zeros(self.n, dtype=np.int64) if want_perm else None
         codes = np.zeros(self.n, dtype=np.uint64) if want_codes else None
         self._chk(self.lib.psb_build_lbvh(self.h, _ptr(perm), _ptr(codes)))
+        self.builds += 1
         return perm, codes
 
     def tree(self):
@@ -152,7 +172,7 @@ class Context:
 
     # ---- interpolation ----
     def interp_points(self, sx, sy, sz, cat: CatalogC, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, hs=None,
-                      prec=L.PSB_PREC_FP64, out=None):
+                      prec=L.PSB_PREC_FP64, out=None, flags=0):
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
         ns = len(sx)
@@ -160,7 +180,8 @@ class Context:
         outs = self._outs(ns, cat.L, dev, out)
         self._chk(self.lib.psb_interp_points(self.h, ns, _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy,
                                              C.byref(cat.c), prec, _ptr_array(outs),
-                                             (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
+                                             (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags | flags,
+                                             C.byref(self.last_stats)))
         return outs
 
     # ---- adjoint ----
@@ -180,7 +201,7 @@ class Context:
         return [np.ascontiguousarray(np.asarray(g, dtype=np.float64)) for g in gout]
 
     def adjoint_points(self, sx, sy, sz, cat: CatalogC, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
-                       hs=None):
+                       hs=None, flags=0):
         """dL/dm, dL/dA_c, dL/dx.. for L = sum_k sum_s gout[k][s] out_k(s), in the particles' given order."""
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
@@ -190,7 +211,8 @@ class Context:
         self._chk(self.lib.psb_adjoint_points(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa),
                                               strategy, C.byref(cat.c), _ptr_array(go), _ptr(g["m"]),
                                               _ptr_array(g["cols"]), _ptr(g["x"]), _ptr(g["y"]), _ptr(g["z"]),
-                                              L.PSB_FLAG_DEVICE_PTRS if dev else 0, C.byref(self.last_stats)))
+                                              (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | flags,
+                                              C.byref(self.last_stats)))
         return g
 
     def adjoint_grid(self, ax, ay, az, cat: CatalogC, gout, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST,
@@ -270,13 +292,17 @@ class Context:
         return outs
 
     def density(self, sx, sy, sz, strategy=L.PSB_GATHER, hmode=L.PSB_H_PER_SAMPLE, hs=None, prec=L.PSB_PREC_FP64,
-                out=None):
+                out=None, number=False):
+        """sum m W (_density_kernel), or sum W (_number_density_kernel) with number=True."""
         sx, sy, sz = self._arr(sx), self._arr(sy), self._arr(sz)
         dev = _is_dev(sx)
         hsa = self._hs(hmode, hs, dev)
         o = out if out is not None else self._outs(len(sx), 1, dev)[0]
+        flags = (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags
+        if number:
+            flags |= L.PSB_FLAG_NUMBER_DENSITY
         self._chk(self.lib.psb_density(self.h, len(sx), _ptr(sx), _ptr(sy), _ptr(sz), hmode, _ptr(hsa), strategy, prec,
-                                       _ptr(o), (L.PSB_FLAG_DEVICE_PTRS if dev else 0) | self.extra_flags, C.byref(self.last_stats)))
+                                       _ptr(o), flags, C.byref(self.last_stats)))
         return o
 
     def digest(self, a, d=None, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, hs=None, fp32c=False):

@@ -1,7 +1,7 @@
 """Sample the reference's line-integrated kernel tables into a small golden fixture.
 
 Reads src/julia/KernelInterpolation/table/line_integrated_kernel_tables.jl of a
-Partia.jl checkout (first argument, default /root/reference) and writes, for
+Partia.jl checkout (first argument, else $PARTIA_REFERENCE_DIR) and writes, for
 each kernel family, every 64th entry of _<K>_Q and _<K>_Inorm (64 + the last
 entry) and the grid spacing Q[2] - Q[1] to line_table_samples.json next to
 this script.  The full tables are not copied.
@@ -25,7 +25,9 @@ def parse_table(root, name):
 
 
 def main():
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PARTIA_REFERENCE_DIR", "")
+    if not root or not os.path.isdir(root):
+        sys.exit("usage: make_lut_fixture.py <Partia.jl checkout>  (or set PARTIA_REFERENCE_DIR)")
     idx = list(range(0, 4096, 64)) + [4095]
     out = {"source": "table/line_integrated_kernel_tables.jl (_<K>_Q, _<K>_Inorm)", "index0": idx, "kernels": {}}
     for k in KERNELS:

@@ -251,3 +251,35 @@ def test_other_kernels_points_vs_brute_force(kid, strategy, name):
             assert lo[1][i] == pytest.approx(ref[1], rel=1e-10, abs=1e-12)
     finally:
         B.set_kernel(0)
+
+
+@pytest.mark.parametrize("strategy,name", [(O.GATHER, "gather"), (O.SCATTER, "scatter"), (O.SYMMETRIC, "symmetric")])
+def test_number_density_and_plain_density_gradient_vs_brute_force(strategy, name):
+    """_number_density_kernel (scalar_interpolation.jl:86-166) and the standalone
+    _gradient_density_kernel (gradient_interpolation.jl:1-170): sum W, and
+    sum m gradW - rho(r) sum (m/rho_b) gradW with rho(r) = sum m W (NaN where
+    rho(r) = 0), against brute force."""
+    P, cols = lattice(8)
+    P = dict(P)
+    rng = np.random.default_rng(17)
+    P["m"] = P["m"] * rng.uniform(0.5, 1.5, len(P["m"]))
+    P["rho"] = rng.uniform(0.7, 1.3, len(P["m"]))
+    orc = make_oracle(P, cols)
+    s = tuple(np.append(rng.uniform(0.1, 0.9, 12), 9.0) for _ in range(3))  # the last sample has no neighbour
+    ha = np.append(rng.uniform(0.1, 0.2, 12), 0.1)
+    nd = orc.density(*s, strategy=strategy, hmode=O.H_PER_SAMPLE, hs=ha, number=True)
+    gd = orc.gradient_density(*s, strategy=strategy, hmode=O.H_PER_SAMPLE, hs=ha)
+    for i in range(13):
+        p = np.array([s[0][i], s[1][i], s[2][i]])
+        sel, d, r, hb = B._neighbours(P, p, ha[i], name)
+        Wv, G = B._weights(d, r, hb, ha[i], name)
+        assert nd[i] == pytest.approx(np.sum(Wv), rel=1e-12, abs=0)
+        rho = np.sum(P["m"][sel] * Wv)
+        if rho == 0:
+            assert np.all(np.isnan(gd[:, i]))
+            continue
+        f_ = np.sum(P["m"][sel] * G, axis=1)
+        b_ = np.sum(P["m"][sel] * G / P["rho"][sel], axis=1)
+        ref = f_ - b_ * rho
+        np.testing.assert_allclose(gd[:, i], ref, rtol=1e-10, atol=1e-12 * np.max(np.abs(f_)))
+    assert nd[12] == 0.0

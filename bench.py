@@ -184,6 +184,45 @@ def timed_call(fn, stream, steps, warmup):
     return float(np.median(ms))
 
 
+def cudaext_leg(ctx, d, axis, steps, warmup, ours):
+    """The reference's CUDA-extension design on the same workload
+    (psb_baseline_cudaext_points: one thread per sample, per-thread DFS, FP64;
+    particles, tree and samples copied from pageable host memory and the 8
+    fields copied back in every call).  Its LBVH comes from this library's
+    build (the reference builds it on the CPU, which is not timed here)."""
+    import torch
+    from partia_b200.engine import CatalogC
+    perm, _ = ctx.build(want_perm=True)
+    tree = ctx.tree()
+    parts = {k: np.ascontiguousarray(d[k][perm]) for k in ("x", "y", "z", "m", "h", "rho")}
+    parts["cols"] = [np.ascontiguousarray(d[k][perm]) for k in ("rho", "Ax", "Ay", "Az")]
+    n = len(axis)
+    X, Y, Z = np.meshgrid(axis, axis, axis, indexing="ij")
+    s = [np.ascontiguousarray(a.ravel(order="F")) for a in (X, Y, Z)]
+    cat = CatalogC(**CATALOG)
+    for _ in range(warmup):
+        ctx.baseline_cudaext_points(parts, tree, *s, cat)
+    host, kern, tot = [], [], []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.baseline_cudaext_points(parts, tree, *s, cat)
+        host.append(time.perf_counter() - t0)
+        kern.append(ctx.last_stats.interp_ms)
+        tot.append(ctx.last_stats.total_ms)
+    pairs = int(ctx.last_stats.pairs)
+    kms, hms = float(np.median(kern)), 1e3 * float(np.median(host))
+    ns = n ** 3
+    return {"design": "one thread per sample (256/block), per-thread stackless DFS for nearest h and the FP64 "
+                      "general kernel; particles, tree and samples H2D and outputs D2H in every call "
+                      "(ext/CUDAExt/.../PointSamples_driver.jl:12-27, kernels/PointSamples_kernel.jl:1-68)",
+            "kernel_ms": kms, "e2e_ms": hms, "event_ms": float(np.median(tot)), "pairs": pairs,
+            "samples_per_s_device": ns / (kms / 1e3), "samples_per_s_e2e": ns / (hms / 1e3),
+            "not_timed": "the reference's CPU LBVH build (the tree is this library's, uploaded every call)",
+            "vs_cudaext_design": {"device_fp32c": kms / ours["fp32c_ms"], "device_fp64": kms / ours["fp64_ms"],
+                                  "e2e": hms / ours["e2e_ms"]}}
+
+
 def lines_and_adjoint(steps, warmup):
     """The line-integrated configurations (clump particles, parallel beam through
     the 30/45-degree frame over [0,1]^2, scatter, column density = plain scalar
@@ -566,6 +605,7 @@ def main():
     ap.add_argument("--no-lines", action="store_true", help="skip the line-integrated and adjoint legs")
     ap.add_argument("--no-large", action="store_true", help="skip the 64M-particle leg")
     ap.add_argument("--no-kernels", action="store_true", help="skip the kernel-family leg")
+    ap.add_argument("--no-cudaext", action="store_true", help="skip the CUDA-extension design baseline leg")
     ap.add_argument("--large-n", type=int, default=64_000_000,
                     help="particles of the large leg (64M = the workload; fewer only for profiling captures)")
     ap.add_argument("--large-grid", type=int, default=256,
@@ -668,6 +708,7 @@ def main():
             scale = b[fin].abs().max().item()
             errs[names[k]] = (a[fin] - b[fin]).abs().max().item() / scale if scale > 0 else 0.0
         fp64 = {"value": v64, "unit": UNIT, "kernel_ms": float(np.median(kern64)),
+                "ms": tot64 / max(2, args.steps // 2),
                 "speedup_fp32c_vs_fp64": value / v64 if world == 1 else None}
 
     # e2e through the C ABI with host buffers (pinned), copies inside the timed region
@@ -729,6 +770,12 @@ def main():
     achieved = b_alg / (kern_ms / 1e3) / 1e9
     tr = ncu_traffic()
 
+    cudaext = None
+    if world == 1 and not args.no_cudaext:
+        ours = {"fp32c_ms": tot32 / args.steps, "fp64_ms": (fp64 or {}).get("ms", float("nan")),
+                "e2e_ms": e2e_host_ms}
+        cudaext = cudaext_leg(ctx, d, axis, 3, 1, ours)
+
     extra = None
     if world == 1 and not args.no_lines:
         extra = lines_and_adjoint(max(3, args.steps // 4), 2)
@@ -772,6 +819,7 @@ def main():
                          "samples_per_span_visit": ctx_span_tests / max(ctx_spans, 1)},
             "fp64": fp64, "fp32c_rel_err_vs_fp64": errs,
             "grad_fwd_time_ratio": extra["adjoint"]["grad_fwd_time_ratio"] if extra else None,
+            "cudaext_design": cudaext,
             "lines": extra["lines"] if extra else None, "adjoint": extra["adjoint"] if extra else None,
             "large": large,
             "kernel_families": kern,

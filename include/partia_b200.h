@@ -350,6 +350,32 @@ int psb_adjoint_beam(psb_ctx* ctx, const void* frame, const void* params,
                      double* gm, double* const* gcols, double* gx, double* gy, double* gz,
                      uint32_t flags, psb_stats* stats);
 
+/* ---- the reference's GPU design, as a baseline ------------------------------- */
+
+/* PointSamples_interpolation with the structure of Partia's CUDA extension
+ * (ext/CUDAExt/KernelInterpolation/grid_interpolation/drivers/PointSamples_driver.jl:12-27,
+ *  ext/CUDAExt/KernelInterpolation/grid_interpolation/kernels/PointSamples_kernel.jl:1-68),
+ * kept to measure this library against it on the same GPU; it is not the
+ * library's interpolation path.  Every argument is a host array: the n
+ * particles in the tree's leaf (Morton) order with ncol columns, and the tree
+ * as psb_get_tree exports it (root, left and escape with unified 1-based ids,
+ * axis-major node boxes, node scales), as the reference builds it on the CPU.
+ * Each call copies all of it and the samples to the device, runs one thread
+ * per sample in blocks of 256 (nearest-particle h by LBVH_find_nearest_h for
+ * gather and symmetric, then the FP64 general interpolation kernel, each a
+ * per-thread stackless DFS, no shared memory), and copies the L outputs back.
+ * Device buffers are the context's and are kept between calls.  FP64 only;
+ * stats->h2d_ms / interp_ms / d2h_ms split the call's event time. */
+int psb_baseline_cudaext_points(psb_ctx* ctx, int64_t n,
+                                const double* x, const double* y, const double* z,
+                                const double* m, const double* h, const double* rho,
+                                int32_t ncol, const double* const* cols, psb_kernel kernel,
+                                int32_t root, const int32_t* left, const int32_t* escape,
+                                const double* node_min, const double* node_max, const double* node_scale,
+                                int64_t ns, const double* sx, const double* sy, const double* sz,
+                                psb_strategy strategy, const psb_catalog* cat,
+                                double* const* out, psb_stats* stats);
+
 /* ---- failure injection (tests) ------------------------------------------------ */
 
 /* No counterpart in the reference, which has no device walks to bound.  For

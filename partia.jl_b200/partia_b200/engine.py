@@ -184,6 +184,28 @@ class Context:
                                              C.byref(self.last_stats)))
         return outs
 
+    # ---- the reference's GPU design (baseline) ----
+    def baseline_cudaext_points(self, parts, tree, sx, sy, sz, cat: CatalogC, strategy=L.PSB_SYMMETRIC, kernel=None):
+        """psb_baseline_cudaext_points: parts = dict of host arrays x y z m h rho
+        and cols (leaf order), tree = Context.tree() of the same particles;
+        samples and outputs are host arrays (copied every call)."""
+        f64 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+        arrs = [f64(parts[k]) for k in ("x", "y", "z", "m", "h", "rho")]
+        cols = [f64(c) for c in parts.get("cols", ())]
+        s = [f64(a) for a in (sx, sy, sz)]
+        ns = len(s[0])
+        outs = [np.empty(ns, dtype=np.float64) for _ in range(cat.L)]
+        t = {k: np.ascontiguousarray(tree[k]) for k in ("left", "escape")}
+        nmin = np.ascontiguousarray(tree["node_min"], dtype=np.float64)
+        nmax = np.ascontiguousarray(tree["node_max"], dtype=np.float64)
+        nsc = np.ascontiguousarray(tree["node_scale"], dtype=np.float64)
+        kern = self.kernel if kernel is None else int(kernel)
+        self._chk(self.lib.psb_baseline_cudaext_points(
+            self.h, len(arrs[0]), *[_ptr(a) for a in arrs], len(cols), _ptr_array(cols), kern, int(tree["root"]),
+            _ptr(t["left"]), _ptr(t["escape"]), _ptr(nmin), _ptr(nmax), _ptr(nsc), ns, *[_ptr(a) for a in s],
+            strategy, C.byref(cat.c), _ptr_array(outs), C.byref(self.last_stats)))
+        return outs
+
     # ---- adjoint ----
     def _grad_outs(self, like_dev):
         n = self.n

@@ -62,3 +62,22 @@ def test_flag_constants_match_header():
     for name in names:
         m = re.search(r"#define\s+%s\s+(0x[0-9a-fA-F]+|\d+)u" % name, hdr)
         assert m and int(m.group(1), 0) == getattr(L, name), name
+
+
+def test_julia_binding_calls_only_declared_symbols():
+    """The Julia package (partia.jl_b200/julia/PartiaB200) ccalls only functions
+    the header declares, and binds every driver entry point Partia's CUDA
+    extension methods need.  (Julia is not in this image; this checks the
+    source against the ABI.)"""
+    import re
+    root = os.path.join(os.path.dirname(os.path.dirname(L.HEADER_PATH)), "partia.jl_b200", "julia", "PartiaB200")
+    srcs = []
+    for d, _, files in os.walk(root):
+        srcs += [open(os.path.join(d, f)).read() for f in files if f.endswith(".jl")]
+    called = set(re.findall(r"ccall\(\(:(psb_\w+), libpsb\)", "\n".join(srcs)))
+    declared = set(L.header_symbols())
+    assert called <= declared, called - declared
+    assert {"psb_create", "psb_destroy", "psb_last_error", "psb_set_particles", "psb_set_values", "psb_build_lbvh",
+            "psb_interp_points", "psb_interp_lines", "psb_adjoint_points"} <= called
+    proj = open(os.path.join(root, "Project.toml")).read()
+    assert "Partia" in proj and "ChainRulesCore" in proj

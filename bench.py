@@ -11,11 +11,14 @@ value: samples/s with particles, LBVH and outputs resident in HBM (grid
 coordinates generated on the device), device time from CUDA events.
 e2e:   the same metric through the C ABI with host buffers: the host sample
 coordinates (pinned) are copied in and the 8 output fields copied out inside
-the timed region every step.
+the timed region every step, timed with the host clock around each call
+(a pageable-buffer variant is reported beside it).
 
 Multi-GPU: samples shard over ranks (each rank owns a contiguous slab of
-z-planes of the grid; the particle set and its LBVH are replicated); there is
-no data-path collective.  --impl reference times the CPU restatement of the
+z-planes of the grid, the slabs cut for equal estimated pair counts from a
+coarse neighbour-digest pass; the particle set and its LBVH are replicated);
+there is no data-path collective, and the total work is fixed (strong
+scaling).  --impl reference times the CPU restatement of the
 reference's multithreaded CPU path (oracle/, "port") on the host cores.
 """
 from __future__ import annotations
@@ -645,9 +648,14 @@ def main():
     build_ms = (time.perf_counter() - t0) * 1e3
     cat = CatalogC(**CATALOG)
 
-    # this rank's slab of z-planes (samples shard; particles and LBVH are replicated)
-    from partia_b200.sharding import grid_slab
-    (z0, z1), _ = grid_slab(NGRID, NGRID, NGRID, rank, world)
+    # this rank's slab of z-planes (samples shard; particles and LBVH are
+    # replicated): slabs of equal estimated pair count from a coarse digest
+    # pass, which every rank computes identically
+    z0, z1 = 0, NGRID
+    if world > 1:
+        from partia_b200.sharding import plane_pair_estimates, weighted_slabs
+        plane_w = plane_pair_estimates(ctx, axis, axis, axis, stride=8)
+        z0, z1 = weighted_slabs(plane_w, world)[rank]
     az = axis[z0:z1]
     ns = NGRID * NGRID * len(az)
     outs = [torch.empty(ns, dtype=torch.float64, device=dev) for _ in range(L_OUT)]

@@ -310,7 +310,7 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
         if (herr) {
             cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
             cudaStreamSynchronize(s);
-            return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+            return device_error(c, herr);
         }
         if (stats) {
             memset(stats, 0, sizeof(*stats));

@@ -481,6 +481,7 @@ static int build_typed(psb_ctx* c) {
         reset_tree(c);
         if (herr & PSB_DERR_INPUT)
             return fail(c, PSB_EINVAL, "particle coordinates must be finite (NaN or Inf found)");
+        if (herr & PSB_DERR_SORT) return device_error(c, herr);
         return fail(c, PSB_ETRAVERSAL, "LBVH refit did not combine every internal node exactly twice");
     }
     double maxabs = 0;

@@ -20,6 +20,12 @@ int cuda_fail(psb_ctx* c, cudaError_t e, const char* what) {
     return fail(c, e == cudaErrorMemoryAllocation ? PSB_ENOMEM : PSB_ECUDA, m);
 }
 
+int device_error(psb_ctx* c, unsigned herr) {
+    if (herr & PSB_DERR_SORT)
+        return fail(c, PSB_ETRAVERSAL, "a radix-sort look-back wait ran out of iterations");
+    return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+}
+
 void* scratch(psb_ctx* c, int k, size_t bytes) {
     if (k < 0 || k >= (int)(sizeof(c->scratch) / sizeof(c->scratch[0]))) return nullptr;
     auto& sl = c->scratch[k];

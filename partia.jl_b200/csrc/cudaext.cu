@@ -256,7 +256,7 @@ extern "C" __attribute__((visibility("default"))) int psb_baseline_cudaext_point
     if (herr) {
         cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
-        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+        return device_error(c, herr);
     }
     if (stats) {
         float ms = 0.f;

@@ -380,7 +380,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     if (herr) {
         cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
-        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+        return device_error(c, herr);
     }
     if (stats) {
         stats->h2d_ms = ms_between(c->ev[0], c->ev[1]);
@@ -577,7 +577,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     if (herr) {
         cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
-        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+        return device_error(c, herr);
     }
     if (stats) {
         memset(stats, 0, sizeof(*stats));

@@ -219,7 +219,7 @@ int noalloc_typed(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const 
                                                                     make_double3(scl[0], scl[1], scl[2]), codes, idx);
         PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
         ++launches;
-        PSB_CUDA_TRY(c, radix_sort_pairs_in(codes, idx, ns, sp, sort_bytes, s, &launches), "sample sort");
+        PSB_CUDA_TRY(c, radix_sort_pairs_in(codes, idx, ns, sp, sort_bytes, s, c->d_err, &launches), "sample sort");
         A.src.order = idx;
     }
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[2], s), "event");
@@ -236,7 +236,7 @@ int noalloc_typed(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const 
     if (herr) {
         cudaMemsetAsync(c->d_err, 0, sizeof(unsigned), s);
         cudaStreamSynchronize(s);
-        return fail(c, PSB_ETRAVERSAL, "a traversal exceeded its step bound (corrupt escape links)");
+        return device_error(c, herr);
     }
     if (stats) {
         float ms = 0.f;

@@ -19,6 +19,7 @@
 #define PSB_DERR_TRAVERSAL 1u   // a traversal or refit loop hit its bound
 #define PSB_DERR_REFIT 2u       // a refit node was not combined exactly once
 #define PSB_DERR_INPUT 4u       // non-finite particle coordinate
+#define PSB_DERR_SORT 8u        // a radix-sort look-back wait ran out of iterations
 
 namespace psb {
 

@@ -87,6 +87,9 @@ namespace psb {
 
 // Record an error message on the context and return the code.
 int fail(psb_ctx* c, int code, const std::string& msg);
+// PSB_ETRAVERSAL with the message of a nonzero device error word (read back
+// after a call's kernels; the caller clears the word).
+int device_error(psb_ctx* c, unsigned herr);
 // Translate a CUDA error into PSB_ECUDA (or PSB_ENOMEM) with a message.
 int cuda_fail(psb_ctx* c, cudaError_t e, const char* what);
 // Grow-on-demand scratch slot k to at least `bytes`; returns nullptr on failure.
@@ -118,17 +121,18 @@ int loop_escapes(psb_ctx* c);
 // scan.cu helpers used by the build and the interpolation drivers
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, psb_ctx* c, int slot_base);
 cudaError_t inclusive_max_scan_i64(int64_t* data, int64_t n, psb_ctx* c, int slot_base);
-// Stable LSD radix sort of (key, value) pairs on the low `bits` bits of key.
-// Results end in keys/vals (the alternates are scratch).
-// skip_constant_digits: read back which 8-bit digits vary (one host sync) and
-// sort only those; otherwise all eight passes run without a host round trip.
+// Stable LSD radix sort (onesweep, 8-bit digits) of (key, value) pairs,
+// results in keys/vals; scratch slot slot_base.  skip_constant_digits: read
+// back which digits vary (one host sync) and sort only those; otherwise all
+// eight passes run without a host round trip.  A look-back wait that runs
+// out sets PSB_DERR_SORT in the context's error word.
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches,
                              bool skip_constant_digits = true);
 // The same sort on caller-provided scratch of at least
 // radix_sort_pairs_scratch_bytes(n) bytes (256-byte aligned); allocates nothing.
 size_t radix_sort_pairs_scratch_bytes(int64_t n);
 cudaError_t radix_sort_pairs_in(uint64_t* keys, uint32_t* vals, int64_t n, void* scratch_space, size_t bytes,
-                                cudaStream_t s, int* launches);
+                                cudaStream_t s, unsigned* err, int* launches);
 
 template <class T> TreeView<T> tree_view(psb_ctx* c);
 

@@ -81,6 +81,26 @@ def test_build_bit_exact(n, seed, dtype):
         assert np.array_equal(to[k], tg[k]), k
 
 
+@pytest.mark.parametrize("n,clustered", [(1_500_000, False), (700_001, True)])
+def test_onesweep_sort_large_is_stable(n, clustered):
+    """The onesweep radix sort over hundreds of tiles (decoupled look-back
+    across them): the build's permutation is the stable sort of the Morton
+    codes (sortperm with Perm ordering, MortonEncoding/toolbox.jl:20-33), also
+    with many duplicate codes (clustered: particles on a coarse lattice)."""
+    rng = np.random.default_rng(99)
+    if clustered:
+        x, y, z = (np.floor(rng.random(n) * 37) / 37 for _ in range(3))
+    else:
+        x, y, z = rng.random(n), rng.random(n), rng.random(n)
+    ctx = Context(0)
+    ctx.set_particles(x, y, z, np.full(n, 1.0 / n), np.full(n, 0.01), np.ones(n))
+    perm, codes = ctx.build(want_perm=True, want_codes=True)
+    raw = O.morton_codes(x, y, z)
+    ref = np.argsort(raw, kind="stable")
+    assert np.array_equal(perm, ref)
+    assert np.all(codes[1:] > codes[:-1])
+
+
 def test_build_duplicates_and_degenerate_axes():
     # identical codes (test/neighbor_search_tests.jl:236-247) and a flat axis
     n = 64

@@ -162,6 +162,14 @@ def host_cpu():
     return {"nproc": os.cpu_count(), "model": model}
 
 
+def roofline_block(b_alg, ms, what):
+    """HBM-roofline fraction of an algorithmic byte count moved in ms."""
+    hbm, kind = peaks()
+    achieved = b_alg / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_kind": kind, "alg_bytes": int(b_alg), "ms": ms, "bytes": what}
+
+
 def make_workload():
     from partia_b200 import workloads as W
     from partia_b200 import linrange
@@ -226,7 +234,7 @@ def cudaext_leg(ctx, d, axis, steps, warmup, ours):
                                   "e2e": hms / ours["e2e_ms"]}}
 
 
-def lines_and_adjoint(steps, warmup):
+def lines_and_adjoint(steps, warmup, n_lines=8_000_000, npix_lines=1024):
     """The line-integrated configurations (clump particles, parallel beam through
     the 30/45-degree frame over [0,1]^2, scatter, column density = plain scalar
     rho): forward throughput of 8M particles x 1024^2 lines in FP32C and FP64,
@@ -249,10 +257,10 @@ def lines_and_adjoint(steps, warmup):
         return ctx
 
     # 8M particles, 1024^2 lines
-    d = W.clumps(8_000_000, 2)
+    d = W.clumps(n_lines, 2)
     h, rho = W.density_h(d)
     ctx = context(d, h, rho)
-    npix = 1024
+    npix = npix_lines
     out32 = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
     out64 = [torch.empty(npix * npix, dtype=torch.float64, device="cuda")]
     f32 = lambda: ctx.interp_beam(fr, prm, npix, npix, cat, strategy=L.PSB_SCATTER, prec=L.PSB_PREC_FP32C, out=out32)
@@ -268,11 +276,16 @@ def lines_and_adjoint(steps, warmup):
     t1000 = timed_call(f32, stream, steps, warmup)
     ctx.extra_flags = 0
     err1000 = ((out32[0][fin] - b[fin]).abs().max() / b[fin].abs().max()).item()
-    res["lines"] = {"workload": "clumps-8M column density, 1024^2 parallel beam, scatter", "N": 8_000_000,
+    res["lines"] = {"workload": f"clumps-{n_lines / 1e6:g}M column density, {npix}^2 parallel beam, scatter",
+                    "N": n_lines,
                     "lines": npix * npix, "pairs": int(pairs), "fp32c_ms": t32, "fp64_ms": t64,
                     "lines_per_s": npix * npix / (t32 / 1e3), "fp64_lines_per_s": npix * npix / (t64 / 1e3),
                     "speedup_fp32c_vs_fp64": t64 / t32, "fp32c_rel_err_vs_fp64": err,
-                    "lut1000_f32": {"fp32c_ms": t1000, "rel_err_vs_fp64_lut4096": err1000}}
+                    "lut1000_f32": {"fp32c_ms": t1000, "rel_err_vs_fp64_lut4096": err1000},
+                    # beam lines are generated on the device (S_in = 0); 1 output of 8 B per line;
+                    # the FP32C pair record is x, y, z, h, m, rho + 1 column in float (28 B)
+                    "roofline": roofline_block(npix * npix * 8 + int(pairs) * (6 + 1) * 4, t32,
+                                               "lines x 8 B out + pairs x 28 B (FP32C records)")}
     ctx.close()
     del out32, out64
 
@@ -387,7 +400,11 @@ def large_leg(steps, warmup, oracle_check=True, n=64_000_000, ng=256):
             "speedup_fp32c_vs_fp64": res["fp64"]["ms"] / res["fp32c"]["ms"],
             "fp32c_rel_err_vs_fp64": errs(outs["fp32c"], outs["fp64"]),
             "float32_storage_rel_err_vs_fp64": errs(outs["float32_storage"], outs["fp64"]),
-            "oracle_subset": ora, "adjoint": res["adjoint"]}
+            "oracle_subset": ora, "adjoint": res["adjoint"],
+            # grid and box samples are generated on the device (S_in = 0); 8 outputs of 8 B;
+            # the FP32C pair record is x, y, z, h, m, rho + 5 columns in float (44 B)
+            "roofline": roofline_block(ns * 8 * 8 + res["fp32c"]["pairs"] * (6 + 5) * 4, res["fp32c"]["ms"],
+                                       "samples x 64 B out + pairs x 44 B (FP32C records)")}
 
 
 def kernel_families(d, axis, steps, warmup):
@@ -609,6 +626,10 @@ def main():
     ap.add_argument("--no-large", action="store_true", help="skip the 64M-particle leg")
     ap.add_argument("--no-kernels", action="store_true", help="skip the kernel-family leg")
     ap.add_argument("--no-cudaext", action="store_true", help="skip the CUDA-extension design baseline leg")
+    ap.add_argument("--lines-n", type=int, default=8_000_000,
+                    help="particles of the line-integrated leg (8M = the workload; fewer only for profiling captures)")
+    ap.add_argument("--lines-npix", type=int, default=1024,
+                    help="beam pixels per side of the line-integrated leg (1024 = the workload)")
     ap.add_argument("--large-n", type=int, default=64_000_000,
                     help="particles of the large leg (64M = the workload; fewer only for profiling captures)")
     ap.add_argument("--large-grid", type=int, default=256,
@@ -786,7 +807,7 @@ def main():
 
     extra = None
     if world == 1 and not args.no_lines:
-        extra = lines_and_adjoint(max(3, args.steps // 4), 2)
+        extra = lines_and_adjoint(max(3, args.steps // 4), 2, args.lines_n, args.lines_npix)
     kern = None
     if world == 1 and not args.no_kernels:
         kern = kernel_families(d, axis, max(3, args.steps // 4), 2)

@@ -34,6 +34,8 @@
  *    Morton order, the LBVH, reusable scratch).  Calls are synchronous with
  *    respect to the caller.  A context is not thread-safe: use one per host
  *    thread.
+ *  - Each call makes the context's device current while it runs and restores
+ *    the caller's current device before it returns.
  */
 #ifndef PARTIA_B200_H
 #define PARTIA_B200_H

@@ -257,7 +257,8 @@ PSB_API int psb_create(psb_ctx** out, int device) {
     psb_ctx* c = new (std::nothrow) psb_ctx();
     if (!c) return PSB_ENOMEM;
     c->device = device;
-    cudaError_t e = cudaSetDevice(device);
+    DeviceGuard dg(device);
+    cudaError_t e = dg.err;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
     for (int k = 0; k < 8 && e == cudaSuccess; ++k) e = cudaEventCreate(&c->ev[k]);
     if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(unsigned));
@@ -279,7 +280,7 @@ PSB_API int psb_create(psb_ctx** out, int device) {
 
 PSB_API int psb_destroy(psb_ctx* c) {
     if (!c) return PSB_OK;
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     release_buffers(c);
     if (c->sctx) psb_destroy(c->sctx);
@@ -332,7 +333,7 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
     if (n > 0 && ncol > 0 && !cols) return fail(c, PSB_EINVAL, "column pointer array must not be NULL");
     for (int k = 0; n > 0 && k < ncol; ++k)
         if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if ((flags & PSB_FLAG_DEVICE_PTRS) && n > 0) {
         int rc = PSB_OK;
         for (const void* p : {x, y, z, m, h, rho})
@@ -376,7 +377,7 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
 PSB_API int psb_build_lbvh(psb_ctx* c, int64_t* perm_out, uint64_t* codes_out) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = build_lbvh(c);
     if (rc) return rc;
     if (perm_out) PSB_CUDA_TRY(c, cudaMemcpyAsync(perm_out, c->order, sizeof(int64_t) * c->n, cudaMemcpyDeviceToHost, c->stream), "perm D2H");
@@ -395,7 +396,7 @@ PSB_API int psb_set_values(psb_ctx* c, const void* m, const void* rho, int32_t n
     if (ncol > 0 && !cols) return fail(c, PSB_EINVAL, "column pointer array must not be NULL");
     for (int k = 0; k < ncol; ++k)
         if (!cols[k]) return fail(c, PSB_EINVAL, "column " + std::to_string(k) + " is NULL");
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (flags & PSB_FLAG_DEVICE_PTRS) {
         int rc = check_device_ptr(c, m, "the mass array");
         if (!rc) rc = check_device_ptr(c, rho, "the density array");
@@ -431,7 +432,7 @@ PSB_API int psb_set_values(psb_ctx* c, const void* m, const void* rho, int32_t n
 PSB_API int psb_test_loop_escapes(psb_ctx* c) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     return loop_escapes(c);
 }
 
@@ -439,7 +440,7 @@ PSB_API int psb_get_tree(psb_ctx* c, int32_t* root, int32_t* left, int32_t* righ
                          double* node_min, double* node_max, double* node_scale) {
     if (!c) return PSB_EINVAL;
     if (!c->built) return fail(c, PSB_ESTATE, "psb_build_lbvh must run first");
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     const int64_t tot = 2 * c->n - 1, nint = c->n - 1;
     if (root) *root = c->root;
     int32_t* src[4] = {c->left, c->right, c->escape, c->parent};
@@ -483,7 +484,7 @@ PSB_API int psb_interp_points(psb_ctx* c, int64_t ns, const void* sx, const void
                               void* const* out, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_samples(c, ns, sx, sy, sz);
     if (rc) return rc;
     return run(c, points_req(ns, sx, sy, sz), hmode, hs, strategy, cat, prec, out, flags, stats, WHAT_INTERP, nullptr,
@@ -496,7 +497,7 @@ PSB_API int psb_interp_grid(psb_ctx* c, const void* ax, int64_t nx, const void* 
                             psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (nx < 0 || ny < 0 || nz < 0) return fail(c, PSB_EINVAL, "grid sizes must be non-negative");
     if ((nx > 0 && !ax) || (ny > 0 && !ay) || (nz > 0 && !az)) return fail(c, PSB_EINVAL, "axis arrays must not be NULL");
     SampleReq r;
@@ -529,7 +530,7 @@ PSB_API int psb_interp_box(psb_ctx* c, const void* frame, const void* params, in
                            psb_precision prec, void* const* out, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_frame(c, frame, params, nx, ny, nz, true);
     if (rc) return rc;
     SampleReq r;
@@ -546,7 +547,7 @@ PSB_API int psb_interp_lines(psb_ctx* c, int64_t nl, const void* ox, const void*
                              uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_samples(c, nl, ox, oy, oz);
     if (!rc) rc = check_samples(c, nl, dx, dy, dz);
     if (rc) return rc;
@@ -561,7 +562,7 @@ PSB_API int psb_interp_beam(psb_ctx* c, const void* frame, const void* params, i
                             psb_precision prec, void* const* out, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_frame(c, frame, params, nx, ny, 1, false);
     if (rc) return rc;
     SampleReq r;
@@ -578,7 +579,7 @@ PSB_API int psb_density(psb_ctx* c, int64_t ns, const void* sx, const void* sy, 
                         psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_samples(c, ns, sx, sy, sz);
     if (rc) return rc;
     void* outs[1] = {out};
@@ -592,7 +593,7 @@ PSB_API int psb_neighbor_digest(psb_ctx* c, int32_t kind, int64_t ns, const void
                                 uint32_t flags) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (kind != 0 && kind != 1) return fail(c, PSB_EINVAL, "kind must be 0 (points) or 1 (lines)");
     int rc = check_samples(c, ns, ax, ay, az);
     if (!rc && kind == 1) rc = check_samples(c, ns, dx, dy, dz);
@@ -622,7 +623,7 @@ PSB_API int psb_adjoint_points(psb_ctx* c, int64_t ns, const void* sx, const voi
                                double* gz, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_samples(c, ns, sx, sy, sz);
     if (rc) return rc;
     return run_adjoint(c, points_req(ns, sx, sy, sz), hmode, hs, strategy, cat, gout, gm, gcols, gx, gy, gz, flags,
@@ -635,7 +636,7 @@ PSB_API int psb_adjoint_grid(psb_ctx* c, const void* ax, int64_t nx, const void*
                              double* gx, double* gy, double* gz, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (nx < 0 || ny < 0 || nz < 0) return fail(c, PSB_EINVAL, "grid sizes must be non-negative");
     if ((nx > 0 && !ax) || (ny > 0 && !ay) || (nz > 0 && !az)) return fail(c, PSB_EINVAL, "axis arrays must not be NULL");
     SampleReq r;
@@ -652,7 +653,7 @@ PSB_API int psb_adjoint_beam(psb_ctx* c, const void* frame, const void* params, 
                              double* gz, uint32_t flags, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     int rc = check_frame(c, frame, params, nx, ny, 1, false);
     if (rc) return rc;
     SampleReq r;

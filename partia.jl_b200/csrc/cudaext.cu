@@ -166,7 +166,7 @@ extern "C" __attribute__((visibility("default"))) int psb_baseline_cudaext_point
     double* const* out, psb_stats* stats) {
     if (!c) return PSB_EINVAL;
     c->err.clear();
-    cudaSetDevice(c->device);
+    DeviceGuard dg(c->device);
     if (n < 1) return fail(c, PSB_EINVAL, "particle count must be positive");
     if (ns < 0) return fail(c, PSB_EINVAL, "sample count must be non-negative");
     if (ncol < 0 || (ncol > 0 && !cols)) return fail(c, PSB_EINVAL, "bad column arrays");

@@ -532,17 +532,25 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const float dz = R0[2] - Lj.z;
             const float d2 = dx * dx + dy * dy + dz * dz;
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-            const float r = d2 * invr;
+            float r = d2 * invr;
             float Wsum = 0.f, csum = 0.f;
             const int64_t li = st.lo[b] + j;
-            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
-            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
             double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            if (qa >= qe || qb >= qe) {
+            bool have_d2d = false;
+            auto exact_d2 = [&]() {
                 const double ex = (double)p[0] - (double)tv.x[li], ey = (double)p[1] - (double)tv.y[li],
                              ez = (double)p[2] - (double)tv.z[li];
                 d2d = fma(ex, ex, fma(ey, ey, ez * ez));
+                have_d2d = true;
+            };
+            const bool wend = KF == 1 && tv.kern >= KERN_C2;  // one Wendland piece up to the edge
+            if (wend) {  // r (hence q) from the exact separation, for every q
+                exact_d2();
+                r = sqrtf((float)d2d);
             }
+            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
+            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
+            if (!have_d2d && (qa >= qe || qb >= qe)) exact_d2();
             if (ST != ST_SCATTER) {
                 float f, df;
                 kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
@@ -551,7 +559,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                const double hbK = qb >= qe ? tv.Kd * (double)tv.h[li] : 0.0;
+                const double hbK = (qb >= qe || wend) ? tv.Kd * (double)tv.h[li] : 0.0;
                 kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), Lj.w, tv.Kf, f, df);
                 if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
                 else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }

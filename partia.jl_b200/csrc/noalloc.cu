@@ -273,8 +273,8 @@ extern "C" __attribute__((visibility("default"))) int psb_interp_points_noalloc(
     if (strategy < 0 || strategy > 2) return fail(c, PSB_EINVAL, "unknown interpolation strategy");
     if (prec < 0 || prec > 1) return fail(c, PSB_EINVAL, "unknown precision mode");
     if (hmode < 0 || hmode > 2) return fail(c, PSB_EINVAL, "unknown smoothing-length mode");
-    cudaError_t e = cudaSetDevice(c->device);
-    if (e != cudaSuccess) return cuda_fail(c, e, "cudaSetDevice");
+    DeviceGuard dg(c->device);
+    if (dg.err != cudaSuccess) return cuda_fail(c, dg.err, "cudaSetDevice");
     return c->dt == PSB_F64 ? noalloc_typed<double>(c, ns, sx, sy, sz, hmode, hs, strategy, cat, prec, out, stats)
                             : noalloc_typed<float>(c, ns, sx, sy, sz, hmode, hs, strategy, cat, prec, out, stats);
 }

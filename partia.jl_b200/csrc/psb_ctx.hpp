@@ -85,6 +85,23 @@ struct psb_ctx {
 
 namespace psb {
 
+// The context's device for the duration of an entry point; the caller's
+// current device is restored on return.
+struct DeviceGuard {
+    int prev = -1, dev;
+    explicit DeviceGuard(int d) : dev(d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) {
+            cudaGetLastError();
+            prev = -1;
+        }
+        if (prev != dev) err = cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0 && prev != dev) cudaSetDevice(prev);
+    }
+    cudaError_t err = cudaSuccess;
+};
+
 // Record an error message on the context and return the code.
 int fail(psb_ctx* c, int code, const std::string& msg);
 // PSB_ETRAVERSAL with the message of a nonzero device error word (read back

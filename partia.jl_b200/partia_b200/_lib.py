@@ -10,7 +10,8 @@ import os
 import re
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "_lib", "libpartia_b200.so")
+# the in-tree build, unless PARTIA_B200_LIB names another build of the same ABI
+LIB_PATH = os.environ.get("PARTIA_B200_LIB") or os.path.join(_HERE, "_lib", "libpartia_b200.so")
 HEADER_PATH = os.path.normpath(os.path.join(_HERE, "..", "..", "include", "partia_b200.h"))
 
 PSB_OK = 0

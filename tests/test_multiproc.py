@@ -185,3 +185,34 @@ def test_weighted_ranges_and_morton_order():
     hi_x = (q >= 2 ** 20)[o]
     k = int(np.count_nonzero(~hi_x))
     assert not np.any(hi_x[:k]) and np.all(hi_x[k:])
+
+
+def test_plane_pair_estimates_with_the_oracle_digest():
+    """plane_pair_estimates' layout logic (subsampled x-y points of every
+    z-plane, column-major) on a stand-in context whose digest is the oracle's;
+    equal to the per-plane sums of the subsample's pair counts, scaled."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from partia_b200 import _lib as L
+    from partia_b200.sharding import plane_pair_estimates, weighted_slabs
+    P, cols, _, _ = _clustered_case()
+    orc = O.Oracle(*P, cols)
+
+    class OracleDigest:
+        def digest(self, a, strategy=None, hmode=None):
+            return orc.digest(a, strategy=O.SYMMETRIC, hmode=O.H_NEAREST)
+
+    ax = np.linspace(-0.4, 0.4, 24)
+    w = plane_pair_estimates(OracleDigest(), ax, ax, ax, stride=4, strategy=L.PSB_SYMMETRIC,
+                             hmode=L.PSB_H_NEAREST)
+    assert w.shape == (24,)
+    sub = ax[::4]
+    for k in (0, 11, 23):
+        X, Y = np.meshgrid(sub, sub, indexing="ij")
+        cnt, _, _ = orc.digest((X.ravel(), Y.ravel(), np.full(X.size, ax[k])), strategy=O.SYMMETRIC,
+                               hmode=O.H_NEAREST)
+        assert w[k] == pytest.approx(cnt.sum() * (24 * 24) / sub.size ** 2)
+    # the clustered core holds most pairs: the middle slab is the thinnest
+    slabs = weighted_slabs(w, 3)
+    sizes = [hi - lo for lo, hi in slabs]
+    assert sizes[1] < sizes[0] and sizes[1] < sizes[2]

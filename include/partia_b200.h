@@ -193,7 +193,10 @@ int psb_set_particles(psb_ctx* ctx, int64_t n, psb_dtype dt,
  * Morton codes -> radix sort -> dedup -> Karras radix tree -> escape links ->
  * bottom-up AABB refit, on the device.  The device copies of all particle
  * arrays are permuted into Morton order.  perm_out[i] (host, nullable) is the
- * 0-based original index of the particle at Morton position i (enc.order - 1);
+ * 0-based original index of the particle at Morton position i (enc.order - 1),
+ * original meaning the order psb_set_particles was given (also when the LBVH
+ * is built again without new particles: the device copies are then already in
+ * Morton order, and the permutation stays relative to the caller's arrays);
  * codes_out (host, nullable) receives the sorted, de-duplicated codes.  A
  * caller that mirrors Partia's in-place contract applies perm_out to its own
  * arrays. */

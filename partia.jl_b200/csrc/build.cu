@@ -118,6 +118,12 @@ __global__ void k_order64(const uint32_t* idx, int64_t n, int64_t* order) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) order[i] = (int64_t)idx[i];
 }
+// a rebuild of arrays an earlier build already permuted: the caller's index of
+// new position i is that of old position idx[i]
+__global__ void k_compose_order(const uint32_t* idx, int64_t n, const int64_t* prev, int64_t* order) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) order[i] = prev[idx[i]];
+}
 
 // ---- 6. Karras radix tree ----------------------------------------------------------
 // delta(i, j) with 1-based i, j: MortonEncoding/toolbox.jl:329-336
@@ -393,9 +399,20 @@ static int build_typed(psb_ctx* c) {
     PSB_CUDA_TRY(c, cudaGetLastError(), "dedup kernels");
 
     // 5. permute particle arrays into Morton order
+    // order: the index each Morton position had when psb_set_particles gave
+    // the arrays, also across repeated builds of the same (already permuted)
+    // device arrays
     PSB_CUDA_TRY(c, dgrow_t(c, &c->order, sizeof(int64_t) * n), "cudaMalloc order");
-    k_order64<<<grid_for(n), BT, 0, s>>>(idx, n, c->order);
-    T* tmp = (T*)scratch(c, 3, es * n);  // dedup values are consumed
+    if (c->order_fresh) {
+        k_order64<<<grid_for(n), BT, 0, s>>>(idx, n, c->order);
+    } else {
+        int64_t* ord2 = (int64_t*)scratch(c, 3, sizeof(int64_t) * n);  // dedup values are consumed
+        if (!ord2) return fail(c, PSB_ENOMEM, "scratch allocation failed (order)");
+        k_compose_order<<<grid_for(n), BT, 0, s>>>(idx, n, c->order, ord2);
+        PSB_CUDA_TRY(c, cudaMemcpyAsync(c->order, ord2, sizeof(int64_t) * n, cudaMemcpyDeviceToDevice, s), "order copy");
+    }
+    c->order_fresh = false;
+    T* tmp = (T*)scratch(c, 3, es * n);  // dedup values and the order copy are consumed
     if (!tmp) return fail(c, PSB_ENOMEM, "scratch allocation failed (permute)");
     std::vector<void*> arrays = {c->x, c->y, c->z, c->m, c->h, c->rho};
     for (void* col : c->cols) arrays.push_back(col);

@@ -342,6 +342,7 @@ PSB_API int psb_set_particles(psb_ctx* c, int64_t n, psb_dtype dt, const void* x
         if (rc) return rc;
     }
     reset_tree(c);
+    c->order_fresh = true;
     PSB_CUDA_TRY(c, load_line_tables(c, (int)kernel), "line table upload");
     c->dt = dt;
     c->es = (dt == PSB_F64) ? 8 : 4;

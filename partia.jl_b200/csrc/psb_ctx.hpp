@@ -32,7 +32,8 @@ struct psb_ctx {
     bool built = false;
     int32_t root = 0;
     uint64_t* codes = nullptr;
-    int64_t* order = nullptr;
+    int64_t* order = nullptr;       // caller's index (as given to psb_set_particles) of each Morton position
+    bool order_fresh = true;        // device arrays still in the caller's order (no build since set_particles)
     int32_t* left = nullptr; int32_t* right = nullptr;
     int32_t* escape = nullptr; int32_t* parent = nullptr;
     int32_t* range_lo = nullptr; int32_t* range_hi = nullptr;

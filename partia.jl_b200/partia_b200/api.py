@@ -225,6 +225,14 @@ def build_input(backend, x_col, y_col, z_col, m_col, h_col, rho_col, quantity_co
 # ---------------------------------------------------------------------------
 # sample containers
 # ---------------------------------------------------------------------------
+def _vectors(t):
+    """The caller's tuple itself when it already holds arrays, so that
+    containers made by similar() share one coordinate tuple, as Julia's do."""
+    if isinstance(t, tuple) and all(isinstance(c, np.ndarray) for c in t):
+        return t
+    return tuple(np.asarray(c) for c in t)
+
+
 class PointSamples:
     def __init__(self, grid, coor):
         grid = np.asarray(grid)
@@ -232,7 +240,7 @@ class PointSamples:
             if len(c) != len(grid):
                 raise DimensionMismatch(f"coor[{d + 1}] length {len(c)} != grid length {len(grid)}")
         self.grid = grid
-        self.coor = tuple(np.asarray(c) for c in coor)
+        self.coor = _vectors(coor)
 
     def __len__(self):
         return len(self.grid)
@@ -248,8 +256,8 @@ class LineSamples:
             if len(origin[d]) != len(grid) or len(direction[d]) != len(grid):
                 raise DimensionMismatch("origin/direction lengths must match the grid length")
         self.grid = grid
-        self.origin = tuple(np.asarray(c) for c in origin)
-        self.direction = tuple(np.asarray(c) for c in direction)
+        self.origin = _vectors(origin)
+        self.direction = _vectors(direction)
 
     def __len__(self):
         return len(self.grid)

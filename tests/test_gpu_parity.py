@@ -101,6 +101,29 @@ def test_onesweep_sort_large_is_stable(n, clustered):
     assert np.all(codes[1:] > codes[:-1])
 
 
+def test_rebuild_keeps_the_callers_order():
+    """psb_build_lbvh again without new particles: the device copies are
+    already in Morton order, and the permutation (and with it every adjoint
+    gradient, returned in the caller's order) stays relative to the arrays
+    psb_set_particles was given."""
+    arrs, cols = make_particles(20_000, 61)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    perm1, codes1 = ctx.build(want_codes=True)
+    rng = np.random.default_rng(62)
+    s = tuple(rng.uniform(0.1, 0.9, 2000) for _ in range(3))
+    cat = CatalogC(scalars=[1], shepard=[1], grads=[-1])
+    gout = [rng.standard_normal(2000) for _ in range(cat.L)]
+    g1 = ctx.adjoint_points(*s, cat, gout, strategy=L.PSB_SYMMETRIC)
+    perm2, codes2 = ctx.build(want_codes=True)
+    assert np.array_equal(perm1, perm2) and np.array_equal(codes1, codes2)
+    g2 = ctx.adjoint_points(*s, cat, gout, strategy=L.PSB_SYMMETRIC)
+    for key in ("m", "x", "y", "z"):
+        assert np.array_equal(g1[key], g2[key]), key
+    for a, b in zip(g1["cols"], g2["cols"]):
+        assert np.array_equal(a, b)
+
+
 def test_build_duplicates_and_degenerate_axes():
     # identical codes (test/neighbor_search_tests.jl:236-247) and a flat axis
     n = 64

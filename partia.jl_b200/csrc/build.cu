@@ -59,16 +59,28 @@ __global__ void k_minmax_partial(const T* x, const T* y, const T* z, int64_t n, 
 
 // bbox[0..5] = min xyz, max xyz; inv[0..2] = 1/(max-min) (0 marks an
 // all-equal axis, which normalises to 0.5).
+// One warp: each lane folds a strided share of the block partials, then the
+// lanes are folded by shuffles (min and max are exact in any order).
 template <class T>
 __global__ void k_minmax_final(const T* part, int nparts, T* bbox, T* inv) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;
+    const int lane = threadIdx.x;
     T v[6];
     for (int k = 0; k < 6; ++k) v[k] = part[k];
-    for (int b = 1; b < nparts; ++b)
+    for (int b = lane; b < nparts; b += 32)
         for (int k = 0; k < 6; ++k) {
             T t = part[(int64_t)b * 6 + k];
             v[k] = (k < 3) ? ((t < v[k]) ? t : v[k]) : ((t > v[k]) ? t : v[k]);
         }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            T t = __shfl_xor_sync(PSB_FULL, v[k], o);
+            v[k] = (k < 3) ? ((t < v[k]) ? t : v[k]) : ((t > v[k]) ? t : v[k]);
+        }
+    }
+    if (lane != 0) return;
     for (int k = 0; k < 6; ++k) bbox[k] = v[k];
     for (int d = 0; d < 3; ++d) {
         T dv = X<T>::sub(v[3 + d], v[d]);

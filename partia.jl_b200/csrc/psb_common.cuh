@@ -26,6 +26,10 @@ namespace psb {
 // A subtree of at most SPAN_LEAVES leaves is handled as one unit ("span") by
 // the traversals; its root is the highest node with at most that many leaves.
 constexpr int SPAN_LEAVES = 32;
+// The traversal kernels size the per-warp stage arrays of a tile's samples
+// (one per lane) and of a span's leaves (one per lane in the leaf-per-lane
+// tests) by the same constant: a span is exactly one warp wide.
+static_assert(SPAN_LEAVES == 32, "a span is one warp wide: stage arrays are indexed by lane");
 
 // ---------------------------------------------------------------------------
 // Exactly rounded arithmetic.  Parity-critical steps (Morton quantisation,

@@ -314,7 +314,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
                                                                     make_double3(sc[0], sc[1], sc[2]), codes, idx);
         PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
         ++launches;
-        PSB_CUDA_TRY(c, radix_sort_pairs(codes, idx, ns, c, 6, &launches, false), "sample sort");
+        PSB_CUDA_TRY(c, radix_sort_pairs(codes, idx, ns, c, 6, &launches, false, SAMPLE_KEY_BITS), "sample sort");
         S.order = idx;
     }
     PSB_CUDA_TRY(c, cudaEventRecord(c->ev[2], s), "event");
@@ -545,7 +545,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
                                                                           codes[b], idx[b]);
             PSB_CUDA_TRY(c, cudaGetLastError(), "sample code kernel");
             ++launches;
-            PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, sort_slot[b], &launches, false), "sample sort");
+            PSB_CUDA_TRY(c, radix_sort_pairs(codes[b], idx[b], cn, c, sort_slot[b], &launches, false, SAMPLE_KEY_BITS), "sample sort");
             S.order = idx[b];
         }
         const bool split = !(flags & PSB_FLAG_SINGLE_KERNEL);

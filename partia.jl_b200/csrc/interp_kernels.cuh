@@ -490,6 +490,13 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
 // Sample ordering: Morton codes of sample positions (line origins) in the
 // particle bounding box, clamped, then the stable radix sort.
 // ---------------------------------------------------------------------------
+// Explicit samples are put in the order of a coarser Morton curve than the
+// particles': the order only groups nearby samples into tiles (every sample's
+// result is independent of its tile), and 10 bits per axis of the particle
+// box (1024 cells) make 30-bit keys, four radix passes instead of eight.
+constexpr int SAMPLE_AXIS_BITS = 10;
+constexpr int SAMPLE_KEY_BITS = 3 * SAMPLE_AXIS_BITS;
+
 template <class T>
 __global__ void k_sample_codes(const T* x, const T* y, const T* z, int64_t ns, double3 lo, double3 sc,
                                uint64_t* codes, uint32_t* idx) {
@@ -502,7 +509,7 @@ __global__ void k_sample_codes(const T* x, const T* y, const T* z, int64_t ns, d
     for (int d = 0; d < 3; ++d) {
         double f = (v[d] - l[d]) * s[d];
         f = f < 0.0 ? 0.0 : (f > 2097151.0 ? 2097151.0 : f);
-        q[d] = (uint64_t)f;
+        q[d] = (uint64_t)f >> (21 - SAMPLE_AXIS_BITS);
     }
     codes[i] = (spread3(q[0]) << 2) | (spread3(q[1]) << 1) | spread3(q[2]);
     idx[i] = (uint32_t)i;

@@ -181,6 +181,8 @@ __device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k
 // in DFS order with the minimum distance.  stage_span(lo, cnt, false) stages
 // the positions of leaves [lo, lo+cnt) in st (Q and eq for float tests, x y z
 // otherwise); st.P / st.px.. hold the samples.
+constexpr int64_t NEAREST_SEED = 8;
+
 template <class T, bool BAND, class Stage, class StageSpan>
 __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, StageSpan& stage_span, int lane,
                                             bool valid, const T p[3], const float pf[3], float pem, int32_t start,
@@ -202,10 +204,11 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
             if (__ldg(&tv.codes[mid]) < code) lo = mid + 1;
             else hi = mid;
         }
-        // the (up to) four particles around that position in Morton order, in
-        // increasing index: the first strict minimum keeps the smallest index
-        const int64_t c0 = lo >= 2 ? lo - 2 : 0;
-        const int64_t c1 = (lo + 2 <= tv.n) ? lo + 2 : tv.n;
+        // the (up to) 2 NEAREST_SEED particles around that position in Morton
+        // order, in increasing index: the first strict minimum keeps the
+        // smallest index.  A closer seed prunes more of the walk.
+        const int64_t c0 = lo >= NEAREST_SEED ? lo - NEAREST_SEED : 0;
+        const int64_t c1 = (lo + NEAREST_SEED <= tv.n) ? lo + NEAREST_SEED : tv.n;
         for (int64_t ci = c0; ci < c1; ++ci) {
             const double dc = (double)ex_d2_pp<T>(p, tv.x[ci], tv.y[ci], tv.z[ci]);
             if (dc < best) { best = dc; bidx = ci; }
@@ -532,25 +535,17 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const float dz = R0[2] - Lj.z;
             const float d2 = dx * dx + dy * dy + dz * dz;
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-            float r = d2 * invr;
+            const float r = d2 * invr;
             float Wsum = 0.f, csum = 0.f;
             const int64_t li = st.lo[b] + j;
+            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
+            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
             double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            bool have_d2d = false;
-            auto exact_d2 = [&]() {
+            if (qa >= qe || qb >= qe) {
                 const double ex = (double)p[0] - (double)tv.x[li], ey = (double)p[1] - (double)tv.y[li],
                              ez = (double)p[2] - (double)tv.z[li];
                 d2d = fma(ex, ex, fma(ey, ey, ez * ez));
-                have_d2d = true;
-            };
-            const bool wend = KF == 1 && tv.kern >= KERN_C2;  // one Wendland piece up to the edge
-            if (wend) {  // r (hence q) from the exact separation, for every q
-                exact_d2();
-                r = sqrtf((float)d2d);
             }
-            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
-            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
-            if (!have_d2d && (qa >= qe || qb >= qe)) exact_d2();
             if (ST != ST_SCATTER) {
                 float f, df;
                 kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
@@ -559,7 +554,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             }
             if (ST != ST_GATHER) {
                 float f, df;
-                const double hbK = (qb >= qe || wend) ? tv.Kd * (double)tv.h[li] : 0.0;
+                const double hbK = qb >= qe ? tv.Kd * (double)tv.h[li] : 0.0;
                 kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), Lj.w, tv.Kf, f, df);
                 if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
                 else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }

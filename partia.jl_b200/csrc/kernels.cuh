@@ -97,9 +97,7 @@ template <class C> __device__ __forceinline__ void kern_fdf(int k, C q, C& f, C&
     }
 }
 
-// f and f' for k != M4 in the float pair sums of double inputs.  For the
-// Wendland kernels (one piece up to the support edge) the callers take q and
-// r from the exact squared separation.  The
+// f and f' for k != M4 in the float pair sums of double inputs.  The
 // innermost spline pieces are expanded (M5 on q < 1/2: 14.375 - 15 q^2 + 6 q^4,
 // M6 on q < 1: 66 - 60 q^2 + 30 q^4 - 10 q^5), so f' carries its factor q
 // exactly instead of a difference of terms of size ~70.  On the piece that
@@ -145,9 +143,7 @@ __device__ __forceinline__ void kern_fdf_f32(int k, float q, float r, float num,
         }
         break;
     case KERN_C2: case KERN_C4: case KERN_C6: {
-        // a = 1 - q/2 = (2 - q)/2 from the double numerator for every q: the
-        // steep powers a^4..a^8 would multiply the relative error of a float q
-        const float a = 0.5f * u;
+        const float a = (q < 1.f) ? 1.f - 0.5f * q : 0.5f * u;
         const float a2 = a * a;
         if (k == KERN_C2) {
             const float a3 = a2 * a;

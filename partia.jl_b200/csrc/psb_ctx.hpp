@@ -144,8 +144,9 @@ cudaError_t inclusive_max_scan_i64(int64_t* data, int64_t n, psb_ctx* c, int slo
 // back which digits vary (one host sync) and sort only those; otherwise all
 // eight passes run without a host round trip.  A look-back wait that runs
 // out sets PSB_DERR_SORT in the context's error word.
+// key_bits: the keys are below 2^key_bits (the digits above are not sorted).
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches,
-                             bool skip_constant_digits = true);
+                             bool skip_constant_digits = true, int key_bits = 64);
 // The same sort on caller-provided scratch of at least
 // radix_sort_pairs_scratch_bytes(n) bytes (256-byte aligned); allocates nothing.
 size_t radix_sort_pairs_scratch_bytes(int64_t n);

@@ -341,7 +341,7 @@ SortSpace carve(char* sp, int64_t n, int64_t ntiles) {
 // back (one host synchronisation) and runs only their passes; otherwise all
 // eight passes run without a host round trip.
 cudaError_t onesweep(uint64_t* keys, uint32_t* vals, int64_t n, const SortSpace& S, cudaStream_t s, unsigned* err,
-                     int* launches, bool skip_constant_digits) {
+                     int* launches, bool skip_constant_digits, int key_bits = 64) {
     const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
     cudaError_t e;
     // vary | hist | tickets are contiguous: one memset
@@ -357,7 +357,7 @@ cudaError_t onesweep(uint64_t* keys, uint32_t* vals, int64_t n, const SortSpace&
     }
     uint64_t* ksrc = keys; uint32_t* vsrc = vals;
     uint64_t* kdst = S.kalt; uint32_t* vdst = S.valt;
-    for (int d = 0; d < RS_DIGITS; ++d) {
+    for (int d = 0; d < RS_DIGITS && 8 * d < key_bits; ++d) {
         if (((vary >> (8 * d)) & 255ull) == 0) continue;
         if ((e = cudaMemsetAsync(S.status, 0, sizeof(unsigned long long) * 256 * (size_t)ntiles, s)) != cudaSuccess)
             return e;
@@ -376,12 +376,13 @@ cudaError_t onesweep(uint64_t* keys, uint32_t* vals, int64_t n, const SortSpace&
 }  // namespace
 
 cudaError_t radix_sort_pairs(uint64_t* keys, uint32_t* vals, int64_t n, psb_ctx* c, int slot_base, int* launches,
-                             bool skip_constant_digits) {
+                             bool skip_constant_digits, int key_bits) {
     if (n <= 1) return cudaSuccess;
     const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
     char* sp = (char*)scratch(c, slot_base, sort_space_bytes(n, ntiles));
     if (!sp) return cudaErrorMemoryAllocation;
-    return onesweep(keys, vals, n, carve(sp, n, ntiles), c->stream, c->d_err, launches, skip_constant_digits);
+    return onesweep(keys, vals, n, carve(sp, n, ntiles), c->stream, c->d_err, launches, skip_constant_digits,
+                    key_bits);
 }
 
 size_t radix_sort_pairs_scratch_bytes(int64_t n) {

@@ -315,6 +315,7 @@ template <class T, int KC> struct PairData<T, true, KC> {
     float col[KC];
     float mb;         // mass (density gradient only)
     float r[3];       // the sample relative to the span's first leaf
+    int64_t li;       // leaf index
     double xd, yd, zd, hd;  // the particle in double (outer kernel piece)
     __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool need_dg,
                                          const float* Rs) {
@@ -324,6 +325,7 @@ template <class T, int KC> struct PairData<T, true, KC> {
         for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&A.colF[c][li]) : 0.f;
         mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
         r[0] = Rs[0]; r[1] = Rs[1]; r[2] = Rs[2];
+        this->li = li;
         xd = __ldg(&tv.x[li]); yd = __ldg(&tv.y[li]); zd = __ldg(&tv.z[li]); hd = __ldg(&tv.h[li]);
     }
 };
@@ -442,23 +444,15 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
             const float dz = cur.r[2] - cur.L.z;
             const float d2 = dx * dx + dy * dy + dz * dz;
             const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-            float r = d2 * invr;
+            const float r = d2 * invr;
             float Wsum = 0.f, csum = 0.f;
-            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            bool have_d2d = false;
-            auto exact_d2 = [&]() {
-                const double ex = (double)p[0] - cur.xd, ey = (double)p[1] - cur.yd, ez = (double)p[2] - cur.zd;
-                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
-                have_d2d = true;
-            };
-            const bool wend = KF == 1 && tv.kern >= KERN_C2;  // one Wendland piece up to the edge
-            if (wend) {  // r (hence q) from the exact separation, for every q
-                exact_d2();
-                r = sqrtf((float)d2d);
-            }
             const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
             const float qb = (ST != ST_GATHER) ? r * cur.K.x : 0.f;
-            if (!have_d2d && (qa >= qe || qb >= qe)) exact_d2();
+            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
+            if (qa >= qe || qb >= qe) {
+                const double ex = (double)p[0] - cur.xd, ey = (double)p[1] - cur.yd, ez = (double)p[2] - cur.zd;
+                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
+            }
             if (ST != ST_SCATTER) {
                 float f, df;
                 kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);

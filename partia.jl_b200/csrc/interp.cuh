@@ -127,14 +127,22 @@ template <class C> __device__ __forceinline__ void m4_fdf(C q, C& f, C& df) {
 // a would carry an absolute error of a few float ulps, a relative error of
 // about 1e-6 at q = 1 that grows without bound towards the support edge,
 // where a sample with few neighbours still gets most of its weight.
+//
+// Every rounding of the float pair terms is written out (__fmul_rn,
+// __fmaf_rn, ...), here, in kern_fdf_f32 and in f32c_pair_weights: a product
+// and a sum left to the compiler may or may not be contracted into one fused
+// multiply-add depending on the code around the inlined call, and the single
+// kernel and the pair-sum kernel must give a pair the same bits.
 __device__ __forceinline__ void m4_fdf_edge(float q, float r, float num, float hf, float& f, float& df) {
     if (q < 1.f) {
-        m4_fdf<float>(q, f, df);
+        f = __fmaf_rn(__fmul_rn(q, q), __fmaf_rn(0.75f, q, -1.5f), 1.f);
+        df = __fmul_rn(q, __fmaf_rn(2.25f, q, -3.f));
         return;
     }
-    const float a = fmaxf(__fdividef(num, hf * (2.f * hf + r)), 0.f);
-    f = 0.25f * a * a * a;
-    df = -0.75f * a * a;
+    const float a = fmaxf(__fdividef(num, __fmul_rn(hf, __fmaf_rn(2.f, hf, r))), 0.f);
+    const float a2 = __fmul_rn(a, a);
+    f = __fmul_rn(__fmul_rn(0.25f, a2), a);
+    df = __fmul_rn(-0.75f, a2);
 }
 
 // f, f' of the kernel family: KF = 0 is M4 (its own forms above), KF = 1 any
@@ -148,6 +156,47 @@ template <int KF> __device__ __forceinline__ void kfdf_edge(int kern, float q, f
                                                             float& f, float& df) {
     if constexpr (KF == 0) m4_fdf_edge(q, r, num, hf, f, df);
     else kern_fdf_f32(kern, q, r, num, hf, Kf, f, df);
+}
+
+// The FP32C weights of one pair of a double particle set (both pair-sum
+// kernels): d = (dx, dy, dz) is the sample minus the particle in float, ia,
+// sa3, sa4 the sample's 1/h, sigma/h^3, sigma/h^4, fa2 = (K h_a)^2 and haf =
+// h_a; K is the particle's leafK record (1/h, sigma/h^3, sigma/h^4, m/rho),
+// hbf its h in float.  exact_d2() returns the squared separation in double
+// (called only for the outer kernel piece), hb_K() K h_b in double.  Returns
+// the weight W (Wsum) and the gradient factor csum (grad W = csum d).
+template <int ST, int KF, class ExactD2, class HbK>
+__device__ __forceinline__ void f32c_pair_weights(int kern, float Kf, float qe, float dx, float dy, float dz, float ia,
+                                                  float sa3, float sa4, double fa2, float haf, float4 K, float hbf,
+                                                  ExactD2 exact_d2, HbK hb_K, float& Wsum, float& csum) {
+    const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
+    const float r = __fmul_rn(d2, invr);
+    const float qa = (ST != ST_SCATTER) ? __fmul_rn(r, ia) : 0.f;
+    const float qb = (ST != ST_GATHER) ? __fmul_rn(r, K.x) : 0.f;
+    double d2d = 0.0;
+    if (qa >= qe || qb >= qe) d2d = exact_d2();
+    Wsum = 0.f;
+    csum = 0.f;
+    if (ST != ST_SCATTER) {
+        float f, df;
+        kfdf_edge<KF>(kern, qa, r, (float)__dadd_rn(fa2, -d2d), haf, Kf, f, df);
+        Wsum = __fmul_rn(sa3, f);
+        csum = __fmul_rn(sa4, df);
+    }
+    if (ST != ST_GATHER) {
+        float f, df;
+        const double hbK = qb >= qe ? hb_K() : 0.0;
+        kfdf_edge<KF>(kern, qb, r, (float)__fma_rn(hbK, hbK, -d2d), hbf, Kf, f, df);
+        if (ST == ST_SCATTER) {
+            Wsum = __fmul_rn(K.y, f);
+            csum = __fmul_rn(K.z, df);
+        } else {
+            Wsum = __fmul_rn(0.5f, __fmaf_rn(K.y, f, Wsum));
+            csum = __fmul_rn(0.5f, __fmaf_rn(K.z, df, csum));
+        }
+    }
+    csum = __fmul_rn(csum, invr);
 }
 
 template <class C> __device__ __forceinline__ C m4_f(C q) {

@@ -530,43 +530,27 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             }
             const float4 Lj = st.Lr[slot];
             const float4 K = st.K[slot];
-            const float dx = R0[0] - Lj.x;
-            const float dy = R0[1] - Lj.y;
-            const float dz = R0[2] - Lj.z;
-            const float d2 = dx * dx + dy * dy + dz * dz;
-            const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-            const float r = d2 * invr;
-            float Wsum = 0.f, csum = 0.f;
+            const float dx = __fsub_rn(R0[0], Lj.x);
+            const float dy = __fsub_rn(R0[1], Lj.y);
+            const float dz = __fsub_rn(R0[2], Lj.z);
             const int64_t li = st.lo[b] + j;
-            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
-            const float qb = (ST != ST_GATHER) ? r * K.x : 0.f;
-            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            if (qa >= qe || qb >= qe) {
-                const double ex = (double)p[0] - (double)tv.x[li], ey = (double)p[1] - (double)tv.y[li],
-                             ez = (double)p[2] - (double)tv.z[li];
-                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
-            }
-            if (ST != ST_SCATTER) {
-                float f, df;
-                kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
-                Wsum = (float)sa3 * f;
-                csum = (float)sa4 * df;
-            }
-            if (ST != ST_GATHER) {
-                float f, df;
-                const double hbK = qb >= qe ? tv.Kd * (double)tv.h[li] : 0.0;
-                kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), Lj.w, tv.Kf, f, df);
-                if (ST == ST_SCATTER) { Wsum = K.y * f; csum = K.z * df; }
-                else { Wsum = 0.5f * (Wsum + K.y * f); csum = 0.5f * (csum + K.z * df); }
-            }
-            csum *= invr;
+            float Wsum, csum;
+            f32c_pair_weights<ST, KF>(
+                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, (float)ha, K, Lj.w,
+                [&]() {
+                    const double ex = __dsub_rn((double)p[0], (double)tv.x[li]);
+                    const double ey = __dsub_rn((double)p[1], (double)tv.y[li]);
+                    const double ez = __dsub_rn((double)p[2], (double)tv.z[li]);
+                    return __fma_rn(ex, ex, __fma_rn(ey, ey, __dmul_rn(ez, ez)));
+                },
+                [&]() { return __dmul_rn(tv.Kd, (double)tv.h[li]); }, Wsum, csum);
             if (WHAT == WHAT_DENSITY) {
-                Dm.add((A.unit_mass ? 1.f : st.mf[slot]) * Wsum);
+                Dm.add(__fmul_rn(A.unit_mass ? 1.f : st.mf[slot], Wsum));
                 return;
             }
-            const float w = K.w * Wsum;
-            const float gc = K.w * csum;
-            const float gx = gc * dx, gy = gc * dy, gz = gc * dz;
+            const float w = __fmul_rn(K.w, Wsum);
+            const float gc = __fmul_rn(K.w, csum);
+            const float gx = __fmul_rn(gc, dx), gy = __fmul_rn(gc, dy), gz = __fmul_rn(gc, dz);
             S1.add(w);
             G[0].add(gx); G[1].add(gy); G[2].add(gz);
             if (SHIFT && !have0) {
@@ -578,16 +562,16 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
 #pragma unroll
             for (int c = 0; c < KC; ++c) {
                 if (c < kc) {
-                    const float a = st.col[c][slot] - (float)a0[c];
-                    Sw[c].add(a * w);
-                    Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+                    const float a = __fsub_rn(st.col[c][slot], (float)a0[c]);
+                    Sw[c].add(__fmul_rn(a, w));
+                    Sg[c][0].add(__fmul_rn(a, gx)); Sg[c][1].add(__fmul_rn(a, gy)); Sg[c][2].add(__fmul_rn(a, gz));
                 }
             }
             if (need_dg) {
                 const float mb = st.mf[slot];
-                Dm.add(mb * Wsum);
-                const float mc = mb * csum;
-                Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+                Dm.add(__fmul_rn(mb, Wsum));
+                const float mc = __fmul_rn(mb, csum);
+                Dg[0].add(__fmul_rn(mc, dx)); Dg[1].add(__fmul_rn(mc, dy)); Dg[2].add(__fmul_rn(mc, dz));
             }
         };
 

@@ -377,10 +377,19 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
     }
 
     // Kernel weights and sums of one pair; weights as in k_points.
+    // (FP32C: every product rounded on its own, as in k_points; FP64 as written)
+    auto mul = [](CT a, CT b) -> CT {
+        if constexpr (std::is_same<CT, float>::value) return __fmul_rn(a, b);
+        else return a * b;
+    };
+    auto sub = [](CT a, CT b) -> CT {
+        if constexpr (std::is_same<CT, float>::value) return __fsub_rn(a, b);
+        else return a - b;
+    };
     auto accumulate = [&](const auto& col, CT dx, CT dy, CT dz, CT Wsum, CT csum, CT mr, CT mb) {
-        const CT w = mr * Wsum;
-        const CT gc = mr * csum;
-        const CT gx = gc * dx, gy = gc * dy, gz = gc * dz;
+        const CT w = mul(mr, Wsum);
+        const CT gc = mul(mr, csum);
+        const CT gx = mul(gc, dx), gy = mul(gc, dy), gz = mul(gc, dz);
         S1.add(w);
         G[0].add(gx); G[1].add(gy); G[2].add(gz);
         if (SHIFT && !have0) {
@@ -393,15 +402,15 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
         for (int c = 0; c < KC; ++c) {
             if (c < kc) {
                 CT a = (CT)col[c];
-                if (SHIFT) a -= a0[c];
-                Sw[c].add(a * w);
-                Sg[c][0].add(a * gx); Sg[c][1].add(a * gy); Sg[c][2].add(a * gz);
+                if constexpr (SHIFT) a = sub(a, a0[c]);
+                Sw[c].add(mul(a, w));
+                Sg[c][0].add(mul(a, gx)); Sg[c][1].add(mul(a, gy)); Sg[c][2].add(mul(a, gz));
             }
         }
         if (need_dg) {
-            Dm.add(mb * Wsum);
-            const CT mc = mb * csum;
-            Dg[0].add(mc * dx); Dg[1].add(mc * dy); Dg[2].add(mc * dz);
+            Dm.add(mul(mb, Wsum));
+            const CT mc = mul(mb, csum);
+            Dg[0].add(mul(mc, dx)); Dg[1].add(mul(mc, dy)); Dg[2].add(mul(mc, dz));
         }
     };
 
@@ -439,34 +448,19 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
         ++n_bodyit;
         if (!hc) continue;
         if constexpr (BAND) {
-            const float dx = cur.r[0] - cur.L.x;
-            const float dy = cur.r[1] - cur.L.y;
-            const float dz = cur.r[2] - cur.L.z;
-            const float d2 = dx * dx + dy * dy + dz * dz;
-            const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
-            const float r = d2 * invr;
-            float Wsum = 0.f, csum = 0.f;
-            const float qa = (ST != ST_SCATTER) ? r * (float)ia : 0.f;
-            const float qb = (ST != ST_GATHER) ? r * cur.K.x : 0.f;
-            double d2d = 0.0;  // the squared separation in double, for the outer kernel piece
-            if (qa >= qe || qb >= qe) {
-                const double ex = (double)p[0] - cur.xd, ey = (double)p[1] - cur.yd, ez = (double)p[2] - cur.zd;
-                d2d = fma(ex, ex, fma(ey, ey, ez * ez));
-            }
-            if (ST != ST_SCATTER) {
-                float f, df;
-                kfdf_edge<KF>(tv.kern, qa, r, (float)(fa2 - d2d), (float)ha, tv.Kf, f, df);
-                Wsum = (float)sa3 * f;
-                csum = (float)sa4 * df;
-            }
-            if (ST != ST_GATHER) {
-                float f, df;
-                const double hbK = tv.Kd * cur.hd;
-                kfdf_edge<KF>(tv.kern, qb, r, (float)fma(hbK, hbK, -d2d), cur.L.w, tv.Kf, f, df);
-                if (ST == ST_SCATTER) { Wsum = cur.K.y * f; csum = cur.K.z * df; }
-                else { Wsum = 0.5f * (Wsum + cur.K.y * f); csum = 0.5f * (csum + cur.K.z * df); }
-            }
-            csum *= invr;
+            const float dx = __fsub_rn(cur.r[0], cur.L.x);
+            const float dy = __fsub_rn(cur.r[1], cur.L.y);
+            const float dz = __fsub_rn(cur.r[2], cur.L.z);
+            float Wsum, csum;
+            f32c_pair_weights<ST, KF>(
+                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, (float)ha, cur.K, cur.L.w,
+                [&]() {
+                    const double ex = __dsub_rn((double)p[0], cur.xd);
+                    const double ey = __dsub_rn((double)p[1], cur.yd);
+                    const double ez = __dsub_rn((double)p[2], cur.zd);
+                    return __fma_rn(ex, ex, __fma_rn(ey, ey, __dmul_rn(ez, ez)));
+                },
+                [&]() { return __dmul_rn(tv.Kd, cur.hd); }, Wsum, csum);
             accumulate(cur.col, dx, dy, dz, Wsum, csum, cur.K.w, cur.mb);
         } else {
             const T e2 = ex_d2_pp<T>(p, cur.x, cur.y, cur.z);

@@ -108,55 +108,62 @@ template <class C> __device__ __forceinline__ void kern_fdf(int k, C q, C& f, C&
 // of a symmetric pair) has num < 0 and gets f = f' = 0.
 __device__ __forceinline__ void kern_fdf_f32(int k, float q, float r, float num, float hf, float Kf, float& f,
                                              float& df) {
+    // every rounding written out, as in m4_fdf_edge (interp.cuh)
     f = 0.f;
     df = 0.f;
-    const float u = fmaxf(__fdividef(num, hf * (Kf * hf + r)), 0.f);  // K - q
+    const float u = fmaxf(__fdividef(num, __fmul_rn(hf, __fmaf_rn(Kf, hf, r))), 0.f);  // K - q
     switch (k) {
     case KERN_M5:
         if (q < 0.5f) {
-            const float q2 = q * q;
-            f = 14.375f + q2 * (6.f * q2 - 15.f);
-            df = q * (24.f * q2 - 30.f);
+            const float q2 = __fmul_rn(q, q);
+            f = __fmaf_rn(q2, __fmaf_rn(6.f, q2, -15.f), 14.375f);
+            df = __fmul_rn(q, __fmaf_rn(24.f, q2, -30.f));
         } else if (q < 1.5f) {
-            const float a = 2.5f - q, b = 1.5f - q, a3 = a * a * a, b3 = b * b * b;
-            f = a3 * a - 5.f * (b3 * b);
-            df = -4.f * a3 + 20.f * b3;
+            const float a = __fsub_rn(2.5f, q), b = __fsub_rn(1.5f, q);
+            const float a3 = __fmul_rn(__fmul_rn(a, a), a), b3 = __fmul_rn(__fmul_rn(b, b), b);
+            f = __fmaf_rn(-5.f, __fmul_rn(b3, b), __fmul_rn(a3, a));
+            df = __fmaf_rn(20.f, b3, __fmul_rn(-4.f, a3));
         } else {
-            const float u3 = u * u * u;
-            f = u3 * u;
-            df = -4.f * u3;
+            const float u3 = __fmul_rn(__fmul_rn(u, u), u);
+            f = __fmul_rn(u3, u);
+            df = __fmul_rn(-4.f, u3);
         }
         break;
     case KERN_M6:
         if (q < 1.f) {
-            const float q2 = q * q;
-            f = 66.f + q2 * (-60.f + q2 * (30.f - 10.f * q));
-            df = q * (-120.f + q2 * (120.f - 50.f * q));
+            const float q2 = __fmul_rn(q, q);
+            f = __fmaf_rn(q2, __fmaf_rn(q2, __fmaf_rn(-10.f, q, 30.f), -60.f), 66.f);
+            df = __fmul_rn(q, __fmaf_rn(q2, __fmaf_rn(-50.f, q, 120.f), -120.f));
         } else if (q < 2.f) {
-            const float a = 3.f - q, b = 2.f - q, a4 = (a * a) * (a * a), b4 = (b * b) * (b * b);
-            f = a4 * a - 6.f * (b4 * b);
-            df = -5.f * a4 + 30.f * b4;
+            const float a = __fsub_rn(3.f, q), b = __fsub_rn(2.f, q);
+            const float a2 = __fmul_rn(a, a), b2 = __fmul_rn(b, b);
+            const float a4 = __fmul_rn(a2, a2), b4 = __fmul_rn(b2, b2);
+            f = __fmaf_rn(-6.f, __fmul_rn(b4, b), __fmul_rn(a4, a));
+            df = __fmaf_rn(30.f, b4, __fmul_rn(-5.f, a4));
         } else {
-            const float u4 = (u * u) * (u * u);
-            f = u4 * u;
-            df = -5.f * u4;
+            const float u2 = __fmul_rn(u, u);
+            const float u4 = __fmul_rn(u2, u2);
+            f = __fmul_rn(u4, u);
+            df = __fmul_rn(-5.f, u4);
         }
         break;
     case KERN_C2: case KERN_C4: case KERN_C6: {
-        const float a = (q < 1.f) ? 1.f - 0.5f * q : 0.5f * u;
-        const float a2 = a * a;
-        if (k == KERN_C2) {
-            const float a3 = a2 * a;
-            f = a3 * a * (2.f * q + 1.f);
-            df = -5.f * q * a3;
-        } else if (k == KERN_C4) {
-            const float a5 = a2 * a2 * a;
-            f = a5 * a * ((35.f / 12.f) * (q * q) + 3.f * q + 1.f);
-            df = (-14.f / 3.f) * q * (1.f + 2.5f * q) * a5;
-        } else {
-            const float a7 = a2 * a2 * a2 * a;
-            f = a7 * a * (4.f * (q * q * q) + 6.25f * (q * q) + 4.f * q + 1.f);
-            df = -5.5f * q * (1.f + 3.5f * q + 4.f * (q * q)) * a7;
+        const float a = (q < 1.f) ? __fmaf_rn(-0.5f, q, 1.f) : __fmul_rn(0.5f, u);
+        const float a2 = __fmul_rn(a, a);
+        if (k == KERN_C2) {  // (2q + 1) a^4, f' = -5 q a^3
+            const float a3 = __fmul_rn(a2, a);
+            f = __fmul_rn(__fmul_rn(a3, a), __fmaf_rn(2.f, q, 1.f));
+            df = __fmul_rn(__fmul_rn(-5.f, q), a3);
+        } else if (k == KERN_C4) {  // (35/12 q^2 + 3 q + 1) a^6, f' = -14/3 q (1 + 5/2 q) a^5
+            const float a5 = __fmul_rn(__fmul_rn(a2, a2), a);
+            f = __fmul_rn(__fmul_rn(a5, a), __fmaf_rn(__fmaf_rn(35.f / 12.f, q, 3.f), q, 1.f));
+            df = __fmul_rn(__fmul_rn(__fmul_rn(-14.f / 3.f, q), __fmaf_rn(2.5f, q, 1.f)), a5);
+        } else {  // (4 q^3 + 25/4 q^2 + 4 q + 1) a^8, f' = -11/2 q (1 + 7/2 q + 4 q^2) a^7
+            const float a7 = __fmul_rn(__fmul_rn(__fmul_rn(a2, a2), a2), a);
+            const float pf = __fmaf_rn(__fmaf_rn(__fmaf_rn(4.f, q, 6.25f), q, 4.f), q, 1.f);
+            const float pd = __fmaf_rn(__fmaf_rn(4.f, q, 3.5f), q, 1.f);
+            f = __fmul_rn(__fmul_rn(a7, a), pf);
+            df = __fmul_rn(__fmul_rn(__fmul_rn(-5.5f, q), pd), a7);
         }
         break;
     }

@@ -79,9 +79,34 @@ def test_gradcheck_beam_column_density():
     def f(m_, x_, z_, A_):
         return AG.interpolate_beam(x_, y, z_, m_, h, rho, [rho, A_], fr, prm, 6, 5, cat)
 
-    inputs = [t.clone().requires_grad_(True) for t in (m, x, z, A)]
-    # a smaller step: the line kernel is a piecewise-linear table in q
-    assert torch.autograd.gradcheck(f, inputs, eps=1e-7, atol=1e-5, rtol=1e-3)
+    # masses and the column enter linearly: the full gradcheck
+    def f_lin(m_, A_):
+        return f(m_, x, z, A_)
+
+    assert torch.autograd.gradcheck(f_lin, [m.clone().requires_grad_(True), A.clone().requires_grad_(True)],
+                                    eps=1e-6, atol=1e-8, rtol=1e-6)
+    # positions: the line kernel is a piecewise-linear table in q, so a
+    # central difference that straddles a table knot averages two slopes.
+    # The backward's slope must match the forward or the backward one-sided
+    # difference (the slope on one side of the knot), or lie between them.
+    eps = 1e-7
+    for which in ("x", "z"):
+        pos = (x if which == "x" else z).clone().requires_grad_(True)
+        out = (f(m, pos, z, A) if which == "x" else f(m, x, pos, A)).reshape(-1)
+        ja = torch.stack([torch.autograd.grad(out[i], pos, retain_graph=True)[0] for i in range(out.numel())])
+        base = out.detach()
+        fwd = torch.empty_like(ja)
+        bwd = torch.empty_like(ja)
+        for j in range(pos.numel()):
+            for sgn, dst in ((1.0, fwd), (-1.0, bwd)):
+                q = pos.detach().clone()
+                q[j] += sgn * eps
+                o = (f(m, q, z, A) if which == "x" else f(m, x, q, A)).reshape(-1)
+                dst[:, j] = sgn * (o - base) / eps
+        tol = 2e-6 + 1e-3 * torch.maximum(fwd.abs(), bwd.abs())
+        lo, hi = torch.minimum(fwd, bwd) - tol, torch.maximum(fwd, bwd) + tol
+        ok = (ja >= lo) & (ja <= hi)
+        assert bool(ok.all()), (which, int((~ok).sum()), float((ja - (fwd + bwd) / 2).abs().max()))
 
 
 def test_h_and_rho_are_held_fixed():

@@ -267,6 +267,30 @@ def test_two_kernel_path_matches_single_kernel(prec, strategy, dtype):
         assert rel_err(two[k], one[k]) <= tol, (k, rel_err(two[k], one[k]))
 
 
+@pytest.mark.parametrize("kid", [L.PSB_KERNEL_M4, L.PSB_KERNEL_M5, L.PSB_KERNEL_M6, L.PSB_KERNEL_C2,
+                                 L.PSB_KERNEL_C4, L.PSB_KERNEL_C6])
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+def test_two_kernel_path_is_bit_identical_to_single_kernel(prec, kid):
+    """Double particles, every kernel family: the pair-sum kernel evaluates
+    each pair with the single kernel's arithmetic in the same order, so the
+    two paths give the same bits.  (Tiles whose pair lists overflow go to the
+    single kernel, and which tiles overflow depends on how a call's samples
+    fall into tiles, so a call's bits must not depend on the path.)"""
+    arrs, cols = make_particles(30_000, 81)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols, kernel=kid)
+    ctx.build(want_perm=False)
+    s = _samples(6000, 82)
+    cat = CatalogC(**CATALOGS["all"])
+    res = []
+    for flags in (0, L.PSB_FLAG_SINGLE_KERNEL):
+        ctx.extra_flags = flags
+        res.append(ctx.interp_points(*s, cat, strategy=L.PSB_SYMMETRIC, hmode=L.PSB_H_NEAREST, prec=prec))
+    ctx.extra_flags = 0
+    for k in range(cat.L):
+        assert np.array_equal(res[0][k], res[1][k], equal_nan=True), k
+
+
 @pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
 def test_two_kernel_path_overflow_tiles(prec):
     """Samples with very large h accept more leaf spans than a pair list holds;

@@ -298,14 +298,19 @@ __device__ __forceinline__ bool warp_traverse_spans(int32_t start, int64_t n, co
                                                     NodeFn node_fn, SpanFn span_fn, int64_t& steps) {
     int32_t node = start;
     int32_t resume = lane_valid ? -1 : 0;
-    const int64_t bound = steps + 4 * n + 8;
-    const int64_t maxid = 2 * n - 1;
+    // A DFS visits each of the 2n - 1 nodes at most once; the bound (4n + 8
+    // steps, capped below 2^32) only ends a walk over a corrupted tree.  32-bit
+    // counters and ids keep the per-step bookkeeping short (n <= 2^30).
+    const uint32_t bound = (uint32_t)(4 * n + 8 < 0xFFFFFFFFll ? 4 * n + 8 : 0xFFFFFFFFll);
+    const uint32_t maxid = (uint32_t)(2 * n - 1);
+    const int32_t n32 = (int32_t)n;
+    uint32_t k = 0;
     bool ok = true;
     while (node != 0) {
-        if (++steps > bound || node < 0 || (int64_t)node > maxid) { ok = false; break; }
+        if (++k >= bound || (uint32_t)node > maxid) { ok = false; break; }
         if (resume == node) resume = -1;
         const bool active = (resume == -1);
-        if (node >= n) {  // a leaf reached directly: a span of one
+        if (node >= n32) {  // a leaf reached directly: a span of one
             const int32_t esc = __ldg(&escape[node - 1]);
             span_fn((int64_t)node - n, 1, active);
             node = esc;
@@ -332,6 +337,7 @@ __device__ __forceinline__ bool warp_traverse_spans(int32_t start, int64_t n, co
         }
         if (__all_sync(PSB_FULL, resume == 0)) break;
     }
+    steps += k;
     return ok;
 }
 

@@ -215,10 +215,13 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
         }
     }
     auto better = [&](double d2, int64_t li) { return d2 < best || (d2 == best && li < bidx); };
+    // the node test compares in float against best rounded up (lb > bestf
+    // implies lb > best): one conversion per improvement, not per step
+    float bestf = __double2float_ru(best);
     auto node_fn = [&](int ni) -> bool {
         if constexpr (BAND) {
             float lb = lb_d2_pbox(pf, pem, __ldg(&tv.node_lo[ni]), __ldg(&tv.node_hi[ni]));
-            return !((double)lb > best);
+            return !(lb > bestf);
         } else {
             return !((double)ex_d2_pbox<T>(p, tv, ni) > best);
         }
@@ -265,7 +268,7 @@ __device__ __forceinline__ T nearest_h_pass(const TreeView<T>& tv, Stage& st, St
             for (; cand; cand &= cand - 1) {
                 const int64_t li = lo + __ffs(cand) - 1;
                 double d2 = (double)ex_d2_pp<T>(p, tv.x[li], tv.y[li], tv.z[li]);
-                if (better(d2, li)) { best = d2; bidx = li; }
+                if (better(d2, li)) { best = d2; bidx = li; bestf = __double2float_ru(best); }
             }
         } else {
             st.best[lane] = (T)best;

@@ -63,7 +63,8 @@ template <class T, int P>
 static cudaError_t dispatch_lines_p(const Args<T>& a, int st, int kc, int what, cudaStream_t s) {
     unsigned g = (unsigned)((a.src.ntiles + 3) / 4);
     if (g == 0) return cudaSuccess;
-    size_t smem = (size_t)LUT_N * (P == PREC_FP64 ? sizeof(double) : sizeof(float));
+    // shared memory only for the FP64 sums over the short float table (k_lines)
+    size_t smem = (P == PREC_FP64 && a.lut_n == LUT_SHORT_N) ? (size_t)LUT_SHORT_N * sizeof(double) : 0;
     if (what == WHAT_INTERP) dispatch_lines_s<T, P, WHAT_INTERP>(a, st, kc, g, smem, s);
     else dispatch_lines_s<T, P, WHAT_DIGEST>(a, st, kc, g, smem, s);
     return cudaGetLastError();

@@ -360,6 +360,28 @@ __global__ void k_to_float(const double* src, int64_t n, float* dst) {
     if (i < n) dst[i] = (float)src[i];
 }
 
+// A column of double inputs relative to the first leaf of each leaf's span,
+// rounded once: the FP32C pair sums add a per-span shift to it
+// (A[first leaf] - A0 in double, rounded once), so A - A0 carries the
+// roundings of the two differences instead of those of A and A0 themselves.
+__global__ void k_span_relative(const double* src, const int32_t* sfirst, int64_t n, float* dst) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = __double2float_rn(__dsub_rn(src[i], src[sfirst[i]]));
+}
+
+// float copies and span-relative copies of the columns (double inputs)
+static int pack_columns(psb_ctx* c, cudaStream_t s) {
+    const int64_t n = c->n;
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->colsr, sizeof(float) * n * c->ncol), "cudaMalloc span-relative columns");
+    for (int k = 0; k < c->ncol; ++k) {
+        k_to_float<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], n, c->colsf + (size_t)k * n);
+        k_span_relative<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], c->sfirst, n,
+                                                   c->colsr + (size_t)k * n);
+    }
+    return PSB_OK;
+}
+
 // The mass-dependent parts of the leaf records (m/rho, m and leafK.w), with
 // k_pack_leaves' arithmetic: a values-only update leaves them as a full
 // build over the same particles would.
@@ -485,16 +507,15 @@ static int build_typed(psb_ctx* c) {
         k_pack_nodes<T><<<grid_for(nint), BT, 0, s>>>(nint, (const T*)c->nmin[0], (const T*)c->nmin[1],
                                                       (const T*)c->nmin[2], (const T*)c->nmax[0], (const T*)c->nmax[1],
                                                       (const T*)c->nmax[2], (const T*)c->nscale, c->node_lo, c->node_hi);
-    int32_t* sfirst = (int32_t*)scratch(c, 2, sizeof(int32_t) * n);  // visit counters consumed
-    if (!sfirst) return fail(c, PSB_ENOMEM, "scratch allocation failed (span roots)");
+    PSB_CUDA_TRY(c, dgrow_t(c, &c->sfirst, sizeof(int32_t) * n), "cudaMalloc span roots");
+    int32_t* sfirst = c->sfirst;
     k_span_roots<<<grid_for(n), BT, 0, s>>>(n, c->parent, c->range_lo, c->range_hi, sfirst);
     k_pack_leaves<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->x, (const T*)c->y, (const T*)c->z, (const T*)c->h,
                                                 (const T*)c->m, (const T*)c->rho, sfirst, c->leaf4, c->mrho, c->mf,
                                                 c->leafK, c->spanb, (float)kern_norm3(c->kern));
     if (sizeof(T) == 8 && c->ncol > 0) {
-        PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
-        for (int k = 0; k < c->ncol; ++k)
-            k_to_float<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], n, c->colsf + (size_t)k * n);
+        const int rc = pack_columns(c, s);
+        if (rc != PSB_OK) return rc;
     }
     PSB_CUDA_TRY(c, cudaGetLastError(), "pack kernels");
 
@@ -530,9 +551,8 @@ static int repack_values_typed(psb_ctx* c) {
     cudaStream_t s = c->stream;
     k_pack_values<T><<<grid_for(n), BT, 0, s>>>(n, (const T*)c->m, (const T*)c->rho, c->mrho, c->mf, c->leafK);
     if (sizeof(T) == 8 && c->ncol > 0) {
-        PSB_CUDA_TRY(c, dgrow_t(c, &c->colsf, sizeof(float) * n * c->ncol), "cudaMalloc float columns");
-        for (int k = 0; k < c->ncol; ++k)
-            k_to_float<<<grid_for(n), BT, 0, s>>>((const double*)c->cols[k], n, c->colsf + (size_t)k * n);
+        const int rc = pack_columns(c, s);
+        if (rc != PSB_OK) return rc;
     }
     PSB_CUDA_TRY(c, cudaGetLastError(), "value pack kernels");
     return PSB_OK;

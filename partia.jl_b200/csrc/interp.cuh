@@ -158,17 +158,71 @@ template <int KF> __device__ __forceinline__ void kfdf_edge(int kern, float q, f
     else kern_fdf_f32(kern, q, r, num, hf, Kf, f, df);
 }
 
+// FP32C weights of one pair for the Wendland families (support 2h).  Their
+// f and f' carry a = 1 - q/2 to the 4th to 8th power, so a relative error e
+// of a becomes 4-8 e in the pair term.  From the float q (rsqrtf, two
+// roundings of the separation) a carries up to about 3.5 float ulps near
+// q = 1, which put C4 and C6 above 1e-6 of the field maxima.  Here
+// t = r / (2 h) is formed in double from the exact squared separation (one
+// double rsqrt) and 1/(2h): per sample for h_a, and for h_b the float 1/h_b
+// refined by one Newton step against 2 h_b in double.  Then a = 1 - t and
+// q = 2 t are each rounded once to float.  A pair outside one h's support
+// (accepted for the other h of a symmetric pair) gets a = 0, so f = f' = 0.
+template <int ST, class ExactD2, class HbK>
+__device__ __forceinline__ void f32c_wendland_weights(int kern, float sa3, float sa4, double ika, float4 K,
+                                                      ExactD2 exact_d2, HbK hb_K, float& Wsum, float& csum) {
+    const double d2d = exact_d2();
+    const double ir = d2d > 0.0 ? rsqrt(d2d) : 0.0;
+    const double rd = __dmul_rn(d2d, ir);
+    Wsum = 0.f;
+    csum = 0.f;
+    if (ST != ST_SCATTER) {
+        const double t = __dmul_rn(rd, ika);  // r / (2 h_a)
+        const float a = fmaxf(__double2float_rn(__dsub_rn(1.0, t)), 0.f);
+        float f, df;
+        wendland_fdf_f32(kern, __double2float_rn(__dadd_rn(t, t)), a, f, df);
+        Wsum = __fmul_rn(sa3, f);
+        csum = __fmul_rn(sa4, df);
+    }
+    if (ST != ST_GATHER) {
+        // 1/(2 h_b): the float record's 1/h_b, halved, and one Newton step
+        const double hbK = hb_K();
+        const double i0 = (double)__fmul_rn(0.5f, K.x);
+        const double ikb = __fma_rn(i0, __fma_rn(-hbK, i0, 1.0), i0);
+        const double t = __dmul_rn(rd, ikb);  // r / (2 h_b)
+        const float a = fmaxf(__double2float_rn(__dsub_rn(1.0, t)), 0.f);
+        float f, df;
+        wendland_fdf_f32(kern, __double2float_rn(__dadd_rn(t, t)), a, f, df);
+        if (ST == ST_SCATTER) {
+            Wsum = __fmul_rn(K.y, f);
+            csum = __fmul_rn(K.z, df);
+        } else {
+            Wsum = __fmul_rn(0.5f, __fmaf_rn(K.y, f, Wsum));
+            csum = __fmul_rn(0.5f, __fmaf_rn(K.z, df, csum));
+        }
+    }
+    csum = __fmul_rn(csum, __double2float_rn(ir));
+}
+
 // The FP32C weights of one pair of a double particle set (both pair-sum
 // kernels): d = (dx, dy, dz) is the sample minus the particle in float, ia,
-// sa3, sa4 the sample's 1/h, sigma/h^3, sigma/h^4, fa2 = (K h_a)^2 and haf =
-// h_a; K is the particle's leafK record (1/h, sigma/h^3, sigma/h^4, m/rho),
+// sa3, sa4 the sample's 1/h, sigma/h^3, sigma/h^4, fa2 = (K h_a)^2, ika =
+// 1/(2 h_a) in double (Wendland families only) and haf = h_a; K is the
+// particle's leafK record (1/h, sigma/h^3, sigma/h^4, m/rho),
 // hbf its h in float.  exact_d2() returns the squared separation in double
 // (called only for the outer kernel piece), hb_K() K h_b in double.  Returns
 // the weight W (Wsum) and the gradient factor csum (grad W = csum d).
 template <int ST, int KF, class ExactD2, class HbK>
 __device__ __forceinline__ void f32c_pair_weights(int kern, float Kf, float qe, float dx, float dy, float dz, float ia,
-                                                  float sa3, float sa4, double fa2, float haf, float4 K, float hbf,
-                                                  ExactD2 exact_d2, HbK hb_K, float& Wsum, float& csum) {
+                                                  float sa3, float sa4, double fa2, double ika, float haf,
+                                                  float4 K, float hbf, ExactD2 exact_d2, HbK hb_K, float& Wsum,
+                                                  float& csum) {
+    if constexpr (KF == 1) {
+        if (kern >= KERN_C2) {  // warp-uniform
+            f32c_wendland_weights<ST>(kern, sa3, sa4, ika, K, exact_d2, hb_K, Wsum, csum);
+            return;
+        }
+    }
     const float d2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
     const float invr = d2 > 0.f ? rsqrtf(d2) : 0.f;
     const float r = __fmul_rn(d2, invr);
@@ -224,6 +278,19 @@ struct KahanF {
     }
     __device__ __forceinline__ double get() const { return (double)s - (double)c; }
 };
+// FP32C sums of double inputs of the kernel families other than M4
+// accumulate A - A0 (A0: the column values of the sample's first accepted
+// neighbour) as colR[leaf] + shift, with colR the column relative to the
+// first leaf of the leaf's span (k_span_relative) and this shift, A[span's
+// first leaf] - A0, formed in double and rounded once.  A - A0 then carries
+// the roundings of those two differences, not those of A and A0 themselves,
+// which the steeper kernels' gradient sums amplify (M4 keeps the cheaper
+// float A - A0).
+template <class T>
+__device__ __forceinline__ float span_shift(const T* col, int64_t lo, int64_t first) {
+    return __double2float_rn(__dsub_rn((double)__ldg(&col[lo]), (double)__ldg(&col[first])));
+}
+
 struct PlainD {
     double s;
     __device__ __forceinline__ void zero() { s = 0.0; }

@@ -143,7 +143,12 @@ static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, in
             PSB_CUDA_TRY(c, cudaStreamWaitEvent(ss[k], c->sev[0], 0), "stream wait");
         }
     }
-    struct Lists { float4* ent4; uint32_t* emask; uint8_t* cnt; void* hab; unsigned* ovf_count; int32_t* ovf_tiles; };
+    struct Lists {
+        float4* ent4; uint32_t* emask; float* eshift; uint8_t* cnt; void* hab; unsigned* ovf_count; int32_t* ovf_tiles;
+    };
+    // FP32C sums of double inputs take per-entry column shifts for the kernels
+    // other than M4 (span_shift; slots 80-86)
+    const bool shifts = sizeof(T) == 8 && prec == PREC_FP32C && A.rec.kc > 0 && c->kern != PSB_KERNEL_M4;
     Lists ls[SPLIT_STREAMS];
     for (int k = 0; k < nsets; ++k) {
         // scratch slots 16-20 (+ slot_off), 48-52, 37-41 and 42-46 (clear of the
@@ -152,6 +157,12 @@ static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, in
         const int so = slot_off + set_off[k];
         ls[k].ent4 = (float4*)scratch(c, 16 + so, sizeof(float4) * (size_t)RCAP * 32 * B);
         ls[k].emask = (uint32_t*)scratch(c, 20 + so, sizeof(uint32_t) * (size_t)RCAP * 32 * B);
+        ls[k].eshift = nullptr;
+        if (shifts) {
+            const int es_slot = 80 + (slot_off == 0 ? k : (slot_off == 32 ? 4 : (slot_off == 14 ? 5 : 6)));
+            ls[k].eshift = (float*)scratch(c, es_slot, sizeof(float) * (size_t)RCAP * 32 * B * A.rec.kc);
+            if (!ls[k].eshift) return fail(c, PSB_ENOMEM, "scratch allocation failed (pair-list shifts)");
+        }
         ls[k].cnt = (uint8_t*)scratch(c, 17 + so, (size_t)32 * B);
         ls[k].hab = scratch(c, 18 + so, sizeof(double) * 32 * (size_t)B);
         char* ovf = (char*)scratch(c, 19 + so, 256 + sizeof(int32_t) * (size_t)B);
@@ -172,6 +183,7 @@ static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, in
         const int64_t nb = std::min<int64_t>(B, nt - t0);
         PSB_CUDA_TRY(c, cudaMemsetAsync(ls[k].ovf_count, 0, sizeof(unsigned), sk), "memset overflow count");
         A.sp.ent4 = ls[k].ent4; A.sp.emask = ls[k].emask; A.sp.cnt = ls[k].cnt; A.sp.ha = ls[k].hab;
+        A.sp.eshift = ls[k].eshift;
         A.sp.ovf_tiles = ls[k].ovf_tiles; A.sp.ovf_count = ls[k].ovf_count;
         A.sp.tile0 = t0; A.sp.ntiles = nb;
         PSB_CUDA_TRY(c, launch_split(A, cprec, st, A.rec.kc, false, sk), "pair-list kernel launch");
@@ -251,6 +263,7 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
     for (size_t q = 0; q < colu.size(); ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
+        A.colR[q] = (sizeof(T) == 8) ? c->colsr + (size_t)colu[q] * c->n : nullptr;
     }
     SampleSrc<T>& S = A.src;
     S.kind = rq.kind;
@@ -477,6 +490,7 @@ static int run_points_pipelined(psb_ctx* c, const SampleReq& rq, int hmode, cons
     for (size_t q = 0; q < colu.size(); ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
+        A.colR[q] = (sizeof(T) == 8) ? c->colsr + (size_t)colu[q] * c->n : nullptr;
     }
     const int nin = 3 + (ph ? 1 : 0);
     char* inb = (char*)scratch(c, 0, es * CH * nin * PIPE_SETS);

@@ -36,6 +36,9 @@ constexpr int RCAP = 32;
 struct SplitBufs {
     float4* ent4;        // [tile][RCAP][32]: (rx, ry, rz, first leaf as int bits)
     uint32_t* emask;     // [tile][RCAP][32]
+    float* eshift;       // FP32C sums of double inputs, kernels other than M4, else null:
+                         // [tile][RCAP][kc][32], the column shifts A[first leaf] - A0 of each entry
+                         // (span_shift)
     uint8_t* cnt;        // [tile][32]
     void* ha;            // [tile][32], element type T
     int32_t* ovf_tiles;  // absolute tile ids
@@ -52,6 +55,7 @@ template <class T> struct Args {
     Recipe rec;
     const T* colT[MAX_KC];
     const float* colF[MAX_KC];
+    const float* colR[MAX_KC];  // double inputs: the columns relative to each leaf's span anchor (span_shift)
     T* out[MAX_OUT];
     int64_t* dig_count;
     uint64_t* dig_hash;

@@ -52,16 +52,16 @@ template <class T, int KC> struct PStage<T, true, KC> {
 template <class T, class Acc, class CT, int KC>
 __device__ __forceinline__ void write_sum_cotangents(const Args<T>& A, int64_t k, const Acc& S1, const Acc (&G)[3],
                                                      const Acc (&Sw)[KC], const Acc (&Sg)[KC][3], const Acc& Dm,
-                                                     const Acc (&Dg)[3], const CT (&a0)[KC]) {
+                                                     const Acc (&Dg)[3], const double (&a0)[KC]) {
     const int kc = A.rec.kc;
     const double s1 = S1.get();
     const double g[3] = {G[0].get(), G[1].get(), G[2].get()};
     double sw[MAX_KC], sg[MAX_KC][3];
 #pragma unroll
     for (int c = 0; c < KC; ++c) {
-        sw[c] = Sw[c].get() + (double)a0[c] * s1;
+        sw[c] = Sw[c].get() + a0[c] * s1;
 #pragma unroll
-        for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get() + (double)a0[c] * g[d];
+        for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get() + a0[c] * g[d];
     }
     const double dm = Dm.get();
     double l[8 + 4 * MAX_KC];
@@ -120,7 +120,7 @@ __device__ __forceinline__ void write_sum_cotangents(const Args<T>& A, int64_t k
 template <class T, class Acc, class CT, int KC>
 __device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k, const Acc& S1, const Acc (&G)[3],
                                                      const Acc (&Sw)[KC], const Acc (&Sg)[KC][3], const Acc& Dm,
-                                                     const Acc (&Dg)[3], const CT (&a0)[KC]) {
+                                                     const Acc (&Dg)[3], const double (&a0)[KC]) {
     if (A.lam) {
         write_sum_cotangents<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
         return;
@@ -136,7 +136,7 @@ __device__ __forceinline__ void write_interp_outputs(const Args<T>& A, int64_t k
 #pragma unroll
         for (int c = 0; c < KC; ++c) {
             sw[c] = Sw[c].get();
-            sh[c] = (double)a0[c];
+            sh[c] = a0[c];
 #pragma unroll
             for (int d = 0; d < 3; ++d) sg[c][d] = Sg[c][d].get();
         }
@@ -299,6 +299,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
     constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
     constexpr bool SHIFT = (PREC == PREC_FP32C);  // accumulate A - A0 (cancellation-free gradients)
+    constexpr bool EXS = BAND && KF == 1;         // A - A0 from span-relative columns (span_shift)
     __shared__ PStage<T, BAND, KC> stage_all[4];
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
@@ -410,6 +411,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     }
     const double kha = tv.Kd * (double)ha;
     const double fa2 = kha * kha;  // (K ha)^2 for the kernel piece at the support edge
+    const double ika = (KF == 1 && ST != ST_SCATTER) ? 0.5 / (double)ha : 0.0;  // Wendland pair terms
     const float qe = (KF == 0) ? 1.f : tv.qedge;
 
     // ---- accumulators ----
@@ -417,6 +419,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
     CT dens = CT(0);
     CT a0[KC];
     bool have0 = false;
+    int64_t first0 = -1;  // EXS: the first accepted leaf (its column values are A0)
     S1.zero(); Dm.zero();
 #pragma unroll
     for (int d = 0; d < 3; ++d) { G[d].zero(); Dg[d].zero(); }
@@ -539,7 +542,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const int64_t li = st.lo[b] + j;
             float Wsum, csum;
             f32c_pair_weights<ST, KF>(
-                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, (float)ha, K, Lj.w,
+                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, ika, (float)ha, K, Lj.w,
                 [&]() {
                     const double ex = __dsub_rn((double)p[0], (double)tv.x[li]);
                     const double ey = __dsub_rn((double)p[1], (double)tv.y[li]);
@@ -556,7 +559,8 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
             const float gx = __fmul_rn(gc, dx), gy = __fmul_rn(gc, dy), gz = __fmul_rn(gc, dz);
             S1.add(w);
             G[0].add(gx); G[1].add(gy); G[2].add(gz);
-            if (SHIFT && !have0) {
+            if (EXS && first0 < 0) first0 = li;
+            if (!EXS && !have0) {
                 have0 = true;
 #pragma unroll
                 for (int c = 0; c < KC; ++c)
@@ -565,7 +569,11 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
 #pragma unroll
             for (int c = 0; c < KC; ++c) {
                 if (c < kc) {
-                    const float a = __fsub_rn(st.col[c][slot], (float)a0[c]);
+                    // A - A0 as in k_bodies: for EXS the span-relative column
+                    // plus the span's shift A[first leaf] - A0 (double, rounded
+                    // once), else the float column less the float A0
+                    const float a = EXS ? __fadd_rn(st.col[c][slot], span_shift(A.colT[c], st.lo[b], first0))
+                                        : __fsub_rn(st.col[c][slot], (float)a0[c]);
                     Sw[c].add(__fmul_rn(a, w));
                     Sg[c][0].add(__fmul_rn(a, gx)); Sg[c][1].add(__fmul_rn(a, gy)); Sg[c][2].add(__fmul_rn(a, gz));
                 }
@@ -636,7 +644,7 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
                     if (need_dg || WHAT == WHAT_DENSITY) st.mf[slot] = __ldg(&tv.mf[li]);
 #pragma unroll
                     for (int c = 0; c < KC; ++c)
-                        if (c < kc) st.col[c][slot] = __ldg(&A.colF[c][li]);
+                        if (c < kc) st.col[c][slot] = __ldg(&(EXS ? A.colR : A.colF)[c][li]);
                 }
             }
             if (lane == 0) st.lo[b] = lo;
@@ -784,7 +792,11 @@ __global__ void __launch_bounds__(128) k_points(const Args<T> A) {
         } else if (WHAT == WHAT_DENSITY) {
             A.out[0][k] = (T)dens;
         } else {
-            write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
+            double a0o[KC];
+#pragma unroll
+            for (int c = 0; c < KC; ++c)
+                a0o[c] = EXS ? ((c < kc && first0 >= 0) ? (double)A.colT[c][first0] : 0.0) : (double)a0[c];
+            write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0o);
         }
     }
     // ---- statistics and errors ----

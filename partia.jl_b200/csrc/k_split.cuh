@@ -277,6 +277,20 @@ __global__ void __launch_bounds__(128, 12) k_collect(const Args<T> A) {
     }
 
     const bool tovf = __any_sync(PSB_FULL, ovf);
+    if (BAND && A.sp.eshift && !tovf && nent > 0) {
+        // the column shifts of this lane's entries, A[lo] - A0 (span_shift),
+        // after the walk: here the entries' loads are independent and overlap,
+        // where inside the walk each would stall it.  A0 are the column values
+        // of the first accepted leaf.
+        const int kc = A.rec.kc;
+        float* esh = A.sp.eshift + (size_t)bt * RCAP * kc * 32 + lane;
+        const int32_t fl = __float_as_int(ent4[0].w) + __ffs(emask[0]) - 1;
+        for (int c = 0; c < kc; ++c) {
+#pragma unroll 4
+            for (int e = 0; e < nent; ++e)
+                esh[((size_t)e * kc + c) * 32] = span_shift(A.colT[c], (int64_t)__float_as_int(ent4[(size_t)e * 32].w), fl);
+        }
+    }
     if (valid && A.ha_out) A.ha_out[k] = ha;
     A.sp.cnt[bt * 32 + lane] = tovf ? (uint8_t)0xFF : (uint8_t)nent;
     ((T*)A.sp.ha)[bt * 32 + lane] = ha;
@@ -307,7 +321,7 @@ template <class T, bool BAND, int KC> struct PairData {
     T x, y, z, h, m, rho;
     T col[KC];
     __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool,
-                                         const float*) {
+                                         const float*, const float* const*) {
         x = __ldg(&tv.x[li]); y = __ldg(&tv.y[li]); z = __ldg(&tv.z[li]);
         h = __ldg(&tv.h[li]); m = __ldg(&tv.m[li]); rho = __ldg(&tv.rho[li]);
 #pragma unroll
@@ -316,17 +330,17 @@ template <class T, bool BAND, int KC> struct PairData {
 };
 template <class T, int KC> struct PairData<T, true, KC> {
     float4 L, K;      // leaf4 and leafK of the particle
-    float col[KC];
+    float col[KC];    // the column in float, or for EXS span-relative (A - A0 once the entry's shift is added)
     float mb;         // mass (density gradient only)
     float r[3];       // the sample relative to the span's first leaf
     int64_t li;       // leaf index
     double xd, yd, zd, hd;  // the particle in double (outer kernel piece)
     __device__ __forceinline__ void load(const TreeView<T>& tv, const Args<T>& A, int64_t li, int kc, bool need_dg,
-                                         const float* Rs) {
+                                         const float* Rs, const float* const* cols) {
         L = __ldg(&tv.leaf4[li]);
         K = __ldg(&tv.leafK[li]);
 #pragma unroll
-        for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&A.colF[c][li]) : 0.f;
+        for (int c = 0; c < KC; ++c) col[c] = (c < kc) ? __ldg(&cols[c][li]) : 0.f;
         mb = need_dg ? __ldg(&tv.mf[li]) : 0.f;
         r[0] = Rs[0]; r[1] = Rs[1]; r[2] = Rs[2];
         this->li = li;
@@ -334,12 +348,13 @@ template <class T, int KC> struct PairData<T, true, KC> {
     }
 };
 
-template <class T, int PREC, int ST, int KC, int KF>
+template <class T, int PREC, int ST, int KC, int KF, bool DG>
 __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T> A) {
     using CT = typename std::conditional<PREC == PREC_FP64, double, float>::type;
     using Acc = typename std::conditional<PREC == PREC_FP64, PlainD, KahanF>::type;
     constexpr bool BAND = (PREC == PREC_FP32C) && (sizeof(T) == 8);
     constexpr bool SHIFT = (PREC == PREC_FP32C);
+    constexpr bool EXS = BAND && KF == 1;  // column shifts formed in double (span_shift), from k_collect
     const TreeView<T>& tv = A.tv;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
@@ -354,7 +369,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
     if (valid) sample_coords(A.src, k, p, dd);
     const T ha = ((const T*)A.sp.ha)[bt * 32 + lane];
     const int kc = A.rec.kc;
-    const bool need_dg = A.rec.need_dg != 0;
+    constexpr bool need_dg = DG;  // A.rec.need_dg (the launch picks the instantiation)
 
     const CT sig = (KF == 0) ? inv_pi<CT>() : (CT)tv.sig;
     CT ia = CT(0), sa3 = CT(0), sa4 = CT(0);
@@ -365,6 +380,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
     }
     const double kha = tv.Kd * (double)ha;
     const double fa2 = kha * kha;  // (K ha)^2 for the kernel piece at the support edge
+    const double ika = (KF == 1 && ST != ST_SCATTER) ? 0.5 / (double)ha : 0.0;  // Wendland pair terms
     const float qe = (KF == 0) ? 1.f : tv.qedge;
     Acc S1, G[3], Sw[KC], Sg[KC][3], Dm, Dg[3];
     CT a0[KC];
@@ -396,7 +412,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
         const CT gx = mul(gc, dx), gy = mul(gc, dy), gz = mul(gc, dz);
         S1.add(w);
         G[0].add(gx); G[1].add(gy); G[2].add(gz);
-        if (SHIFT && !have0) {
+        if (SHIFT && !EXS && !have0) {
             have0 = true;
 #pragma unroll
             for (int c = 0; c < KC; ++c)
@@ -405,8 +421,8 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
 #pragma unroll
         for (int c = 0; c < KC; ++c) {
             if (c < kc) {
-                CT a = (CT)col[c];
-                if constexpr (SHIFT) a = sub(a, a0[c]);
+                CT a = (CT)col[c];  // EXS: already A - A0
+                if constexpr (SHIFT && !EXS) a = sub(a, a0[c]);
                 Sw[c].add(mul(a, w));
                 Sg[c][0].add(mul(a, gx)); Sg[c][1].add(mul(a, gy)); Sg[c][2].add(mul(a, gz));
             }
@@ -422,32 +438,46 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
     // in flight while the current pair is summed.
     const float4* ent4 = A.sp.ent4 + (size_t)bt * RCAP * 32 + lane;
     const uint32_t* emask = A.sp.emask + (size_t)bt * RCAP * 32 + lane;
+    const float* esh = EXS ? A.sp.eshift + (size_t)bt * RCAP * kc * 32 + lane : nullptr;
     int e = 0;
     unsigned m = 0;
     int64_t lo = 0;
     float Rs[3] = {0.f, 0.f, 0.f};
+    float sh[KC];          // EXS: the entry's column shifts A[lo] - A0 (written by k_collect)
+#pragma unroll
+    for (int c = 0; c < KC; ++c) sh[c] = 0.f;
     PairData<T, BAND, KC> nx;
     bool hn = false;
     auto fetch = [&]() {
         if (m == 0 && e < n) {
             const float4 q = ent4[(size_t)e * 32];
-            m = emask[(size_t)e * 32];
+            m = emask[(size_t)e * 32];  // never 0: k_collect writes entries with accepted leaves only
             ++e;
             lo = (int64_t)__float_as_int(q.w);
             Rs[0] = q.x; Rs[1] = q.y; Rs[2] = q.z;
+            if constexpr (EXS) {
+#pragma unroll
+                for (int c = 0; c < KC; ++c) sh[c] = (c < kc) ? esh[((size_t)(e - 1) * kc + c) * 32] : 0.f;
+            }
         }
         hn = m != 0;
         if (hn) {
             const int j = __ffs(m) - 1;
             m &= m - 1;
-            nx.load(tv, A, lo + j, kc, need_dg, Rs);
+            nx.load(tv, A, lo + j, kc, need_dg, Rs, EXS ? A.colR : A.colF);
         }
     };
     unsigned long long n_bodyit = 0;
     fetch();
     while (__any_sync(PSB_FULL, hn)) {
         const bool hc = hn;
-        const PairData<T, BAND, KC> cur = nx;
+        PairData<T, BAND, KC> cur = nx;
+        if constexpr (EXS) {
+            // A - A0: the shifts of cur's entry (fetch may start the next one);
+            // added here, an iteration after the loads, not as they return
+#pragma unroll
+            for (int c = 0; c < KC; ++c) cur.col[c] = __fadd_rn(cur.col[c], sh[c]);
+        }
         fetch();
         ++n_bodyit;
         if (!hc) continue;
@@ -457,7 +487,7 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
             const float dz = __fsub_rn(cur.r[2], cur.L.z);
             float Wsum, csum;
             f32c_pair_weights<ST, KF>(
-                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, (float)ha, cur.K, cur.L.w,
+                tv.kern, tv.Kf, qe, dx, dy, dz, (float)ia, (float)sa3, (float)sa4, fa2, ika, (float)ha, cur.K, cur.L.w,
                 [&]() {
                     const double ex = __dsub_rn((double)p[0], cur.xd);
                     const double ey = __dsub_rn((double)p[1], cur.yd);
@@ -497,7 +527,17 @@ __global__ void __launch_bounds__(128, (KC <= 4) ? 4 : 2) k_bodies(const Args<T>
         }
     }
 
-    if (valid) write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0);
+    if (valid) {
+        // EXS: A0 are the column values of the first accepted leaf (the first
+        // pair of the first entry)
+        int64_t first = -1;
+        if (EXS && n > 0) first = (int64_t)__float_as_int(ent4[0].w) + __ffs(emask[0]) - 1;
+        double a0o[KC];
+#pragma unroll
+        for (int c = 0; c < KC; ++c)
+            a0o[c] = EXS ? ((c < kc && first >= 0) ? (double)A.colT[c][first] : 0.0) : (double)a0[c];
+        write_interp_outputs<T, Acc, CT, KC>(A, k, S1, G, Sw, Sg, Dm, Dg, a0o);
+    }
     if (lane == 0 && A.stats) atomicAdd(&A.stats[5], n_bodyit);
 }
 

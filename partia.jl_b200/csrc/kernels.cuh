@@ -28,7 +28,9 @@ __host__ __device__ inline double kern_norm3(int k) {
 }
 
 // First q of the piece that reaches the support edge: from there on the float
-// pair sums take K - q from K^2 h^2 - d^2 formed in double (see kern_fdf_f32).
+// pair sums of M4, M5 and M6 take K - q from K^2 h^2 - d^2 formed in double
+// (see kern_fdf_f32).  The Wendland families take q and 1 - q/2 from the
+// exact separation for every q (f32c_wendland_weights in interp.cuh).
 __host__ __device__ inline float kern_qedge(int k) {
     return k == KERN_M5 ? 1.5f : (k == KERN_M6 ? 2.f : 1.f);
 }
@@ -97,7 +99,8 @@ template <class C> __device__ __forceinline__ void kern_fdf(int k, C q, C& f, C&
     }
 }
 
-// f and f' for k != M4 in the float pair sums of double inputs.  The
+// f and f' for M5 and M6 in the float pair sums of double inputs (the
+// Wendland families have wendland_fdf_f32 below).  The
 // innermost spline pieces are expanded (M5 on q < 1/2: 14.375 - 15 q^2 + 6 q^4,
 // M6 on q < 1: 66 - 60 q^2 + 30 q^4 - 10 q^5), so f' carries its factor q
 // exactly instead of a difference of terms of size ~70.  On the piece that
@@ -147,28 +150,31 @@ __device__ __forceinline__ void kern_fdf_f32(int k, float q, float r, float num,
             df = __fmul_rn(-5.f, u4);
         }
         break;
-    case KERN_C2: case KERN_C4: case KERN_C6: {
-        const float a = (q < 1.f) ? __fmaf_rn(-0.5f, q, 1.f) : __fmul_rn(0.5f, u);
-        const float a2 = __fmul_rn(a, a);
-        if (k == KERN_C2) {  // (2q + 1) a^4, f' = -5 q a^3
-            const float a3 = __fmul_rn(a2, a);
-            f = __fmul_rn(__fmul_rn(a3, a), __fmaf_rn(2.f, q, 1.f));
-            df = __fmul_rn(__fmul_rn(-5.f, q), a3);
-        } else if (k == KERN_C4) {  // (35/12 q^2 + 3 q + 1) a^6, f' = -14/3 q (1 + 5/2 q) a^5
-            const float a5 = __fmul_rn(__fmul_rn(a2, a2), a);
-            f = __fmul_rn(__fmul_rn(a5, a), __fmaf_rn(__fmaf_rn(35.f / 12.f, q, 3.f), q, 1.f));
-            df = __fmul_rn(__fmul_rn(__fmul_rn(-14.f / 3.f, q), __fmaf_rn(2.5f, q, 1.f)), a5);
-        } else {  // (4 q^3 + 25/4 q^2 + 4 q + 1) a^8, f' = -11/2 q (1 + 7/2 q + 4 q^2) a^7
-            const float a7 = __fmul_rn(__fmul_rn(__fmul_rn(a2, a2), a2), a);
-            const float pf = __fmaf_rn(__fmaf_rn(__fmaf_rn(4.f, q, 6.25f), q, 4.f), q, 1.f);
-            const float pd = __fmaf_rn(__fmaf_rn(4.f, q, 3.5f), q, 1.f);
-            f = __fmul_rn(__fmul_rn(a7, a), pf);
-            df = __fmul_rn(__fmul_rn(__fmul_rn(-5.5f, q), pd), a7);
-        }
-        break;
-    }
     default:
         break;
+    }
+}
+
+// f and f' of a Wendland family (C2, C4, C6) in the float pair sums, from q
+// and a = 1 - q/2 (formed more accurately than from q; f32c_wendland_weights),
+// in the factored forms.
+__device__ __forceinline__ void wendland_fdf_f32(int k, float q, float a, float& f, float& df) {
+    // every rounding written out, as in m4_fdf_edge (interp.cuh)
+    const float a2 = __fmul_rn(a, a);
+    if (k == KERN_C2) {  // (2q + 1) a^4, f' = -5 q a^3
+        const float a3 = __fmul_rn(a2, a);
+        f = __fmul_rn(__fmul_rn(a3, a), __fmaf_rn(2.f, q, 1.f));
+        df = __fmul_rn(__fmul_rn(-5.f, q), a3);
+    } else if (k == KERN_C4) {  // (35/12 q^2 + 3 q + 1) a^6, f' = -14/3 q (1 + 5/2 q) a^5
+        const float a5 = __fmul_rn(__fmul_rn(a2, a2), a);
+        f = __fmul_rn(__fmul_rn(a5, a), __fmaf_rn(__fmaf_rn(35.f / 12.f, q, 3.f), q, 1.f));
+        df = __fmul_rn(__fmul_rn(__fmul_rn(-14.f / 3.f, q), __fmaf_rn(2.5f, q, 1.f)), a5);
+    } else {  // (4 q^3 + 25/4 q^2 + 4 q + 1) a^8, f' = -11/2 q (1 + 7/2 q + 4 q^2) a^7
+        const float a7 = __fmul_rn(__fmul_rn(__fmul_rn(a2, a2), a2), a);
+        const float pf = __fmaf_rn(__fmaf_rn(__fmaf_rn(4.f, q, 6.25f), q, 4.f), q, 1.f);
+        const float pd = __fmaf_rn(__fmaf_rn(4.f, q, 3.5f), q, 1.f);
+        f = __fmul_rn(__fmul_rn(a7, a), pf);
+        df = __fmul_rn(__fmul_rn(__fmul_rn(-5.5f, q), pd), a7);
     }
 }
 

@@ -72,12 +72,19 @@ static cudaError_t dispatch_lines_p(const Args<T>& a, int st, int kc, int what, 
 
 // two-kernel point path: k_collect (bodies = false) or k_bodies (bodies = true)
 // over the batch a.sp
+template <class T, int P, int S, int KF, bool DG>
+static void dispatch_bodies_kfd(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
+    if (kc <= 1) k_bodies<T, P, S, 1, KF, DG><<<g, 128, 0, s>>>(a);
+    else if (kc <= 2) k_bodies<T, P, S, 2, KF, DG><<<g, 128, 0, s>>>(a);
+    else if (kc <= 4) k_bodies<T, P, S, 4, KF, DG><<<g, 128, 0, s>>>(a);
+    else k_bodies<T, P, S, 8, KF, DG><<<g, 128, 0, s>>>(a);
+}
+// DG: the catalog has a density gradient (its sums and the masses in
+// registers only where they are used)
 template <class T, int P, int S, int KF>
 static void dispatch_bodies_kf(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {
-    if (kc <= 1) k_bodies<T, P, S, 1, KF><<<g, 128, 0, s>>>(a);
-    else if (kc <= 2) k_bodies<T, P, S, 2, KF><<<g, 128, 0, s>>>(a);
-    else if (kc <= 4) k_bodies<T, P, S, 4, KF><<<g, 128, 0, s>>>(a);
-    else k_bodies<T, P, S, 8, KF><<<g, 128, 0, s>>>(a);
+    if (a.rec.need_dg) dispatch_bodies_kfd<T, P, S, KF, true>(a, kc, g, s);
+    else dispatch_bodies_kfd<T, P, S, KF, false>(a, kc, g, s);
 }
 template <class T, int P, int S>
 static void dispatch_bodies_k(const Args<T>& a, int kc, unsigned g, cudaStream_t s) {

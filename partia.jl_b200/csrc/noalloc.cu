@@ -196,6 +196,7 @@ int noalloc_typed(psb_ctx* c, int64_t ns, const void* sx, const void* sy, const 
     for (int q = 0; q < A.rec.kc; ++q) {
         A.colT[q] = (const T*)c->cols[colu[q]];
         A.colF[q] = (sizeof(T) == 8) ? c->colsf + (size_t)colu[q] * c->n : (const float*)c->cols[colu[q]];
+        A.colR[q] = (sizeof(T) == 8) ? c->colsr + (size_t)colu[q] * c->n : nullptr;
     }
     A.src.kind = SRC_ARRAYS;
     A.src.ns = ns;

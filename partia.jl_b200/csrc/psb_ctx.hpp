@@ -46,6 +46,8 @@ struct psb_ctx {
     float4* leafK = nullptr;  // per leaf (1/h, sigma/h^3, sigma/h^4, m/rho), float
     float2* spanb = nullptr;  // at a span's first leaf: (max |leaf4.xyz|_1, max h) over the span, rounded up
     float* colsf = nullptr;  // float copies of the columns (double inputs), ncol x n
+    int32_t* sfirst = nullptr;  // first leaf of each leaf's span (double inputs)
+    float* colsr = nullptr;  // columns relative to the span's first leaf, A[i] - A[sfirst[i]] in float, ncol x n
     float coord_err = 0.f;
     double bbox[6] = {0, 0, 0, 0, 0, 0};  // particle min x,y,z, max x,y,z
 

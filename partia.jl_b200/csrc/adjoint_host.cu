@@ -22,22 +22,56 @@ namespace psb {
 
 int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu);
 
+// pass: 0 = k_adj_points (whole tiles, or the listed ones), 1 = its pair-list
+// form (k_adj_collect), 2 = k_adj_bodies
 template <int KC, bool SCAL, int KF>
-static void launch_adj_points_ks(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
-    if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
-    else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
-    else k_adj_points<ST_SYMMETRIC, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+static void launch_adj_points_ks(const AdjArgs& a, int st, int pass, unsigned g, cudaStream_t s) {
+    if (pass == 1) {
+        if (st == ST_GATHER) k_adj_points<ST_GATHER, 1, true, KF, true><<<g, 128, 0, s>>>(a);
+        else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, 1, true, KF, true><<<g, 128, 0, s>>>(a);
+        else k_adj_points<ST_SYMMETRIC, 1, true, KF, true><<<g, 128, 0, s>>>(a);
+    } else if (pass == 2) {
+        if (st == ST_GATHER) k_adj_bodies<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+        else if (st == ST_SCATTER) k_adj_bodies<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+        else k_adj_bodies<ST_SYMMETRIC, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+    } else {
+        if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+        else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+        else k_adj_points<ST_SYMMETRIC, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+    }
 }
 // kf: 0 = the M4 code, 1 = the other kernel families
 template <int KC>
-static void launch_adj_points_k(const AdjArgs& a, int st, bool scal, int kf, unsigned g, cudaStream_t s) {
+static void launch_adj_points_k(const AdjArgs& a, int st, bool scal, int kf, int pass, unsigned g, cudaStream_t s) {
     if (kf == 0) {
-        if (scal) launch_adj_points_ks<KC, true, 0>(a, st, g, s);
-        else launch_adj_points_ks<KC, false, 0>(a, st, g, s);
+        if (scal) launch_adj_points_ks<KC, true, 0>(a, st, pass, g, s);
+        else launch_adj_points_ks<KC, false, 0>(a, st, pass, g, s);
     } else {
-        if (scal) launch_adj_points_ks<KC, true, 1>(a, st, g, s);
-        else launch_adj_points_ks<KC, false, 1>(a, st, g, s);
+        if (scal) launch_adj_points_ks<KC, true, 1>(a, st, pass, g, s);
+        else launch_adj_points_ks<KC, false, 1>(a, st, pass, g, s);
     }
+}
+static void launch_adj_rows(int kcl, bool scal, const double* lam, int64_t ns, int kc, const TreeView<double>& sv,
+                            double* rec, cudaStream_t s) {
+    const unsigned g = (unsigned)((ns + 255) / 256);
+    if (scal) {
+        if (kcl == 1) k_adj_rows<1, true><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else if (kcl == 2) k_adj_rows<2, true><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else if (kcl == 4) k_adj_rows<4, true><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else k_adj_rows<8, true><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+    } else {
+        if (kcl == 1) k_adj_rows<1, false><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else if (kcl == 2) k_adj_rows<2, false><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else if (kcl == 4) k_adj_rows<4, false><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+        else k_adj_rows<8, false><<<g, 256, 0, s>>>(lam, ns, kc, sv, rec);
+    }
+}
+static void launch_adj_points(const AdjArgs& a, int kcl, int st, bool scal, int kf, int pass, unsigned g,
+                              cudaStream_t s) {
+    if (kcl == 1) launch_adj_points_k<1>(a, st, scal, kf, pass, g, s);
+    else if (kcl == 2) launch_adj_points_k<2>(a, st, scal, kf, pass, g, s);
+    else if (kcl == 4) launch_adj_points_k<4>(a, st, scal, kf, pass, g, s);
+    else launch_adj_points_k<8>(a, st, scal, kf, pass, g, s);
 }
 template <int KC>
 static void launch_adj_beam_k(const AdjArgs& a, int st, unsigned g, cudaStream_t s) {
@@ -273,12 +307,54 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             J.lam = lams;
             const unsigned g = (unsigned)((n + 127) / 128);
             const int kf = (c->kern == PSB_KERNEL_M4) ? 0 : 1;
-            if (kcl == 1) launch_adj_points_k<1>(J, st, scal, kf, g, s);
-            else if (kcl == 2) launch_adj_points_k<2>(J, st, scal, kf, g, s);
-            else if (kcl == 4) launch_adj_points_k<4>(J, st, scal, kf, g, s);
-            else launch_adj_points_k<8>(J, st, scal, kf, g, s);
-            PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
-            launches += 2;
+            if (c->adj_split) {
+                // Two kernels: the walk writes each particle tile's pair lists
+                // into blocks of a pool (k_adj_collect, at the walk's own
+                // register budget), then one lane per particle sums its pairs
+                // (k_adj_bodies).  Tiles the pool could not hold are
+                // recomputed by k_adj_points.  The pool starts at two blocks
+                // per tile and grows to the blocks the last call asked for
+                // (at most 8 GiB).
+                const int64_t ntiles = (n + 31) / 32;
+                const int64_t cap = (int64_t)(8ll << 30) / (int64_t)(ADJ_CH * 32 * 8 + 32 + 4);
+                if (c->adj_blocks <= 0) c->adj_blocks = std::min<int64_t>(cap, 2 * ntiles + 64);
+                const int64_t nb = c->adj_blocks;
+                const int nqc = scal ? 1 + kcl : 8 + 4 * kcl;
+                const int nrec = 6 + ((nqc + 1) & ~1);  // AdjRec<kcl, scal>::N
+                const size_t b_ent = sizeof(uint2) * (size_t)nb * ADJ_CH * 32, b_cnt = (size_t)nb * 32,
+                             b_next = sizeof(int32_t) * (size_t)nb, b_tile = sizeof(int32_t) * (size_t)ntiles;
+                char* pool = (char*)scratch(c, 87, b_ent + b_cnt + b_next + 2 * b_tile + 256);
+                double* recs = (double*)scratch(c, 88, sizeof(double) * (size_t)nrec * ns);
+                if (!pool || !recs) return fail(c, PSB_ENOMEM, "scratch allocation failed (adjoint pair lists)");
+                AdjLists& al = J.al;
+                al.ent = (uint2*)pool;
+                al.bcnt = (uint8_t*)(pool + b_ent);
+                al.bnext = (int32_t*)(pool + b_ent + b_cnt);
+                al.head = (int32_t*)(pool + b_ent + b_cnt + b_next);
+                al.ovf_tiles = (int32_t*)(pool + b_ent + b_cnt + b_next + b_tile);
+                al.top = (unsigned*)(pool + b_ent + b_cnt + b_next + 2 * b_tile);
+                al.ovf_count = al.top + 1;
+                al.nblocks = nb;
+                J.lamT = recs;
+                PSB_CUDA_TRY(c, cudaMemsetAsync(al.top, 0, 2 * sizeof(unsigned), s), "memset pool counters");
+                launch_adj_rows(kcl, scal, lams, ns, kc, J.sv, recs, s);
+                launch_adj_points(J, kcl, st, scal, kf, 1, g, s);
+                launch_adj_points(J, kcl, st, scal, kf, 2, g, s);
+                AdjArgs F = J;
+                F.tile_list = al.ovf_tiles;
+                F.tile_count = al.ovf_count;
+                launch_adj_points(F, kcl, st, scal, kf, 0, g, s);
+                PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
+                unsigned ptop = 0;
+                PSB_CUDA_TRY(c, cudaMemcpyAsync(&ptop, al.top, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "pool D2H");
+                PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+                if ((int64_t)ptop > nb) c->adj_blocks = std::min<int64_t>(cap, (int64_t)ptop + ptop / 4 + 64);
+                launches += 6;
+            } else {
+                launch_adj_points(J, kcl, st, scal, kf, 0, g, s);
+                PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
+                launches += 2;
+            }
         } else {
             J.lam = lam;
             SampleSrc<double>& B = J.beam;
@@ -317,7 +393,7 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             float ms = 0.f;
             cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]);
             stats->interp_ms = ms;
-            stats->pairs = (int64_t)hst[0];
+            stats->pairs = (int64_t)(hst[0] + hst[6]);  // k_adj_points, k_adj_bodies
             stats->warp_steps = (int64_t)hst[2];
             stats->spans = (int64_t)hst[3];       // spans visited (point samples)
             stats->span_tests = (int64_t)hst[4];  // particle-span tests

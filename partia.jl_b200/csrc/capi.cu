@@ -437,6 +437,15 @@ PSB_API int psb_test_loop_escapes(psb_ctx* c) {
     return loop_escapes(c);
 }
 
+PSB_API int psb_test_adjoint_pool(psb_ctx* c, int64_t blocks, int32_t split) {
+    if (!c) return PSB_EINVAL;
+    c->err.clear();
+    if (blocks < 0) return fail(c, PSB_EINVAL, "blocks must be non-negative");
+    if (blocks > 0) c->adj_blocks = blocks;
+    c->adj_split = split ? 1 : 0;
+    return PSB_OK;
+}
+
 PSB_API int psb_get_tree(psb_ctx* c, int32_t* root, int32_t* left, int32_t* right, int32_t* escape, int32_t* parent,
                          double* node_min, double* node_max, double* node_scale) {
     if (!c) return PSB_EINVAL;

@@ -28,6 +28,24 @@
 
 namespace psb {
 
+// Pair lists of the two-kernel adjoint: one chain of blocks per tile of 32
+// particles, taken from a pool with an atomic counter.  A block holds up to
+// ADJ_CH entries per lane; an entry is a span of the sample tree (its first
+// sample) and the mask of the samples that pair with the lane's particle.
+// A tile for which the pool runs out is listed and recomputed by
+// k_adj_points.
+constexpr int ADJ_CH = 16;
+struct AdjLists {
+    uint2* ent;           // [block][ADJ_CH][32]: (first sample of the span, mask)
+    uint8_t* bcnt;        // [block][32]: entries of each lane in the block
+    int32_t* bnext;       // [block]: the tile's next block, -1 after its last
+    int32_t* head;        // [tile]: first block, -1 without pairs, -2 overflowed
+    unsigned* top;        // blocks taken
+    int64_t nblocks;      // pool size
+    int32_t* ovf_tiles;   // overflowed tiles
+    unsigned* ovf_count;
+};
+
 struct AdjArgs {
     TreeView<double> pt;          // particles (Morton order)
     TreeView<double> sv;          // samples, in the order of their own LBVH; h = h_a
@@ -49,6 +67,11 @@ struct AdjArgs {
     const double* lut;
     unsigned* err;
     unsigned long long* stats;    // [0] pairs, [2] walk steps
+    // the two-kernel point path (k_adj_collect + k_adj_bodies)
+    AdjLists al;
+    const double* lamT;           // records of the samples for k_adj_bodies (AdjRec, sample-tree order)
+    const int32_t* tile_list;     // k_adj_points over these particle tiles only (the lists' overflow), or null
+    const unsigned* tile_count;
 };
 
 // M4 at delta = x_s - x_b: W, gradW = sigma/h^5 g1(q) delta and the Hessian
@@ -120,6 +143,134 @@ __device__ __forceinline__ void hmul(const double H[6], const double v[3], doubl
     o[2] = H[4] * v[0] + H[5] * v[1] + H[2] * v[2];
 }
 
+// Per-particle sums of the pair terms; the particle's factors 1/rho_b,
+// m_b/rho_b and m_b are applied once after its last pair:
+// dL/dm_b = sW / rho_b + sD, dL/dA_c,b = m_b/rho_b sA_c,
+// dL/dx_b = -(m_b/rho_b vS + m_b vD)
+template <int KC> struct AdjAcc {
+    double sW, sD, vS[3], vD[3], sA[KC];
+    __device__ __forceinline__ void zero() {
+        sW = 0.0; sD = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) { vS[d] = 0.0; vD[d] = 0.0; }
+#pragma unroll
+        for (int c = 0; c < KC; ++c) sA[c] = 0.0;
+    }
+};
+
+// The sum cotangents of a pair's sample, by meaning: S1, G (3), Dm, Dg (3),
+// Sw_c, Sg_c (3 per column); a scalar catalog (SCAL) has S1 and Sw_c only.
+// RowsStrided reads compact row r at ls[r * rs] (rows S1, G, Dm, Dg, Sw_c,
+// Sg_c in that order, kc columns; SCAL: S1, Sw_c): the staged rows of
+// k_adj_points or the global cotangent rows.
+struct RowsStrided {
+    const double* ls;
+    int64_t rs;
+    int kc;
+    template <bool SCAL> __device__ __forceinline__ double S1() const { return ls[0]; }
+    __device__ __forceinline__ double G(int d) const { return ls[(1 + d) * rs]; }
+    __device__ __forceinline__ double Dm() const { return ls[4 * rs]; }
+    __device__ __forceinline__ double Dg(int d) const { return ls[(5 + d) * rs]; }
+    template <bool SCAL> __device__ __forceinline__ double Sw(int c) const { return ls[((SCAL ? 1 : 8) + c) * rs]; }
+    __device__ __forceinline__ double Sg(int c, int d) const { return ls[(8 + kc + 3 * c + d) * rs]; }
+};
+// Per-sample records of k_adj_bodies: x, y, z, h_a, 1/h_a, 0, then the sum
+// cotangents with the columns at fixed places for KC columns (those past the
+// catalog's kc are 0), padded to whole 16-byte pairs: one record is read with
+// 128-bit loads, where separate arrays would take a 32-byte sector per value.
+template <int KC, bool SCAL> struct AdjRec {
+    static constexpr int NQ = SCAL ? 1 + KC : 8 + 4 * KC;
+    static constexpr int N = 6 + ((NQ + 1) & ~1);  // doubles per record
+};
+template <int KC, bool SCAL> struct RowsRec {
+    double q[AdjRec<KC, SCAL>::N - 6];
+    template <bool S> __device__ __forceinline__ double S1() const { return q[0]; }
+    __device__ __forceinline__ double G(int d) const { return q[1 + d]; }
+    __device__ __forceinline__ double Dm() const { return q[4]; }
+    __device__ __forceinline__ double Dg(int d) const { return q[5 + d]; }
+    template <bool S> __device__ __forceinline__ double Sw(int c) const { return q[(S ? 1 : 8) + c]; }
+    __device__ __forceinline__ double Sg(int c, int d) const { return q[8 + KC + 3 * c + d]; }
+};
+
+// The terms of one pair (sample at (sxv, syv, szv) with h_a = ha, 1/ha = iha;
+// particle xb, hb, ihb = 1/hb, columns Ab) with the sample's sum cotangents R.
+template <int ST, int KC, bool SCAL, int KF, class Rows>
+__device__ __forceinline__ void adj_pair(const TreeView<double>& pt, const double xb[3], double hb, double ihb,
+                                         const double (&Ab)[KC], int kc, double sxv, double syv, double szv, double ha,
+                                         double iha, const Rows& R, AdjAcc<KC>& S) {
+    const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
+    const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
+    const double ir = (r2 > 0.0) ? rsqrt(r2) : 0.0;
+    const double r = r2 * ir;
+    double W, g[3], H[6];
+    if (ST == ST_GATHER) {
+        whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, W, g, H);
+    } else if (ST == ST_SCATTER) {
+        whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, W, g, H);
+    } else {
+        double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
+        whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, Wa, ga3, Ha);
+        whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, Wb, gb3, Hb);
+        W = 0.5 * (Wa + Wb);
+        for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
+        if (!SCAL)
+            for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
+    }
+    if constexpr (SCAL) {
+        double aS = R.template S1<SCAL>();
+#pragma unroll
+        for (int c = 0; c < KC; ++c) {
+            if (c < kc) {
+                const double lsw = R.template Sw<SCAL>(c);
+                aS += lsw * Ab[c];
+                S.sA[c] += lsw * W;
+            }
+        }
+        S.sW += aS * W;
+        for (int d = 0; d < 3; ++d) S.vS[d] += aS * g[d];
+        return;
+    }
+    const double lS1 = R.template S1<SCAL>();
+    const double lG[3] = {R.G(0), R.G(1), R.G(2)};
+    const double lDm = R.Dm();
+    const double lDg[3] = {R.Dg(0), R.Dg(1), R.Dg(2)};
+    double aS = lS1, aG[3] = {lG[0], lG[1], lG[2]};
+#pragma unroll
+    for (int c = 0; c < KC; ++c) {
+        if (c < kc) {
+            const double lsw = R.template Sw<SCAL>(c);
+            const double lsg[3] = {R.Sg(c, 0), R.Sg(c, 1), R.Sg(c, 2)};
+            aS += lsw * Ab[c];
+            aG[0] += Ab[c] * lsg[0]; aG[1] += Ab[c] * lsg[1]; aG[2] += Ab[c] * lsg[2];
+            S.sA[c] += lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2];
+        }
+    }
+    S.sW += aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2];
+    S.sD += lDm * W + lDg[0] * g[0] + lDg[1] * g[1] + lDg[2] * g[2];
+    double Ha[3], Hd[3];
+    hmul(H, aG, Ha);
+    hmul(H, lDg, Hd);
+    for (int d = 0; d < 3; ++d) {
+        S.vS[d] += aS * g[d] + Ha[d];
+        S.vD[d] += lDm * g[d] + Hd[d];
+    }
+}
+
+// the gradients of particle b (Morton position) from its sums
+template <int KC>
+__device__ __forceinline__ void adj_write(const AdjArgs& A, int64_t b, const AdjAcc<KC>& S, double mb, double rhob,
+                                          int kc) {
+    const double mr = mb / rhob;
+    const int64_t o = A.porder[b];
+    A.gm[o] = S.sW / rhob + S.sD;
+    A.gx[o] = -(mr * S.vS[0] + mb * S.vD[0]);
+    A.gy[o] = -(mr * S.vS[1] + mb * S.vD[1]);
+    A.gz[o] = -(mr * S.vS[2] + mb * S.vD[2]);
+#pragma unroll
+    for (int c = 0; c < KC; ++c)
+        if (c < kc && A.gcol[c]) A.gcol[c][o] = mr * S.sA[c];
+}
+
 struct AStage {
     double sx[SPAN], sy[SPAN], sz[SPAN], sh[SPAN];  // samples of the span, h_a
     double sih[SPAN];                               // 1 / h_a
@@ -145,17 +296,24 @@ template <int KC, bool SCAL> struct ALam {
 // the cotangent row (in A.lam) of staged row r
 template <bool SCAL> __device__ __forceinline__ int lam_row(int r) { return SCAL ? (r == 0 ? 0 : 7 + r) : r; }
 
-template <int ST, int KC, bool SCAL, int KF>
-__global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs A) {
+// COL: the pair-list pass of the two-kernel path (k_adj_collect): the same
+// walk and pair decisions, with each lane's accepted samples of a span
+// written to its tile's chain of list blocks instead of summed.
+template <int ST, int KC, bool SCAL, int KF, bool COL = false>
+__global__ void __launch_bounds__(128, (COL || SCAL) ? 8 : 4) k_adj_points(const AdjArgs A) {
     __shared__ AStage stage_all[4];
-    constexpr bool STAGE = SCAL || KC <= 4;
+    constexpr bool STAGE = !COL && (SCAL || KC <= 4);
     __shared__ ALam<STAGE ? KC : 1, SCAL> lam_all[STAGE ? 4 : 1];
     const TreeView<double>& pt = A.pt;
     const TreeView<double>& sv = A.sv;
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     AStage& st = stage_all[wib];
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    if (A.tile_list) {  // the tiles the two-kernel path handed back
+        if (tile >= (int64_t)*A.tile_count) return;
+        tile = A.tile_list[tile];
+    }
     if (tile * 32 >= pt.n) return;  // warp-uniform
     const int64_t b = tile * 32 + lane;
     const bool valid = b < pt.n;
@@ -197,14 +355,9 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         esmax = fmaxf(esmax, __shfl_xor_sync(PSB_FULL, esmax, o));
         rbmax = fmaxf(rbmax, __shfl_xor_sync(PSB_FULL, rbmax, o));
     }
-    const double mr = mb / rhob;
     const double ihb = 1.0 / hb;
-    // pair sums; the particle's factors 1/rho_b, m_b/rho_b and m_b are applied
-    // once after the walk: dL/dm_b = sW / rho_b + sD, dL/dA_c,b = m_b/rho_b sA_c,
-    // dL/dx_b = -(m_b/rho_b vS + m_b vD)
-    double sW = 0.0, sD = 0.0, vS[3] = {0.0, 0.0, 0.0}, vD[3] = {0.0, 0.0, 0.0}, sA[KC];
-#pragma unroll
-    for (int c = 0; c < KC; ++c) sA[c] = 0.0;
+    AdjAcc<KC> S;
+    S.zero();
     const int kc = A.kc;
     const int64_t L = A.lam_stride;
     unsigned long long n_pairs = 0, n_spans = 0, n_parts = 0, n_leaves = 0;  // work counters (warp-uniform)
@@ -214,66 +367,38 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     // li: the sample; jj: its slot in the span
     auto pair = [&](int64_t li, int jj, double sxv, double syv, double szv, double ha, double iha) {
         ++n_pairs;
-        const double dl[3] = {sxv - xb[0], syv - xb[1], szv - xb[2]};
-        const double r2 = dl[0] * dl[0] + dl[1] * dl[1] + dl[2] * dl[2];
-        const double ir = (r2 > 0.0) ? rsqrt(r2) : 0.0;
-        const double r = r2 * ir;
-        double W, g[3], H[6];
-        if (ST == ST_GATHER) {
-            whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, W, g, H);
-        } else if (ST == ST_SCATTER) {
-            whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, W, g, H);
-        } else {
-            double Wa, ga3[3], Ha[6], Wb, gb3[3], Hb[6];
-            whess<KF, !SCAL>(pt, dl, r, ir, ha, iha, Wa, ga3, Ha);
-            whess<KF, !SCAL>(pt, dl, r, ir, hb, ihb, Wb, gb3, Hb);
-            W = 0.5 * (Wa + Wb);
-            for (int d = 0; d < 3; ++d) g[d] = 0.5 * (ga3[d] + gb3[d]);
-            if (!SCAL)
-                for (int d = 0; d < 6; ++d) H[d] = 0.5 * (Ha[d] + Hb[d]);
-        }
-        if constexpr (SCAL) {
-            const double* ls = lst + jj;
-            double aS = ls[0];
-#pragma unroll
-            for (int c = 0; c < KC; ++c) {
-                if (c < kc) {
-                    const double lsw = ls[(1 + c) * SPAN];
-                    aS += lsw * Ab[c];
-                    sA[c] += lsw * W;
-                }
-            }
-            sW += aS * W;
-            for (int d = 0; d < 3; ++d) vS[d] += aS * g[d];
-            return;
-        }
         // row r of this sample: staged, or from global memory
-        const double* ls = STAGE ? lst + jj : A.lam + li;
-        const int64_t rs = STAGE ? (int64_t)SPAN : L;
-        const double lS1 = ls[0];
-        const double lG[3] = {ls[rs], ls[2 * rs], ls[3 * rs]};
-        const double lDm = ls[4 * rs];
-        const double lDg[3] = {ls[5 * rs], ls[6 * rs], ls[7 * rs]};
-        double aS = lS1, aG[3] = {lG[0], lG[1], lG[2]};
-#pragma unroll
-        for (int c = 0; c < KC; ++c) {
-            if (c < kc) {
-                const double lsw = ls[(8 + c) * rs];
-                const double lsg[3] = {ls[(8 + kc + 3 * c) * rs], ls[(9 + kc + 3 * c) * rs],
-                                       ls[(10 + kc + 3 * c) * rs]};
-                aS += lsw * Ab[c];
-                aG[0] += Ab[c] * lsg[0]; aG[1] += Ab[c] * lsg[1]; aG[2] += Ab[c] * lsg[2];
-                sA[c] += lsw * W + lsg[0] * g[0] + lsg[1] * g[1] + lsg[2] * g[2];
+        const RowsStrided R{STAGE ? lst + jj : A.lam + li, STAGE ? (int64_t)SPAN : L, kc};
+        adj_pair<ST, KC, SCAL, KF>(pt, xb, hb, ihb, Ab, kc, sxv, syv, szv, ha, iha, R, S);
+    };
+
+    // COL: this tile's chain of list blocks (block, this lane's entries in it)
+    int64_t blk = -1;
+    int pos = 0;
+    bool dead = false;  // the pool ran out: the tile is listed for k_adj_points
+    auto emit = [&](int64_t lo, unsigned acc) {
+        const bool want = acc != 0;
+        if (dead || !__any_sync(PSB_FULL, want)) return;
+        if (blk < 0 || __any_sync(PSB_FULL, want && pos == ADJ_CH)) {  // a new block for the warp
+            unsigned long long nb = 0;
+            if (lane == 0) nb = atomicAdd(A.al.top, 1u);
+            nb = __shfl_sync(PSB_FULL, nb, 0);
+            if ((int64_t)nb >= A.al.nblocks) {
+                dead = true;
+                return;
             }
+            if (blk >= 0) {
+                A.al.bcnt[blk * 32 + lane] = (uint8_t)pos;
+                if (lane == 0) A.al.bnext[blk] = (int32_t)nb;
+            } else if (lane == 0) {
+                A.al.head[tile] = (int32_t)nb;
+            }
+            blk = (int64_t)nb;
+            pos = 0;
         }
-        sW += aS * W + aG[0] * g[0] + aG[1] * g[1] + aG[2] * g[2];
-        sD += lDm * W + lDg[0] * g[0] + lDg[1] * g[1] + lDg[2] * g[2];
-        double Ha[3], Hd[3];
-        hmul(H, aG, Ha);
-        hmul(H, lDg, Hd);
-        for (int d = 0; d < 3; ++d) {
-            vS[d] += aS * g[d] + Ha[d];
-            vD[d] += lDm * g[d] + Hd[d];
+        if (want) {
+            A.al.ent[((size_t)blk * ADJ_CH + pos) * 32 + lane] = make_uint2((unsigned)lo, acc);
+            ++pos;
         }
     };
 
@@ -320,7 +445,7 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
         if (lane < cnt) {
             st.sx[lane] = __ldg(&sv.x[lo + lane]); st.sy[lane] = __ldg(&sv.y[lo + lane]);
             st.sz[lane] = __ldg(&sv.z[lo + lane]); st.sh[lane] = __ldg(&sv.h[lo + lane]);
-            st.sih[lane] = 1.0 / st.sh[lane];
+            if (!COL) st.sih[lane] = 1.0 / st.sh[lane];
             const float4 Lq = __ldg(&sv.leaf4[lo + lane]);
             Qme = make_float4(Lq.x + o0, Lq.y + o1, Lq.z + o2, Lq.w);
             st.Q[lane] = Qme;
@@ -380,33 +505,43 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
             const double e2 = ex_d2_pp<double>(ps, xb[0], xb[1], xb[2]);
             if (e2 <= ex_r2<ST, double>(ra2, hb, Kd)) acc |= 1u << jj;
         }
-        if constexpr (STAGE) {  // stage the span's cotangent rows (a warp-uniform decision)
-            if (__any_sync(PSB_FULL, acc != 0)) {
-                double* lw = lam_all[wib].q;
-                const int nq = SCAL ? 1 + kc : 8 + 4 * kc;
-                if (lane < cnt)
-                    for (int r = 0; r < nq; ++r) lw[r * SPAN + lane] = __ldg(&A.lam[lam_row<SCAL>(r) * L + lo + lane]);
-                __syncwarp();
+        if constexpr (COL) {
+            emit(lo, acc);
+        } else {
+            if constexpr (STAGE) {  // stage the span's cotangent rows (a warp-uniform decision)
+                if (__any_sync(PSB_FULL, acc != 0)) {
+                    double* lw = lam_all[wib].q;
+                    const int nq = SCAL ? 1 + kc : 8 + 4 * kc;
+                    if (lane < cnt)
+                        for (int r = 0; r < nq; ++r)
+                            lw[r * SPAN + lane] = __ldg(&A.lam[lam_row<SCAL>(r) * L + lo + lane]);
+                    __syncwarp();
+                }
             }
+            for (; acc; acc &= acc - 1) {
+                const int jj = __ffs(acc) - 1;
+                pair(lo + jj, jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj], st.sih[jj]);
+            }
+            if constexpr (STAGE) __syncwarp();  // the rows are read before the next span's
         }
-        for (; acc; acc &= acc - 1) {
-            const int jj = __ffs(acc) - 1;
-            pair(lo + jj, jj, st.sx[jj], st.sy[jj], st.sz[jj], st.sh[jj], st.sih[jj]);
-        }
-        if constexpr (STAGE) __syncwarp();  // the rows are read before the next span's
     };
     const int32_t start = (sv.root == 0) ? (int32_t)sv.n : sv.root;
     const bool ok = warp_traverse_spans(start, sv.n, sv.links, sv.escape, valid, node_fn, span_fn, steps);
 
-    if (valid) {
-        const int64_t o = A.porder[b];
-        A.gm[o] = sW / rhob + sD;
-        A.gx[o] = -(mr * vS[0] + mb * vD[0]);
-        A.gy[o] = -(mr * vS[1] + mb * vD[1]);
-        A.gz[o] = -(mr * vS[2] + mb * vD[2]);
-#pragma unroll
-        for (int c = 0; c < KC; ++c)
-            if (c < kc && A.gcol[c]) A.gcol[c][o] = mr * sA[c];
+    if constexpr (COL) {
+        if (dead) {
+            if (lane == 0) {
+                A.al.head[tile] = -2;
+                A.al.ovf_tiles[atomicAdd(A.al.ovf_count, 1u)] = (int32_t)tile;
+            }
+        } else if (blk >= 0) {
+            A.al.bcnt[blk * 32 + lane] = (uint8_t)pos;
+            if (lane == 0) A.al.bnext[blk] = -1;
+        } else if (lane == 0) {
+            A.al.head[tile] = -1;
+        }
+    } else if (valid) {
+        adj_write<KC>(A, b, S, mb, rhob, kc);
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
@@ -419,6 +554,111 @@ __global__ void __launch_bounds__(128, SCAL ? 8 : 4) k_adj_points(const AdjArgs 
     }
 
     if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
+}
+
+// The pair terms of the two-kernel path: one lane per particle runs through
+// its tile's list blocks in one flattened loop (a warp iteration does the
+// pairs of up to 32 particles until the shortest lists run out), reading each
+// pair's sample and its sum cotangents (sample-major rows, lamT) from global
+// memory.  Pairs come in the order of k_adj_points, with the same terms
+// (adj_pair), so both give the same bits.
+template <int ST, int KC, bool SCAL, int KF>
+__global__ void __launch_bounds__(128, 4) k_adj_bodies(const AdjArgs A) {
+    const TreeView<double>& pt = A.pt;
+    const int lane = threadIdx.x & 31;
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tile * 32 >= pt.n) return;  // warp-uniform
+    const int32_t h0 = A.al.head[tile];
+    if (h0 == -2) return;  // overflowed: k_adj_points owns the tile
+    const int64_t b = tile * 32 + lane;
+    const bool valid = b < pt.n;
+    const int kc = A.kc;
+    double xb[3] = {0.0, 0.0, 0.0}, hb = 1.0, mb = 0.0, rhob = 1.0, Ab[KC];
+#pragma unroll
+    for (int c = 0; c < KC; ++c) Ab[c] = 0.0;
+    if (valid) {
+        xb[0] = pt.x[b]; xb[1] = pt.y[b]; xb[2] = pt.z[b];
+        hb = pt.h[b]; mb = pt.m[b]; rhob = pt.rho[b];
+#pragma unroll
+        for (int c = 0; c < KC; ++c)
+            if (c < kc) Ab[c] = A.colT[c][b];
+    }
+    const double ihb = 1.0 / hb;
+    AdjAcc<KC> S;
+    S.zero();
+    // this lane's list: block, entry in it, entries of the lane in it
+    int64_t blk = h0;
+    int e = 0, ne = (valid && blk >= 0) ? A.al.bcnt[blk * 32 + lane] : 0;
+    unsigned m = 0;
+    int64_t lo = 0;
+    auto next = [&]() -> bool {  // the next pair of this lane's list: sample lo + ffs(m) - 1
+        while (m == 0) {
+            if (e < ne) {
+                const uint2 q = A.al.ent[((size_t)blk * ADJ_CH + e) * 32 + lane];
+                lo = (int64_t)q.x;
+                m = q.y;
+                ++e;
+            } else {
+                if (blk < 0 || !valid) return false;
+                blk = A.al.bnext[blk];
+                if (blk < 0) return false;
+                e = 0;
+                ne = A.al.bcnt[blk * 32 + lane];
+            }
+        }
+        return true;
+    };
+    unsigned long long n_pairs = 0;
+    bool has = next();
+    while (__any_sync(PSB_FULL, has)) {
+        if (has) {
+            const int64_t s = lo + __ffs(m) - 1;
+            m &= m - 1;
+            ++n_pairs;
+            using RC = AdjRec<KC, SCAL>;
+            const double2* rp = reinterpret_cast<const double2*>(A.lamT + s * RC::N);
+            const double2 h0 = __ldg(rp), h1 = __ldg(rp + 1), h2 = __ldg(rp + 2);
+            RowsRec<KC, SCAL> R;
+#pragma unroll
+            for (int k = 0; k < (RC::N - 6) / 2; ++k) {
+                const double2 v = __ldg(rp + 3 + k);
+                R.q[2 * k] = v.x;
+                R.q[2 * k + 1] = v.y;
+            }
+            adj_pair<ST, KC, SCAL, KF>(pt, xb, hb, ihb, Ab, kc, h0.x, h0.y, h1.x, h1.y, h2.x, R, S);
+            has = next();
+        }
+    }
+    if (valid) adj_write<KC>(A, b, S, mb, rhob, kc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+    if (lane == 0 && A.stats) atomicAdd(&A.stats[6], n_pairs);
+}
+
+// The records of k_adj_bodies (AdjRec), one per sample of the sample tree:
+// position, h_a, 1/h_a and the sum cotangents (lam: rows [q][sample] in the
+// tree's order) at the record's fixed places.
+template <int KC, bool SCAL>
+__global__ void k_adj_rows(const double* lam, int64_t ns, int kc, const TreeView<double> sv, double* rec) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    using RC = AdjRec<KC, SCAL>;
+    double* o = rec + i * RC::N;
+    const double h = sv.h[i];
+    o[0] = sv.x[i]; o[1] = sv.y[i]; o[2] = sv.z[i]; o[3] = h; o[4] = 1.0 / h;
+    for (int r = 5; r < RC::N; ++r) o[r] = 0.0;
+    double* q = o + 6;
+    auto row = [&](int r) { return lam[(int64_t)r * ns + i]; };  // compact row r (kc columns)
+    if (SCAL) {
+        q[0] = row(0);
+        for (int c = 0; c < kc; ++c) q[1 + c] = row(8 + c);  // lambda_Sw_c
+    } else {
+        for (int r = 0; r < 8; ++r) q[r] = row(r);
+        for (int c = 0; c < kc; ++c) {
+            q[8 + c] = row(8 + c);
+            for (int d = 0; d < 3; ++d) q[8 + KC + 3 * c + d] = row(8 + kc + 3 * c + d);
+        }
+    }
 }
 
 // line-integrated kernel and its r-derivative: the slope of the table segment

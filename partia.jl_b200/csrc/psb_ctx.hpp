@@ -75,6 +75,8 @@ struct psb_ctx {
     int64_t adj_lam_stride = 0;
     void* adj_ha = nullptr;
     struct psb_ctx* sctx = nullptr;  // LBVH over the samples of the last adjoint call
+    int64_t adj_blocks = 0;           // list-block pool of the two-kernel point adjoint (grown to the last need)
+    int adj_split = 1;                // 0: the point adjoint runs k_adj_points alone (psb_test_adjoint_pool)
 
     cudaEvent_t ev[8] = {};
     // copy streams (in, out) and three more compute streams of the chunked

@@ -78,6 +78,7 @@ _SIGS = {
     "psb_build_lbvh": ([_vp, _vp, _vp], C.c_int),
     "psb_set_values": ([_vp, _vp, _vp, _i32, _vp, _u32], C.c_int),
     "psb_test_loop_escapes": ([_vp], C.c_int),
+    "psb_test_adjoint_pool": ([_vp, C.c_int64, C.c_int32], C.c_int),
     "psb_baseline_cudaext_points": ([_vp, _i64] + [_vp] * 6 + [_i32, _vp, C.c_int, _i32] + [_vp] * 5 +
                                     [_i64, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp], C.c_int),
     "psb_get_tree": ([_vp] * 9, C.c_int),

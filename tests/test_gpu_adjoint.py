@@ -139,6 +139,35 @@ def test_point_adjoint_device_pointers_and_unused_column():
         assert np.abs(g["cols"][c]).max() == 0
 
 
+@pytest.mark.parametrize("kernel", [L.PSB_KERNEL_M4, L.PSB_KERNEL_C4])
+@pytest.mark.parametrize("strategy,spec", [(L.PSB_SYMMETRIC, CAT), (L.PSB_GATHER, CAT),
+                                           (L.PSB_SCATTER, dict(scalars=[0, 2], shepard=[1, 0]))])
+def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
+    """The two-kernel point adjoint (pair lists in pooled blocks, then one
+    lane per particle) visits every particle's pairs in the single kernel's
+    order with the same terms: the same bits, also when a small pool leaves
+    tiles to the single kernel, and equal to the oracle."""
+    orc, ctx = setup(6000, 131, kernel)
+    rng = np.random.default_rng(132)
+    ns = 3000
+    s = tuple(rng.uniform(-0.05, 1.05, ns) for _ in range(3))
+    nl = O.Catalog(**spec).L
+    gout = [rng.standard_normal(ns) for _ in range(nl)]
+    res = []
+    for blocks, split in ((0, 1), (0, 0), (3, 1)):  # default pool, single kernel, 3 blocks
+        assert ctx.lib.psb_test_adjoint_pool(ctx.h, blocks, split) == L.PSB_OK
+        res.append(ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy))
+        assert ctx.last_stats.pairs > 0
+    for g in res[1:]:
+        for key in ("m", "x", "y", "z"):
+            assert np.array_equal(g[key], res[0][key]), key
+        for c in range(4):
+            assert np.array_equal(g["cols"][c], res[0]["cols"][c]), c
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=strategy)
+    compare(res[0], r, 4)
+    assert ctx.lib.psb_test_adjoint_pool(ctx.h, -1, 1) == L.PSB_EINVAL
+
+
 def test_grid_adjoint_matches_points():
     orc, ctx = setup(5000, 105)
     ax = np.linspace(0.05, 0.95, 14)

@@ -168,6 +168,37 @@ def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
     assert ctx.lib.psb_test_adjoint_pool(ctx.h, -1, 1) == L.PSB_EINVAL
 
 
+@pytest.mark.parametrize("spec", [
+    dict(scalars=[0, 4, 5], shepard=[1, 0, 1], grads=[4, 5], divs=[1, 2, 3], curls=[5, 4, 1]),
+    dict(scalars=[0, 1, 2, 3, 4, 5], shepard=[1, 0, 1, 0, 1, 0])])  # scalar catalog
+def test_point_adjoint_six_columns(spec):
+    """Six columns take the 8-column instantiations: records with the columns
+    past the fourth, and the general form's cotangents read from global
+    memory in the single kernel.  The two forms give the same bits, and both
+    equal the oracle."""
+    arrs, cols = particles(5000, 141)
+    rng = np.random.default_rng(142)
+    cols = cols + [np.cos(2 * arrs[1]) + 0.1 * rng.standard_normal(5000), arrs[2] ** 2 - arrs[0]]
+    orc = O.Oracle(*arrs, cols=cols)
+    ctx = Context(0)
+    ctx.set_particles(*arrs, cols=cols)
+    ctx.build(want_perm=False)
+    ns = 2500
+    s = tuple(rng.uniform(-0.05, 1.05, ns) for _ in range(3))
+    nl = O.Catalog(**spec).L
+    gout = [rng.standard_normal(ns) for _ in range(nl)]
+    res = []
+    for split in (1, 0):
+        assert ctx.lib.psb_test_adjoint_pool(ctx.h, 0, split) == L.PSB_OK
+        res.append(ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=L.PSB_SYMMETRIC))
+    for key in ("m", "x", "y", "z"):
+        assert np.array_equal(res[0][key], res[1][key]), key
+    for c in range(6):
+        assert np.array_equal(res[0]["cols"][c], res[1]["cols"][c]), c
+    r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=O.SYMMETRIC)
+    compare(res[0], r, 6)
+
+
 def test_grid_adjoint_matches_points():
     orc, ctx = setup(5000, 105)
     ax = np.linspace(0.05, 0.95, 14)

@@ -202,6 +202,42 @@ static int run_split(psb_ctx* c, Args<T>& A, int prec, int st, int* launches, in
     return PSB_OK;
 }
 
+// Heavy tiles first for parallel beams.  A line's work is the particles
+// whose support it crosses, and lines through dense clumps take many times
+// the mean: in index order the heaviest tiles can start last and leave the
+// SMs idle at the end (on the 8M-particle clump beam, a list-scheduling
+// estimate from the per-tile pair counts puts the last CTA at 1.19x the
+// ideal finish, 1.01x with the heaviest first).  The cost of a tile is
+// estimated from the particles projected onto the frame plane: each adds
+// the lines its support can cross, pi (K h / dx) (K h / dy) + 1, to the
+// tile of its centre pixel.  Only the order of the tiles changes, never a
+// result.
+template <class T>
+__global__ void k_beam_tile_cost(const TreeView<T> tv, const SampleSrc<T> s, int64_t nbx, float* cost) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= tv.n) return;
+    const double v0 = (double)tv.x[i] - (double)s.frame[0], v1 = (double)tv.y[i] - (double)s.frame[1],
+                 v2 = (double)tv.z[i] - (double)s.frame[2];
+    const double xi = v0 * (double)s.frame[3] + v1 * (double)s.frame[4] + v2 * (double)s.frame[5];
+    const double eta = v0 * (double)s.frame[6] + v1 * (double)s.frame[7] + v2 * (double)s.frame[8];
+    const double dx = ((double)s.params[1] - (double)s.params[0]) / (double)(s.nx - 1);
+    const double dy = ((double)s.params[3] - (double)s.params[2]) / (double)(s.ny - 1);
+    const double u = (xi - (double)s.params[0]) / dx, w = (eta - (double)s.params[2]) / dy;
+    const double r = tv.Kd * (double)tv.h[i];
+    const double ru = fabs(r / dx), rw = fabs(r / dy);
+    if (!(u > -ru - 1.0 && u < (double)s.nx + ru && w > -rw - 1.0 && w < (double)s.ny + rw)) return;
+    const int64_t ic = (int64_t)fmin(fmax(rint(u), 0.0), (double)(s.nx - 1));
+    const int64_t jc = (int64_t)fmin(fmax(rint(w), 0.0), (double)(s.ny - 1));
+    atomicAdd(&cost[(jc >> 2) * nbx + (ic >> 3)], (float)(3.141592653589793 * ru * rw + 1.0));
+}
+// keys for an ascending sort that puts the largest cost first
+__global__ void k_cost_keys(const float* cost, int64_t n, uint64_t* keys, uint32_t* vals) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    keys[t] = 0xFFFFFFFFull - (uint64_t)__float_as_uint(cost[t]);
+    vals[t] = (uint32_t)t;
+}
+
 template <class T>
 static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs, int st, const psb_catalog* cat,
                      int prec, void* const* out, uint32_t flags, psb_stats* stats, int what, int64_t* dcount,
@@ -365,6 +401,21 @@ static int run_typed(psb_ctx* c, const SampleReq& rq, int hmode, const void* hs,
             int rc = run_split(c, A, prec, st, &launches);
             if (rc) return rc;
         } else {
+            if (rq.line && A.src.kind == SRC_BEAM && A.src.ntiles >= 4096) {  // heavy tiles first
+                const int64_t nt = A.src.ntiles, nbx = (A.src.nx + 7) >> 3;
+                float* cost = (float*)scratch(c, 93, sizeof(float) * nt);
+                uint64_t* keys = (uint64_t*)scratch(c, 94, sizeof(uint64_t) * nt);
+                uint32_t* vals = (uint32_t*)scratch(c, 95, sizeof(uint32_t) * nt);
+                if (!cost || !keys || !vals) return fail(c, PSB_ENOMEM, "scratch allocation failed (tile order)");
+                PSB_CUDA_TRY(c, cudaMemsetAsync(cost, 0, sizeof(float) * nt, s), "memset tile costs");
+                if (c->n > 0)
+                    k_beam_tile_cost<T><<<(unsigned)((c->n + 255) / 256), 256, 0, s>>>(A.tv, A.src, nbx, cost);
+                k_cost_keys<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(cost, nt, keys, vals);
+                PSB_CUDA_TRY(c, cudaGetLastError(), "tile cost kernels");
+                PSB_CUDA_TRY(c, radix_sort_pairs(keys, vals, nt, c, 6, &launches, false, 32), "tile order sort");
+                A.tile_list = (const int32_t*)vals;
+                launches += 2;
+            }
             cudaError_t e = rq.line ? launch_lines<T>(A, prec, st, A.rec.kc, what, s)
                                     : launch_points<T>(A, prec, st, A.rec.kc, what, s);
             PSB_CUDA_TRY(c, e, "interpolation kernel launch");

@@ -286,8 +286,9 @@ __global__ void __launch_bounds__(128) k_lines(const Args<T> A) {
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     LStage<KC>& st = lstage_all[wib];
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
+    int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + wib;
     if (tile >= A.src.ntiles) return;
+    if (A.tile_list) tile = A.tile_list[tile];  // a permutation of the tiles (heavy first)
     const int64_t k = sample_of(A.src, tile, lane);
     const bool valid = k >= 0;
     T o[3] = {T(0), T(0), T(0)}, m[3] = {T(0), T(0), T(1)};

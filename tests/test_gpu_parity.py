@@ -436,6 +436,36 @@ def test_grid_box_beam_match_explicit_samples():
         assert np.array_equal(a, b, equal_nan=True)
 
 
+@pytest.mark.parametrize("prec", [L.PSB_PREC_FP64, L.PSB_PREC_FP32C])
+def test_large_beam_heavy_tiles_first_matches_explicit_lines(prec):
+    """A beam of at least 4096 tiles runs its tiles heaviest first (an
+    estimate from the particles projected onto the frame plane); only the
+    order changes, so every line equals the same line given explicitly, bit
+    for bit, for all three strategies, and the pair count is the oracle's."""
+    from partia_b200 import workloads as W
+    arrs, cols = make_particles(30_000, 83)
+    orc, ctx, _, _ = pair(arrs, cols)
+    fr = W.Frame((0.5, 0.5, 0.5), (0.3, -0.2, 1.0), (1.0, 0.0, -0.3))
+    fr.rotate(0.2, 0.1, -0.4)
+    farr = fr.as_array()
+    nx, ny = 520, 256  # 65 x 64 = 4160 tiles of 8 x 4 lines
+    prm = np.array([-0.6, 0.6, -0.55, 0.55])
+    lcat = CatalogC(scalars=[0, 1], shepard=[0, 1])
+    ox = W.plane_coordinates(farr, (prm[0], prm[1], nx), (prm[2], prm[3], ny))
+    fw = tuple(np.full(nx * ny, farr[9 + c]) for c in range(3))
+    hs = np.array([0.03])
+    for st in (L.PSB_SCATTER, L.PSB_GATHER, L.PSB_SYMMETRIC):
+        hm = L.PSB_H_CONSTANT
+        gl = ctx.interp_beam(farr, prm, nx, ny, lcat, strategy=st, hmode=hm, hs=hs, prec=prec)
+        pairs = ctx.last_stats.pairs
+        pl = ctx.interp_lines(ox, fw, lcat, strategy=st, hmode=hm, hs=hs, prec=prec)
+        assert ctx.last_stats.pairs == pairs
+        for a, b in zip(gl, pl):
+            assert np.array_equal(a, b, equal_nan=True), st
+    co, _, _ = orc.digest(ox, fw, strategy=O.SYMMETRIC, hmode=O.H_CONSTANT, hs=hs)
+    assert int(co.sum()) == pairs
+
+
 def test_error_paths():
     ctx = Context(0)
     cat = CatalogC(scalars=[0])

@@ -394,12 +394,13 @@ int psb_test_loop_escapes(psb_ctx* ctx);
 
 /* No counterpart in the reference.  For tests of the point and grid adjoint
  * (psb_adjoint_points, psb_adjoint_grid): split = 1 (the default) runs them as
- * two kernels, a walk that writes each tile of 32 particles' pair lists into
- * blocks of a pool and a pass that sums them, with the tiles that did not
- * fit recomputed by the single-kernel walk; split = 0 runs the single kernel
- * alone.  blocks > 0 sets the pool's size for the next call (each block holds
- * 16 list entries per particle of a tile; a call grows the pool to what it
- * needed), so a small pool exercises the recomputed tiles.  All settings give
+ * a walk that writes each tile of 32 particles' pair lists into blocks of a
+ * pool, a pass that sums each block's pairs, and a pass that adds each
+ * particle's block sums in the walk's order; split = 0 runs the single-kernel
+ * walk, which adds the same terms in one running sum (the same values to
+ * rounding).  blocks > 0 sets the pool's size for the next call (each block
+ * holds 16 list entries per particle of a tile); a call whose pool runs out
+ * grows it and walks again, so a small pool exercises that path and gives
  * the same bits. */
 int psb_test_adjoint_pool(psb_ctx* ctx, int64_t blocks, int32_t split);
 

@@ -23,7 +23,8 @@ namespace psb {
 int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std::vector<int>& colu);
 
 // pass: 0 = k_adj_points (whole tiles, or the listed ones), 1 = its pair-list
-// form (k_adj_collect), 2 = k_adj_bodies
+// form (k_adj_collect), 2 = k_adj_bodies (grid over list blocks), 3 =
+// k_adj_combine
 template <int KC, bool SCAL, int KF>
 static void launch_adj_points_ks(const AdjArgs& a, int st, int pass, unsigned g, cudaStream_t s) {
     if (pass == 1) {
@@ -34,6 +35,8 @@ static void launch_adj_points_ks(const AdjArgs& a, int st, int pass, unsigned g,
         if (st == ST_GATHER) k_adj_bodies<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
         else if (st == ST_SCATTER) k_adj_bodies<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
         else k_adj_bodies<ST_SYMMETRIC, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
+    } else if (pass == 3) {
+        k_adj_combine<KC><<<g, 128, 0, s>>>(a);
     } else {
         if (st == ST_GATHER) k_adj_points<ST_GATHER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
         else if (st == ST_SCATTER) k_adj_points<ST_SCATTER, KC, SCAL, KF><<<g, 128, 0, s>>>(a);
@@ -308,48 +311,73 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
             const unsigned g = (unsigned)((n + 127) / 128);
             const int kf = (c->kern == PSB_KERNEL_M4) ? 0 : 1;
             if (c->adj_split) {
-                // Two kernels: the walk writes each particle tile's pair lists
-                // into blocks of a pool (k_adj_collect, at the walk's own
-                // register budget), then one lane per particle sums its pairs
-                // (k_adj_bodies).  Tiles the pool could not hold are
-                // recomputed by k_adj_points.  The pool starts at two blocks
-                // per tile and grows to the blocks the last call asked for
-                // (at most 8 GiB).
+                // Two kernels and a combine: the walk writes each particle
+                // tile's pair lists into blocks of a pool (k_adj_points in its
+                // list form, at the walk's own register budget); one warp per
+                // list block sums the block's pairs into partial sums
+                // (k_adj_bodies), and the partial sums of each particle are
+                // added in its chain's order (k_adj_combine).  If the pool runs
+                // out, it grows to what the walk asked for and the walk runs
+                // again; after three rounds (or at the pool's 32 GiB cap) the
+                // tiles still left run in k_adj_points.  A call grows the pool
+                // for the next; it starts at two blocks per tile.
                 const int64_t ntiles = (n + 31) / 32;
-                const int64_t cap = (int64_t)(8ll << 30) / (int64_t)(ADJ_CH * 32 * 8 + 32 + 4);
+                const int nf = 8 + kcl;  // AdjAcc<kcl>::NF
+                const int64_t per_block = (int64_t)ADJ_CH * 32 * 8 + 32 + 8 + (int64_t)nf * 32 * 8;
+                const int64_t cap = (int64_t)(32ll << 30) / per_block;
                 if (c->adj_blocks <= 0) c->adj_blocks = std::min<int64_t>(cap, 2 * ntiles + 64);
-                const int64_t nb = c->adj_blocks;
                 const int nqc = scal ? 1 + kcl : 8 + 4 * kcl;
                 const int nrec = 6 + ((nqc + 1) & ~1);  // AdjRec<kcl, scal>::N
-                const size_t b_ent = sizeof(uint2) * (size_t)nb * ADJ_CH * 32, b_cnt = (size_t)nb * 32,
-                             b_next = sizeof(int32_t) * (size_t)nb, b_tile = sizeof(int32_t) * (size_t)ntiles;
-                char* pool = (char*)scratch(c, 87, b_ent + b_cnt + b_next + 2 * b_tile + 256);
                 double* recs = (double*)scratch(c, 88, sizeof(double) * (size_t)nrec * ns);
-                if (!pool || !recs) return fail(c, PSB_ENOMEM, "scratch allocation failed (adjoint pair lists)");
-                AdjLists& al = J.al;
-                al.ent = (uint2*)pool;
-                al.bcnt = (uint8_t*)(pool + b_ent);
-                al.bnext = (int32_t*)(pool + b_ent + b_cnt);
-                al.head = (int32_t*)(pool + b_ent + b_cnt + b_next);
-                al.ovf_tiles = (int32_t*)(pool + b_ent + b_cnt + b_next + b_tile);
-                al.top = (unsigned*)(pool + b_ent + b_cnt + b_next + 2 * b_tile);
-                al.ovf_count = al.top + 1;
-                al.nblocks = nb;
+                if (!recs) return fail(c, PSB_ENOMEM, "scratch allocation failed (adjoint records)");
                 J.lamT = recs;
-                PSB_CUDA_TRY(c, cudaMemsetAsync(al.top, 0, 2 * sizeof(unsigned), s), "memset pool counters");
                 launch_adj_rows(kcl, scal, lams, ns, kc, J.sv, recs, s);
-                launch_adj_points(J, kcl, st, scal, kf, 1, g, s);
-                launch_adj_points(J, kcl, st, scal, kf, 2, g, s);
-                AdjArgs F = J;
-                F.tile_list = al.ovf_tiles;
-                F.tile_count = al.ovf_count;
-                launch_adj_points(F, kcl, st, scal, kf, 0, g, s);
+                AdjLists& al = J.al;
+                unsigned ptop = 0, povf = 0;
+                for (int round = 0;; ++round) {
+                    const int64_t nb = c->adj_blocks;
+                    const size_t b_ent = sizeof(uint2) * (size_t)nb * ADJ_CH * 32, b_cnt = (size_t)nb * 32,
+                                 b_next = sizeof(int32_t) * (size_t)nb, b_part = sizeof(double) * (size_t)nb * nf * 32,
+                                 b_tile = sizeof(int32_t) * (size_t)ntiles;
+                    char* pool = (char*)scratch(c, 87, b_part + b_ent + b_cnt + 2 * b_next + 2 * b_tile + 256);
+                    if (!pool) return fail(c, PSB_ENOMEM, "scratch allocation failed (adjoint pair lists)");
+                    al.part = (double*)pool;
+                    al.ent = (uint2*)(pool + b_part);
+                    al.bcnt = (uint8_t*)(pool + b_part + b_ent);
+                    al.bnext = (int32_t*)(pool + b_part + b_ent + b_cnt);
+                    al.btile = (int32_t*)(pool + b_part + b_ent + b_cnt + b_next);
+                    al.head = (int32_t*)(pool + b_part + b_ent + b_cnt + 2 * b_next);
+                    al.ovf_tiles = (int32_t*)(pool + b_part + b_ent + b_cnt + 2 * b_next + b_tile);
+                    al.top = (unsigned*)(pool + b_part + b_ent + b_cnt + 2 * b_next + 2 * b_tile);
+                    al.ovf_count = al.top + 1;
+                    al.nblocks = nb;
+                    PSB_CUDA_TRY(c, cudaMemsetAsync(al.top, 0, 2 * sizeof(unsigned), s), "memset pool counters");
+                    launch_adj_points(J, kcl, st, scal, kf, 1, g, s);
+                    PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint walk launch");
+                    unsigned hc[2] = {0, 0};
+                    PSB_CUDA_TRY(c, cudaMemcpyAsync(hc, al.top, sizeof(hc), cudaMemcpyDeviceToHost, s), "pool D2H");
+                    PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
+                    ptop = hc[0];
+                    povf = hc[1];
+                    launches += 1;
+                    if (povf == 0 || round == 2 || nb >= cap) break;
+                    // the tiles that ran out stopped asking: at least double the pool
+                    c->adj_blocks = std::min<int64_t>(cap, std::max<int64_t>(2 * nb, (int64_t)ptop + ptop / 4 + 64));
+                }
+                const int64_t used = std::min<int64_t>((int64_t)ptop, c->adj_blocks);
+                if (used > 0) launch_adj_points(J, kcl, st, scal, kf, 2, (unsigned)((used + 3) / 4), s);
+                launch_adj_points(J, kcl, st, scal, kf, 3, g, s);
+                if (povf) {  // tiles the largest pool could not hold
+                    AdjArgs F = J;
+                    F.tile_list = al.ovf_tiles;
+                    F.tile_count = al.ovf_count;
+                    launch_adj_points(F, kcl, st, scal, kf, 0, g, s);
+                    ++launches;
+                }
                 PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
-                unsigned ptop = 0;
-                PSB_CUDA_TRY(c, cudaMemcpyAsync(&ptop, al.top, sizeof(unsigned), cudaMemcpyDeviceToHost, s), "pool D2H");
-                PSB_CUDA_TRY(c, cudaStreamSynchronize(s), "synchronize");
-                if ((int64_t)ptop > nb) c->adj_blocks = std::min<int64_t>(cap, (int64_t)ptop + ptop / 4 + 64);
-                launches += 6;
+                if ((int64_t)ptop > c->adj_blocks)
+                    c->adj_blocks = std::min<int64_t>(cap, (int64_t)ptop + ptop / 4 + 64);
+                launches += 3;
             } else {
                 launch_adj_points(J, kcl, st, scal, kf, 0, g, s);
                 PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");

@@ -32,13 +32,17 @@ namespace psb {
 // particles, taken from a pool with an atomic counter.  A block holds up to
 // ADJ_CH entries per lane; an entry is a span of the sample tree (its first
 // sample) and the mask of the samples that pair with the lane's particle.
-// A tile for which the pool runs out is listed and recomputed by
-// k_adj_points.
+// The warp takes a new block when any lane's is full, so where a chain's
+// blocks begin and end follows from the walk alone.  A tile for which the
+// pool runs out is marked and listed (the host grows the pool and walks
+// again).
 constexpr int ADJ_CH = 16;
 struct AdjLists {
     uint2* ent;           // [block][ADJ_CH][32]: (first sample of the span, mask)
     uint8_t* bcnt;        // [block][32]: entries of each lane in the block
     int32_t* bnext;       // [block]: the tile's next block, -1 after its last
+    int32_t* btile;       // [block]: the block's tile
+    double* part;         // [block][8 + KC][32]: the block's partial sums (AdjAcc fields)
     int32_t* head;        // [tile]: first block, -1 without pairs, -2 overflowed
     unsigned* top;        // blocks taken
     int64_t nblocks;      // pool size
@@ -148,6 +152,7 @@ __device__ __forceinline__ void hmul(const double H[6], const double v[3], doubl
 // dL/dm_b = sW / rho_b + sD, dL/dA_c,b = m_b/rho_b sA_c,
 // dL/dx_b = -(m_b/rho_b vS + m_b vD)
 template <int KC> struct AdjAcc {
+    static constexpr int NF = 8 + KC;  // fields, in the order of f()
     double sW, sD, vS[3], vD[3], sA[KC];
     __device__ __forceinline__ void zero() {
         sW = 0.0; sD = 0.0;
@@ -155,6 +160,10 @@ template <int KC> struct AdjAcc {
         for (int d = 0; d < 3; ++d) { vS[d] = 0.0; vD[d] = 0.0; }
 #pragma unroll
         for (int c = 0; c < KC; ++c) sA[c] = 0.0;
+    }
+    // field i: sW, sD, vS (3), vD (3), sA (KC)
+    __device__ __forceinline__ double& f(int i) {
+        return i == 0 ? sW : (i == 1 ? sD : (i < 5 ? vS[i - 2] : (i < 8 ? vD[i - 5] : sA[i - 8])));
     }
 };
 
@@ -393,6 +402,7 @@ __global__ void __launch_bounds__(128, (COL || SCAL) ? 8 : 4) k_adj_points(const
             } else if (lane == 0) {
                 A.al.head[tile] = (int32_t)nb;
             }
+            if (lane == 0) A.al.btile[nb] = (int32_t)tile;
             blk = (int64_t)nb;
             pos = 0;
         }
@@ -556,55 +566,50 @@ __global__ void __launch_bounds__(128, (COL || SCAL) ? 8 : 4) k_adj_points(const
     if (!ok && lane == 0) atomicOr(A.err, PSB_DERR_TRAVERSAL);
 }
 
-// The pair terms of the two-kernel path: one lane per particle runs through
-// its tile's list blocks in one flattened loop (a warp iteration does the
-// pairs of up to 32 particles until the shortest lists run out), reading each
-// pair's sample and its sum cotangents (sample-major rows, lamT) from global
-// memory.  Pairs come in the order of k_adj_points, with the same terms
-// (adj_pair), so both give the same bits.
+// The pair terms of the two-kernel path, one list block per warp: lane j
+// sums the pairs of the block's entries of particle j of the block's tile
+// (its own partial sums, from zero) and stores them with the block.  A block
+// holds at most ADJ_CH entries per lane, so the work items are of like size
+// however long a particle's list is: a tile of large-h particles in the
+// outskirts (pair lists 60 times the mean tile's) spreads over as many warps
+// as it has blocks, where one warp per tile left it running long after the
+// others.  Each pair reads its sample as one record (AdjRec) with 128-bit
+// loads.
 template <int ST, int KC, bool SCAL, int KF>
 __global__ void __launch_bounds__(128, 4) k_adj_bodies(const AdjArgs A) {
     const TreeView<double>& pt = A.pt;
     const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile * 32 >= pt.n) return;  // warp-uniform
-    const int32_t h0 = A.al.head[tile];
-    if (h0 == -2) return;  // overflowed: k_adj_points owns the tile
+    const int64_t blk = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t used = (int64_t)*A.al.top;
+    if (blk >= (used < A.al.nblocks ? used : A.al.nblocks)) return;  // warp-uniform
+    const int64_t tile = A.al.btile[blk];
     const int64_t b = tile * 32 + lane;
     const bool valid = b < pt.n;
     const int kc = A.kc;
-    double xb[3] = {0.0, 0.0, 0.0}, hb = 1.0, mb = 0.0, rhob = 1.0, Ab[KC];
+    double xb[3] = {0.0, 0.0, 0.0}, hb = 1.0, Ab[KC];
 #pragma unroll
     for (int c = 0; c < KC; ++c) Ab[c] = 0.0;
     if (valid) {
         xb[0] = pt.x[b]; xb[1] = pt.y[b]; xb[2] = pt.z[b];
-        hb = pt.h[b]; mb = pt.m[b]; rhob = pt.rho[b];
+        hb = pt.h[b];
 #pragma unroll
         for (int c = 0; c < KC; ++c)
             if (c < kc) Ab[c] = A.colT[c][b];
     }
     const double ihb = 1.0 / hb;
-    AdjAcc<KC> S;
-    S.zero();
-    // this lane's list: block, entry in it, entries of the lane in it
-    int64_t blk = h0;
-    int e = 0, ne = (valid && blk >= 0) ? A.al.bcnt[blk * 32 + lane] : 0;
+    AdjAcc<KC> P;
+    P.zero();
+    const int ne = valid ? A.al.bcnt[blk * 32 + lane] : 0;
+    int e = 0;
     unsigned m = 0;
     int64_t lo = 0;
-    auto next = [&]() -> bool {  // the next pair of this lane's list: sample lo + ffs(m) - 1
+    auto next = [&]() -> bool {  // the next pair: sample lo + ffs(m) - 1
         while (m == 0) {
-            if (e < ne) {
-                const uint2 q = A.al.ent[((size_t)blk * ADJ_CH + e) * 32 + lane];
-                lo = (int64_t)q.x;
-                m = q.y;
-                ++e;
-            } else {
-                if (blk < 0 || !valid) return false;
-                blk = A.al.bnext[blk];
-                if (blk < 0) return false;
-                e = 0;
-                ne = A.al.bcnt[blk * 32 + lane];
-            }
+            if (e >= ne) return false;
+            const uint2 q = A.al.ent[((size_t)blk * ADJ_CH + e) * 32 + lane];
+            lo = (int64_t)q.x;
+            m = q.y;
+            ++e;
         }
         return true;
     };
@@ -625,14 +630,55 @@ __global__ void __launch_bounds__(128, 4) k_adj_bodies(const AdjArgs A) {
                 R.q[2 * k] = v.x;
                 R.q[2 * k + 1] = v.y;
             }
-            adj_pair<ST, KC, SCAL, KF>(pt, xb, hb, ihb, Ab, kc, h0.x, h0.y, h1.x, h1.y, h2.x, R, S);
+            adj_pair<ST, KC, SCAL, KF>(pt, xb, hb, ihb, Ab, kc, h0.x, h0.y, h1.x, h1.y, h2.x, R, P);
             has = next();
         }
     }
-    if (valid) adj_write<KC>(A, b, S, mb, rhob, kc);
+    if (A.al.head[tile] == blk && A.al.bnext[blk] < 0) {
+        // the tile's only block: its sums are the particles' (k_adj_combine
+        // starts from the first block's sums, so both give the same bits)
+        if (valid) adj_write<KC>(A, b, P, pt.m[b], pt.rho[b], kc);
+    } else {
+        double* o = A.al.part + (size_t)blk * AdjAcc<KC>::NF * 32 + lane;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, o);
+        for (int f = 0; f < AdjAcc<KC>::NF; ++f) o[(size_t)f * 32] = P.f(f);
+    }
+#pragma unroll
+    for (int q = 16; q > 0; q >>= 1) n_pairs += __shfl_xor_sync(PSB_FULL, n_pairs, q);
     if (lane == 0 && A.stats) atomicAdd(&A.stats[6], n_pairs);
+}
+
+// The gradients of each particle of a tile of several blocks (and zeros for
+// a tile without pairs): its blocks' partial sums added in the order of its
+// tile's chain (the order the walk met the spans), then the particle's
+// factors (adj_write).  The blocks' boundaries follow from the
+// walk, so the result does not depend on the pool or on which block landed
+// where in it.
+template <int KC>
+__global__ void __launch_bounds__(128) k_adj_combine(const AdjArgs A) {
+    const TreeView<double>& pt = A.pt;
+    const int lane = threadIdx.x & 31;
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tile * 32 >= pt.n) return;
+    const int64_t b = tile * 32 + lane;
+    if (b >= pt.n) return;
+    int64_t blk = A.al.head[tile];
+    if (blk == -2) return;  // overflowed: k_adj_points owns the tile
+    AdjAcc<KC> T;
+    T.zero();
+    if (blk >= 0) {
+        int64_t nxt = A.al.bnext[blk];
+        if (nxt < 0) return;  // one block: k_adj_bodies wrote the gradients
+        const double* o = A.al.part + (size_t)blk * AdjAcc<KC>::NF * 32 + lane;
+#pragma unroll
+        for (int f = 0; f < AdjAcc<KC>::NF; ++f) T.f(f) = o[(size_t)f * 32];
+        for (blk = nxt; blk >= 0; blk = A.al.bnext[blk]) {
+            o = A.al.part + (size_t)blk * AdjAcc<KC>::NF * 32 + lane;
+#pragma unroll
+            for (int f = 0; f < AdjAcc<KC>::NF; ++f) T.f(f) += o[(size_t)f * 32];
+        }
+    }
+    adj_write<KC>(A, b, T, pt.m[b], pt.rho[b], A.kc);
 }
 
 // The records of k_adj_bodies (AdjRec), one per sample of the sample tree:

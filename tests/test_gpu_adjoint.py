@@ -143,10 +143,11 @@ def test_point_adjoint_device_pointers_and_unused_column():
 @pytest.mark.parametrize("strategy,spec", [(L.PSB_SYMMETRIC, CAT), (L.PSB_GATHER, CAT),
                                            (L.PSB_SCATTER, dict(scalars=[0, 2], shepard=[1, 0]))])
 def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
-    """The two-kernel point adjoint (pair lists in pooled blocks, then one
-    lane per particle) visits every particle's pairs in the single kernel's
-    order with the same terms: the same bits, also when a small pool leaves
-    tiles to the single kernel, and equal to the oracle."""
+    """The two-kernel point adjoint (pair lists in pooled blocks, partial sums
+    per list block, added per particle in the walk's order): the same bits
+    whatever the pool's size (a pool of 3 blocks grows and walks again),
+    within 1e-12 of the single kernel (which adds the same terms in one
+    running sum) and equal to the oracle."""
     orc, ctx = setup(6000, 131, kernel)
     rng = np.random.default_rng(132)
     ns = 3000
@@ -154,15 +155,17 @@ def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
     nl = O.Catalog(**spec).L
     gout = [rng.standard_normal(ns) for _ in range(nl)]
     res = []
-    for blocks, split in ((0, 1), (0, 0), (3, 1)):  # default pool, single kernel, 3 blocks
+    for blocks, split in ((0, 1), (3, 1), (0, 0)):  # default pool, 3 blocks, single kernel
         assert ctx.lib.psb_test_adjoint_pool(ctx.h, blocks, split) == L.PSB_OK
         res.append(ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy))
         assert ctx.last_stats.pairs > 0
-    for g in res[1:]:
-        for key in ("m", "x", "y", "z"):
-            assert np.array_equal(g[key], res[0][key]), key
-        for c in range(4):
-            assert np.array_equal(g["cols"][c], res[0]["cols"][c]), c
+    for key in ("m", "x", "y", "z"):
+        assert np.array_equal(res[1][key], res[0][key]), key
+        assert close(res[2][key], res[0][key]) <= 1e-12, key
+    for c in range(4):
+        assert np.array_equal(res[1]["cols"][c], res[0]["cols"][c]), c
+        if np.abs(res[0]["cols"][c]).max() > 0:
+            assert close(res[2]["cols"][c], res[0]["cols"][c]) <= 1e-12, c
     r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=strategy)
     compare(res[0], r, 4)
     assert ctx.lib.psb_test_adjoint_pool(ctx.h, -1, 1) == L.PSB_EINVAL
@@ -174,7 +177,7 @@ def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
 def test_point_adjoint_six_columns(spec):
     """Six columns take the 8-column instantiations: records with the columns
     past the fourth, and the general form's cotangents read from global
-    memory in the single kernel.  The two forms give the same bits, and both
+    memory in the single kernel.  The two forms agree within 1e-12, and both
     equal the oracle."""
     arrs, cols = particles(5000, 141)
     rng = np.random.default_rng(142)
@@ -192,11 +195,13 @@ def test_point_adjoint_six_columns(spec):
         assert ctx.lib.psb_test_adjoint_pool(ctx.h, 0, split) == L.PSB_OK
         res.append(ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=L.PSB_SYMMETRIC))
     for key in ("m", "x", "y", "z"):
-        assert np.array_equal(res[0][key], res[1][key]), key
+        assert close(res[1][key], res[0][key]) <= 1e-12, key
     for c in range(6):
-        assert np.array_equal(res[0]["cols"][c], res[1]["cols"][c]), c
+        if np.abs(res[0]["cols"][c]).max() > 0:
+            assert close(res[1]["cols"][c], res[0]["cols"][c]) <= 1e-12, c
     r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=O.SYMMETRIC)
     compare(res[0], r, 6)
+    compare(res[1], r, 6)
 
 
 def test_grid_adjoint_matches_points():

@@ -401,7 +401,8 @@ int psb_test_loop_escapes(psb_ctx* ctx);
  * rounding).  blocks > 0 sets the pool's size for the next call (each block
  * holds 16 list entries per particle of a tile); a call whose pool runs out
  * grows it and walks again, so a small pool exercises that path and gives
- * the same bits. */
+ * the same bits.  split = 2 is split = 1 with a pool that keeps its size: the
+ * tiles that do not fit run in the single-kernel walk. */
 int psb_test_adjoint_pool(psb_ctx* ctx, int64_t blocks, int32_t split);
 
 /* ---- interpolation without device allocation -------------------------------- */

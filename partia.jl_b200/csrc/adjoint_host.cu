@@ -360,7 +360,7 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
                     ptop = hc[0];
                     povf = hc[1];
                     launches += 1;
-                    if (povf == 0 || round == 2 || nb >= cap) break;
+                    if (povf == 0 || c->adj_split == 2 || round == 2 || nb >= cap) break;
                     // the tiles that ran out stopped asking: at least double the pool
                     c->adj_blocks = std::min<int64_t>(cap, std::max<int64_t>(2 * nb, (int64_t)ptop + ptop / 4 + 64));
                 }
@@ -375,7 +375,7 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
                     ++launches;
                 }
                 PSB_CUDA_TRY(c, cudaGetLastError(), "adjoint kernel launch");
-                if ((int64_t)ptop > c->adj_blocks)
+                if ((int64_t)ptop > c->adj_blocks && c->adj_split != 2)
                     c->adj_blocks = std::min<int64_t>(cap, (int64_t)ptop + ptop / 4 + 64);
                 launches += 3;
             } else {

@@ -442,7 +442,8 @@ PSB_API int psb_test_adjoint_pool(psb_ctx* c, int64_t blocks, int32_t split) {
     c->err.clear();
     if (blocks < 0) return fail(c, PSB_EINVAL, "blocks must be non-negative");
     if (blocks > 0) c->adj_blocks = blocks;
-    c->adj_split = split ? 1 : 0;
+    if (split < 0 || split > 2) return fail(c, PSB_EINVAL, "split must be 0, 1 or 2");
+    c->adj_split = split;
     return PSB_OK;
 }
 

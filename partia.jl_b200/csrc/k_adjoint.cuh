@@ -583,6 +583,9 @@ __global__ void __launch_bounds__(128, 4) k_adj_bodies(const AdjArgs A) {
     const int64_t used = (int64_t)*A.al.top;
     if (blk >= (used < A.al.nblocks ? used : A.al.nblocks)) return;  // warp-uniform
     const int64_t tile = A.al.btile[blk];
+    // A tile the pool ran out on is k_adj_points' (its last block's counts
+    // were never written): skip its blocks.
+    if (A.al.head[tile] == -2) return;  // warp-uniform
     const int64_t b = tile * 32 + lane;
     const bool valid = b < pt.n;
     const int kc = A.kc;

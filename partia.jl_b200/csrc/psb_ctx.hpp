@@ -76,7 +76,7 @@ struct psb_ctx {
     void* adj_ha = nullptr;
     struct psb_ctx* sctx = nullptr;  // LBVH over the samples of the last adjoint call
     int64_t adj_blocks = 0;           // list-block pool of the two-kernel point adjoint (grown to the last need)
-    int adj_split = 1;                // 0: the point adjoint runs k_adj_points alone (psb_test_adjoint_pool)
+    int adj_split = 1;                // 0: k_adj_points alone; 2: the pool keeps its size (psb_test_adjoint_pool)
 
     cudaEvent_t ev[8] = {};
     // copy streams (in, out) and three more compute streams of the chunked

@@ -155,10 +155,12 @@ def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
     nl = O.Catalog(**spec).L
     gout = [rng.standard_normal(ns) for _ in range(nl)]
     res = []
+    npairs = []
     for blocks, split in ((0, 1), (3, 1), (0, 0)):  # default pool, 3 blocks, single kernel
         assert ctx.lib.psb_test_adjoint_pool(ctx.h, blocks, split) == L.PSB_OK
         res.append(ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy))
-        assert ctx.last_stats.pairs > 0
+        npairs.append(ctx.last_stats.pairs)
+    assert npairs[0] > 0 and npairs[1] == npairs[0] and npairs[2] == npairs[0]
     for key in ("m", "x", "y", "z"):
         assert np.array_equal(res[1][key], res[0][key]), key
         assert close(res[2][key], res[0][key]) <= 1e-12, key
@@ -168,7 +170,16 @@ def test_point_adjoint_two_kernels_bit_identical(kernel, strategy, spec):
             assert close(res[2]["cols"][c], res[0]["cols"][c]) <= 1e-12, c
     r = orc.adjoint_points(*s, O.Catalog(**spec), gout, strategy=strategy)
     compare(res[0], r, 4)
+    # a pool of 3 blocks that keeps its size: most tiles run in the single kernel
+    assert ctx.lib.psb_test_adjoint_pool(ctx.h, 3, 2) == L.PSB_OK
+    g = ctx.adjoint_points(*s, CatalogC(**spec), gout, strategy=strategy)
+    assert ctx.last_stats.pairs == npairs[0]
+    for key in ("m", "x", "y", "z"):
+        assert close(g[key], res[0][key]) <= 1e-12, key
+    compare(g, r, 4)
     assert ctx.lib.psb_test_adjoint_pool(ctx.h, -1, 1) == L.PSB_EINVAL
+    assert ctx.lib.psb_test_adjoint_pool(ctx.h, 0, 3) == L.PSB_EINVAL
+    assert ctx.lib.psb_test_adjoint_pool(ctx.h, 0, 1) == L.PSB_OK
 
 
 @pytest.mark.parametrize("spec", [

@@ -25,13 +25,25 @@ int make_recipe(psb_ctx* c, const psb_catalog* cat, bool line, Recipe& rec, std:
 // Sort keys of the particle tiles for the adjoint's walk, heaviest first:
 // a tile's walk and pairs grow with its particles' supports, and the tiles of
 // large-h particles in the outskirts hold many times the mean tile's pairs.
-// Cost: the sum of h^3 over the tile's 32 particles.
-__global__ void k_adj_tile_keys(const double* h, int64_t n, int64_t ntiles, uint64_t* keys, uint32_t* vals) {
+// Cost: the sum of h^3 over the tile's particles whose support reaches the
+// samples' box (box = min x, y, z, max x, y, z; K the support).  The key is
+// the cost's power of two only, and the radix sort is stable: tiles of like
+// cost keep their Morton order, and with it the walk's locality in the
+// sample tree.
+__global__ void k_adj_tile_keys(const double* x, const double* y, const double* z, const double* h, int64_t n,
+                                int64_t ntiles, double K, double b0, double b1, double b2, double b3, double b4,
+                                double b5, uint64_t* keys, uint32_t* vals) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= ntiles) return;
     double c = 0.0;
-    for (int64_t b = t * 32; b < t * 32 + 32 && b < n; ++b) c += h[b] * h[b] * h[b];
-    keys[t] = 0xFFFFFFFFull - (uint64_t)__float_as_uint((float)c);
+    for (int64_t b = t * 32; b < t * 32 + 32 && b < n; ++b) {
+        const double r = K * h[b];
+        const double dx = fmax(fmax(b0 - x[b], x[b] - b3), 0.0), dy = fmax(fmax(b1 - y[b], y[b] - b4), 0.0),
+                     dz = fmax(fmax(b2 - z[b], z[b] - b5), 0.0);
+        if (dx <= r && dy <= r && dz <= r) c += h[b] * h[b] * h[b];
+    }
+    const int e = c > 0.0 ? ilogb(c) + 1100 : 0;  // 0 .. ~2100, larger for more cost
+    keys[t] = (uint64_t)(4095 - e);
     vals[t] = (uint32_t)t;
 }
 
@@ -347,18 +359,25 @@ int run_adjoint(psb_ctx* c, const SampleReq& rq0, int hmode, const void* hs, int
                 launch_adj_rows(kcl, scal, lams, ns, kc, J.sv, recs, s);
                 AdjLists& al = J.al;
                 unsigned ptop = 0, povf = 0;
-                // the walk takes its tiles heaviest first (and with them the pool's
-                // blocks, which k_adj_bodies then runs in that order)
+                // The walk takes its tiles heaviest first (and with them the pool's
+                // blocks, which k_adj_bodies then runs in that order) when there
+                // are few tiles per SM: then the heavy tiles set the end (C2:
+                // 65,536 tiles, 8-field backward 22.1 -> 21.5 ms).  With many (the
+                // 2M tiles of 64M particles) the tail is a small part, and the
+                // Morton order's locality in the sample tree counts for more
+                // (there the cost-ordered walk took 101.5 against 99.8 ms).
                 AdjArgs W = J;
-                {
+                if (ntiles < (1ll << 18)) {
                     uint64_t* tk = (uint64_t*)scratch(c, 94, sizeof(uint64_t) * (size_t)ntiles);
                     char* tv = (char*)scratch(c, 95, sizeof(uint32_t) * (size_t)ntiles + 16);
                     if (!tk || !tv) return fail(c, PSB_ENOMEM, "scratch allocation failed (tile order)");
-                    k_adj_tile_keys<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>((const double*)c->h, n, ntiles, tk,
-                                                                                   (uint32_t*)(tv + 16));
+                    const double* bb = c->sctx->bbox;  // the samples' box
+                    k_adj_tile_keys<<<(unsigned)((ntiles + 255) / 256), 256, 0, s>>>(
+                        (const double*)c->x, (const double*)c->y, (const double*)c->z, (const double*)c->h, n, ntiles,
+                        (double)J.pt.Kd, bb[0], bb[1], bb[2], bb[3], bb[4], bb[5], tk, (uint32_t*)(tv + 16));
                     unsigned cnt = (unsigned)ntiles;
                     PSB_CUDA_TRY(c, cudaMemcpyAsync(tv, &cnt, sizeof(unsigned), cudaMemcpyHostToDevice, s), "tile count");
-                    PSB_CUDA_TRY(c, radix_sort_pairs(tk, (uint32_t*)(tv + 16), ntiles, c, 6, &launches, false, 32),
+                    PSB_CUDA_TRY(c, radix_sort_pairs(tk, (uint32_t*)(tv + 16), ntiles, c, 6, &launches, false, 16),
                                  "tile order sort");
                     W.tile_list = (const int32_t*)(tv + 16);
                     W.tile_count = (const unsigned*)tv;

@@ -331,7 +331,11 @@ int psb_neighbor_digest(psb_ctx* ctx, int32_t kind, int64_t ns,
  * density) needs no forward pass.  The
  * pair terms are summed per particle by a traversal of an LBVH over the
  * samples (points, grids), or of the pixel lattice (beams), with the forward's
- * inclusion arithmetic: no float atomics.  gout, hs and the gradient arrays
+ * inclusion arithmetic: no float atomics.  Points and grids keep the
+ * traversal's pair lists in a device pool of the context that grows to what
+ * a call needs and stays for the next (at most 32 GiB; a call that outgrows it
+ * walks again, so a context's first large call is the slowest); the results
+ * do not depend on the pool's size.  gout, hs and the gradient arrays
  * are device pointers with PSB_FLAG_DEVICE_PTRS, host pointers otherwise;
  * grid axes, frame and params are host pointers. */
 int psb_adjoint_points(psb_ctx* ctx, int64_t ns,

@@ -48,8 +48,7 @@ __global__ void k_adj_tile_keys(const double* x, const double* y, const double* 
 }
 
 // pass: 0 = k_adj_points (whole tiles, or the listed ones), 1 = its pair-list
-// form (k_adj_collect), 2 = k_adj_bodies (grid over list blocks), 3 =
-// k_adj_combine
+// form (COL), 2 = k_adj_bodies (grid over list blocks), 3 = k_adj_combine
 template <int KC, bool SCAL, int KF>
 static void launch_adj_points_ks(const AdjArgs& a, int st, int pass, unsigned g, cudaStream_t s) {
     if (pass == 1) {

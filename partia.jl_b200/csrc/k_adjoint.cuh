@@ -71,7 +71,7 @@ struct AdjArgs {
     const double* lut;
     unsigned* err;
     unsigned long long* stats;    // [0] pairs, [2] walk steps
-    // the two-kernel point path (k_adj_collect + k_adj_bodies)
+    // the two-kernel point path (k_adj_points' list form, k_adj_bodies, k_adj_combine)
     AdjLists al;
     const double* lamT;           // records of the samples for k_adj_bodies (AdjRec, sample-tree order)
     const int32_t* tile_list;     // k_adj_points over these particle tiles only (the lists' overflow), or null
@@ -305,7 +305,7 @@ template <int KC, bool SCAL> struct ALam {
 // the cotangent row (in A.lam) of staged row r
 template <bool SCAL> __device__ __forceinline__ int lam_row(int r) { return SCAL ? (r == 0 ? 0 : 7 + r) : r; }
 
-// COL: the pair-list pass of the two-kernel path (k_adj_collect): the same
+// COL: the pair-list pass of the two-kernel path (the list form): the same
 // walk and pair decisions, with each lane's accepted samples of a span
 // written to its tile's chain of list blocks instead of summed.
 template <int ST, int KC, bool SCAL, int KF, bool COL = false>
